@@ -1,0 +1,114 @@
+"""CPU oracle (test infrastructure only).
+
+Python binding of oracle/liblsg_oracle.so, the C restatement of LoAdSG's
+prewavelet matvec, Jacobi diagonal and CG.  Only tests/, the smoke check in
+__graft_entry__.py and bench.py's CPU-baseline legs import this package; the
+product path (loadsg_b200) never does.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE, "oracle"], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liblsg_oracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        L.lsgo_grid_create.restype = P
+        L.lsgo_grid_create.argtypes = [ctypes.c_int, P, P, ctypes.c_int64]
+        L.lsgo_grid_free.argtypes = [P]
+        L.lsgo_num_depths.argtypes = [P]
+        L.lsgo_depths.argtypes = [P, P]
+        L.lsgo_sorted_depths.argtypes = [P, ctypes.c_int, P]
+        L.lsgo_num_cells.restype = ctypes.c_int64
+        L.lsgo_num_cells.argtypes = [P, P]
+        L.lsgo_lookup.restype = ctypes.c_int64
+        L.lsgo_lookup.argtypes = [P, P]
+        L.lsgo_matvec.argtypes = [P, ctypes.c_int, P, P, P]
+        L.lsgo_diag.argtypes = [P, ctypes.c_int, P, P]
+        L.lsgo_cg.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_double, ctypes.c_int, P]
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class OracleGrid:
+    """A grid given by its points (N x d 1D indices, storage order) and active flags."""
+
+    def __init__(self, points, active):
+        self.points = np.ascontiguousarray(points, dtype=np.int32)
+        self.active = np.ascontiguousarray(active, dtype=np.uint8)
+        self.n, self.d = self.points.shape
+        self._h = lib().lsgo_grid_create(self.d, _ptr(self.points), _ptr(self.active), self.n)
+        if not self._h:
+            raise ValueError("invalid grid")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().lsgo_grid_free(self._h)
+            self._h = None
+
+    def depths(self):
+        nd = lib().lsgo_num_depths(self._h)
+        out = np.zeros((nd, self.d), np.int32)
+        lib().lsgo_depths(self._h, _ptr(out))
+        return out
+
+    def sorted_depths(self, case):
+        nd = lib().lsgo_num_depths(self._h)
+        out = np.zeros((nd, self.d), np.int32)
+        k = lib().lsgo_sorted_depths(self._h, case, _ptr(out))
+        return out[:k]
+
+    def num_cells(self, T):
+        T = np.ascontiguousarray(T, np.int32)
+        return lib().lsgo_num_cells(self._h, _ptr(T))
+
+    def lookup(self, idx):
+        idx = np.ascontiguousarray(idx, np.int32)
+        return lib().lsgo_lookup(self._h, _ptr(idx))
+
+    @staticmethod
+    def _params(params):
+        p = np.zeros(256, np.float64)
+        params = np.asarray(params, np.float64)
+        p[: len(params)] = params
+        return p
+
+    def matvec(self, family, params, x, y=None):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.n) if y is None else np.array(y, np.float64)
+        p = self._params(params)
+        if lib().lsgo_matvec(self._h, family, _ptr(p), _ptr(x), _ptr(y)) != 0:
+            raise MemoryError("oracle matvec failed")
+        return y
+
+    def diag(self, family, params):
+        out = np.zeros(self.n)
+        p = self._params(params)
+        lib().lsgo_diag(self._h, family, _ptr(p), _ptr(out))
+        return out
+
+    def cg(self, family, params, f, eps, maxit=500, x0=None):
+        f = np.ascontiguousarray(f, np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, np.float64)
+        p = self._params(params)
+        it = np.zeros(1, np.int32)
+        lib().lsgo_cg(self._h, family, _ptr(p), _ptr(f), _ptr(x), eps, maxit, _ptr(it))
+        return x, int(it[0])

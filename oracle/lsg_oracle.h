@@ -1,0 +1,45 @@
+/*
+ * lsg_oracle -- CPU restatement of LoAdSG's prewavelet matvec and CG.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py load this library, and only
+ * as the checker.  The product (loadsg_b200) never links or calls it.
+ *
+ * It follows the reference's algorithm step by step, on full-length vectors
+ * indexed by storage index, with a hash map standing in for the reference's
+ * hash grids.  Every function cites the reference code it restates
+ * (paths relative to library/source/).  Parity with the compiled reference is
+ * pinned by the .npz fixtures in tests/golden, generated by oracle/ref_harness.cpp.
+ */
+#ifndef LSG_ORACLE_H
+#define LSG_ORACLE_H
+#include <stdint.h>
+
+typedef struct lsgo_grid lsgo_grid;
+
+/* points: N*d 1D indices in storage order; active: N flags (1 = active). */
+lsgo_grid *lsgo_grid_create(int d, const int32_t *points, const uint8_t *active, int64_t n);
+void lsgo_grid_free(lsgo_grid *g);
+
+/* DepthList (iterator/depthIterator.h:14-50): depths in first-appearance order. */
+int lsgo_num_depths(const lsgo_grid *g);
+void lsgo_depths(const lsgo_grid *g, int32_t *out /* num_depths*d */);
+/* sortDepths (iterator/depthIterator.cpp:7-45) for case bit mask c; returns count. */
+int lsgo_sorted_depths(const lsgo_grid *g, int c, int32_t *out /* num_depths*d */);
+/* Number of cells of depth T+1 inside the grid (cells/CellStructure.h:23-61). */
+int64_t lsgo_num_cells(const lsgo_grid *g, const int32_t *T);
+/* Storage index of a point given by its d 1D indices, or -1. */
+int64_t lsgo_lookup(const lsgo_grid *g, const int32_t *idx);
+
+/* y[active] = A_prew x  (MatrixVectorHomogen::multiplication over
+ * LocalStiffnessMatrices with the midpoint-coefficient plugin); entries of y at
+ * hanging nodes are left untouched, as in the reference. */
+int lsgo_matvec(lsgo_grid *g, int family, const double *params, const double *x, double *y);
+/* Jacobi diagonal a(psi_i, psi_i) (Preconditioning::precondLocalStiffnessMatrix). */
+int lsgo_diag(lsgo_grid *g, int family, const double *params, double *diag);
+/* CG::solveHomogen with the reference stopping rule (delta = r^T D^-1 r > eps,
+ * break when delta' < eps^2, at most maxit iterations).  x is in/out. */
+int lsgo_cg(lsgo_grid *g, int family, const double *params, const double *f, double *x, double eps,
+            int maxit, int *iterations);
+
+#endif

@@ -1,0 +1,336 @@
+// Reference harness: TEST INFRASTRUCTURE ONLY.
+//
+// A driver of our own that is compiled against the unmodified LoAdSG sources
+// (oracle/Makefile builds them in place) and calls only the reference's public
+// API.  It generates the golden vectors that pin the oracle and the CUDA path:
+//   * grids built by AdaptiveSparseGrid::AddRecursiveSonsOfPoint
+//     (library/source/sgrid/sparseGrid.cc:557-566), optional refinement by
+//     AddPoint of sons, then completeDirichletGrid (sparseGrid.cc:771-787);
+//   * integer tables read back through the reference's own lookups
+//     (DepthList, sortDepths, MultiDepthHashGrid, CellData, nextFiveP);
+//   * the variable-coefficient matvec through the reference plugin point
+//     StencilTemplate::integration (library/source/stencils/Stencil.h:740)
+//     consumed by LocalStiffnessMatricesMemoryDistribution and
+//     MatrixVectorHomogen::multiplication (MatrixVectorHomogen.h:659-759);
+//   * the Jacobi diagonal (Preconditioning, applications/cg_method.h:81-754)
+//     and CG::solveHomogen (cg_method.h:759-886).
+// Outputs are raw little-endian arrays in an output directory plus meta.txt;
+// tests/golden/make_golden.py packs them into .npz fixtures.
+#include "sparseEXPDE.h"
+#include "coefficient.h"
+
+#include <chrono>
+#include <cstdio>
+#include <fstream>
+#include <map>
+#include <string>
+#include <vector>
+
+static const int D = DimensionSparseGrid;
+
+// ---------------------------------------------------------------- options
+static std::map<std::string, std::string> g_opt;
+static std::string opt(const char *k, const char *def) {
+    auto it = g_opt.find(k);
+    return it == g_opt.end() ? std::string(def) : it->second;
+}
+static std::vector<double> parse_list(const std::string &s) {
+    std::vector<double> v;
+    size_t i = 0;
+    while (i < s.size()) {
+        size_t j = s.find(',', i);
+        if (j == std::string::npos) j = s.size();
+        if (j > i) v.push_back(atof(s.substr(i, j - i).c_str()));
+        i = j + 1;
+    }
+    return v;
+}
+
+// ---------------------------------------------------------------- I/O
+static std::string g_out;
+static std::ofstream g_meta;
+template <class T>
+static void dump(const char *name, const std::vector<T> &v) {
+    std::string p = g_out + "/" + name;
+    FILE *f = fopen(p.c_str(), "wb");
+    if (!f) { perror(p.c_str()); exit(2); }
+    if (!v.empty()) fwrite(v.data(), sizeof(T), v.size(), f);
+    fclose(f);
+    g_meta << "array " << name << " " << v.size() << "\n";
+}
+static std::vector<double> read_f64(const std::string &p, size_t n) {
+    std::vector<double> v(n, 0.0);
+    FILE *f = fopen(p.c_str(), "rb");
+    if (!f) { perror(p.c_str()); exit(2); }
+    size_t got = fread(v.data(), sizeof(double), n, f);
+    fclose(f);
+    if (got != n) { fprintf(stderr, "short read %s\n", p.c_str()); exit(2); }
+    return v;
+}
+
+// ---------------------------------------------------------------- plugin
+// Midpoint-coefficient diffusion: a(x_c) times the exact Q1 stiffness entry.
+class MidpointDiffusion : public StencilTemplate {
+public:
+    int family;
+    std::vector<double> p;
+    MidpointDiffusion(AdaptiveSparseGrid &g, int fam, std::vector<double> par)
+        : StencilTemplate(g), family(fam), p(par) { p.resize(LSG_COEF_MAXPARAM, 0.0); }
+    double integration(CellDimension &cell, CellIndexDirection &dp, CellIndexDirection &dq) override {
+        double h[D], xc[D];
+        unsigned mp = 0, mq = 0;
+        for (int d = 0; d < D; ++d) {
+            double lo = cell.getLeftBoundary(d), hi = cell.getRightBoundary(d);
+            h[d] = hi - lo;
+            xc[d] = 0.5 * (lo + hi);
+            if (dp.getDirection(d) == Right) mp |= 1u << d;
+            if (dq.getDirection(d) == Right) mq |= 1u << d;
+        }
+        return lsg_coef_eval(family, p.data(), D, xc) * lsg_q1_stiffness(D, h, mp, mq);
+    }
+};
+
+// ---------------------------------------------------------------- grid
+static bool refine_point(const IndexDimension &I, int round, const std::string &target, double theta) {
+    double thr = theta / double(1 << (round - 1));
+    if (target == "corner") {
+        for (int d = 0; d < D; ++d)
+            if (!(I.coordinate(d) < thr)) return false;
+        return true;
+    }
+    if (target == "plane") return fabs(I.coordinate(0) - 0.5) < thr;
+    return false;
+}
+
+static void build_grid(AdaptiveSparseGrid &grid) {
+    int level = atoi(opt("level", "3").c_str());
+    int refine = atoi(opt("refine", "0").c_str());
+    double theta = atof(opt("theta", "0.5").c_str());
+    std::string target = opt("target", "corner");
+    IndexDimension center;
+    grid.AddRecursiveSonsOfPoint(center, level);
+    for (int r = 1; r <= refine; ++r) {
+        std::vector<IndexDimension> todo;
+        for (unsigned long k = 0; k < grid.getMaximalOccupiedSecondTable(); ++k) {
+            if (!grid.getActiveTable()[k]) continue;
+            IndexDimension I = grid.getIndexOfTable(k);
+            if (refine_point(I, r, target, theta)) todo.push_back(I);
+        }
+        for (auto &I : todo)
+            for (int d = 0; d < D; ++d) {
+                grid.AddPoint(I.leftSon(d));
+                grid.AddPoint(I.rightSon(d));
+            }
+    }
+    if (refine > 0 || opt("complete", "0") == "1") grid.completeDirichletGrid();
+}
+
+static void dump_grid(AdaptiveSparseGrid &grid) {
+    unsigned long N = grid.getMaximalOccupiedSecondTable();
+    std::vector<int32_t> idx(N * D);
+    std::vector<uint8_t> act(N);
+    for (unsigned long k = 0; k < N; ++k) {
+        IndexDimension I = grid.getIndexOfTable(k);
+        for (int d = 0; d < D; ++d) idx[k * D + d] = I.getIndex(d);
+        act[k] = grid.getActiveTable()[k] ? 1 : 0;
+    }
+    dump("points.i32", idx);
+    dump("active.u8", act);
+    g_meta << "N " << N << "\nd " << D << "\ndofs " << grid.getDOFS() << "\n";
+}
+
+// ---------------------------------------------------------------- tables
+static long lookup(AdaptiveSparseGrid &grid, IndexDimension I) {
+    unsigned long k;
+    if (grid.occupied(k, I)) return (long)k;
+    return -1;
+}
+
+static void dump_tables(AdaptiveSparseGrid &grid) {
+    unsigned long N = grid.getMaximalOccupiedSecondTable();
+    DepthList dl(grid);
+    std::vector<int32_t> depths;
+    std::vector<Depth> dv;
+    for (auto it = dl.begin_all(); it != dl.end_all(); ++it) {
+        dv.push_back(*it);
+        for (int d = 0; d < D; ++d) depths.push_back(it->at(d));
+    }
+    dump("depthlist.i32", depths);
+    // per-case sorted depth order (CasesIterator bit i = restriction in dim i)
+    std::vector<int32_t> sorted, sorted_off;
+    for (CasesIterator ci; ci.goon(); ++ci) {
+        bool *r = ci.getcase();
+        dl.sortDepths(r);
+        sorted_off.push_back((int32_t)sorted.size() / D);
+        for (Depth T : *dl.getSortierteTiefen())
+            for (int d = 0; d < D; ++d) sorted.push_back(T.at(d));
+    }
+    sorted_off.push_back((int32_t)sorted.size() / D);
+    dump("sorted.i32", sorted);
+    dump("sorted_off.i32", sorted_off);
+    // points of exact depth (MultiDepthHashGrid insertion order)
+    std::vector<int32_t> exact, exact_off;
+    for (Depth T : dv) {
+        exact_off.push_back((int32_t)exact.size());
+        SingleDepthHashGrid &g = grid.getMultiDepthHashGrid()->getGridForDepth(T);
+        for (auto k : g._mapPosToGridPos) exact.push_back((int32_t)k);
+    }
+    exact_off.push_back((int32_t)exact.size());
+    dump("exact.i32", exact);
+    dump("exact_off.i32", exact_off);
+    // multilevel store size
+    MultiLevelAdaptiveSparseGrid mgrid(&grid);
+    g_meta << "mgrid_size " << mgrid.getMaximalOccupiedSecondTable() << "\n";
+    // same-level 1D neighbours (IndexDimension::nextLeft/nextRight) per dim
+    std::vector<int32_t> nb(N * D * 2);
+    for (unsigned long k = 0; k < N; ++k) {
+        IndexDimension I = grid.getIndexOfTable(k);
+        for (int d = 0; d < D; ++d) {
+            nb[(k * D + d) * 2 + 0] = (int32_t)lookup(grid, I.nextLeft(d));
+            nb[(k * D + d) * 2 + 1] = (int32_t)lookup(grid, I.nextRight(d));
+        }
+    }
+    dump("nbr1d.i32", nb);
+    // prewavelet 5^d stencil of every active point at its own depth (nextFiveP,
+    // indices/index.cc:252-327) as used by calcNodal (MatrixVectorHomogen.cpp:43-74)
+    std::vector<int32_t> st_j, st_off;
+    std::vector<double> st_w;
+    for (unsigned long k = 0; k < N; ++k) {
+        st_off.push_back((int32_t)st_j.size());
+        if (!grid.getActiveTable()[k]) continue;
+        IndexDimension I = grid.getIndexOfTable(k);
+        Depth T(I);
+        MultiDimFiveCompass mc;
+        for (; mc.hasNext(); ++mc) {
+            double w = 1.0;
+            IndexDimension J = I.nextFiveP(&mc, T, &w);
+            if (mc.goon()) {
+                st_j.push_back((int32_t)lookup(grid, J));
+                st_w.push_back(w);
+            }
+        }
+    }
+    st_off.push_back((int32_t)st_j.size());
+    dump("stencil_j.i32", st_j);
+    dump("stencil_w.f64", st_w);
+    dump("stencil_off.i32", st_off);
+    // cells of depth T+1 for every depth T, corners in CellIndexIterator order
+    CellData cd(grid);
+    std::vector<int32_t> cells, cells_off, corner_idx;
+    for (Depth T : dv) {
+        Depth Tc = T;
+        ++Tc;
+        cells_off.push_back((int32_t)(cells.size() >> D));
+        const SingleDepthHashCellStructure &cg = cd.getGridForDepth(Tc);
+        for (size_t i = 0; i < cg.getNumberOfEntries(); ++i) {
+            CellDimension cell = cg._map.getIndexOfTable(i);
+            for (CellIndexIterator it(&cell); it.goon(); ++it) {
+                IndexDimension P = it.getIndex();
+                cells.push_back(P.isNotAtBoundary() ? (int32_t)lookup(grid, P) : -1);
+                for (int d = 0; d < D; ++d) corner_idx.push_back(P.getIndex(d));
+            }
+        }
+    }
+    cells_off.push_back((int32_t)(cells.size() >> D));
+    dump("cells.i32", cells);
+    dump("cells_off.i32", cells_off);
+    dump("cell_corners.i32", corner_idx);
+}
+
+// ---------------------------------------------------------------- numerics
+static MidpointDiffusion make_plugin(AdaptiveSparseGrid &grid) {
+    int fam = atoi(opt("coef", "1").c_str());
+    std::vector<double> p = parse_list(opt("cp", "1,0.5,1,1,1,1,1,1,1,1"));
+    return MidpointDiffusion(grid, fam, p);
+}
+
+static void set_vec(VectorSparseG &v, const std::vector<double> &x) {
+    for (unsigned long k = 0; k < x.size(); ++k) v.setValue(k, x[k]);
+}
+static std::vector<double> get_vec(VectorSparseG &v, unsigned long N) {
+    std::vector<double> y(N);
+    for (unsigned long k = 0; k < N; ++k) y[k] = v.getValue(k);
+    return y;
+}
+
+int main(int argc, char **argv) {
+    if (argc < 3) {
+        fprintf(stderr, "usage: %s grid|tables|matvec|poisson|diag|cg outdir [key=value ...]\n", argv[0]);
+        return 2;
+    }
+    std::string cmd = argv[1];
+    g_out = argv[2];
+    for (int i = 3; i < argc; ++i) {
+        std::string a = argv[i];
+        size_t e = a.find('=');
+        if (e != std::string::npos) g_opt[a.substr(0, e)] = a.substr(e + 1);
+    }
+    g_meta.open(g_out + "/meta_" + cmd + ".txt");
+    AdaptiveSparseGrid grid;
+    build_grid(grid);
+    unsigned long N = grid.getMaximalOccupiedSecondTable();
+    if (cmd == "grid") {
+        dump_grid(grid);
+    } else if (cmd == "tables") {
+        dump_tables(grid);
+    } else if (cmd == "matvec" || cmd == "poisson") {
+        std::vector<double> x = read_f64(opt("x", ""), N);
+        MultiLevelAdaptiveSparseGrid mgrid(&grid);
+        MatrixVectorHomogen m(grid, mgrid, true, false);
+        VectorSparseG xv(grid), yv(grid);
+        set_vec(xv, x);
+        auto t0 = std::chrono::steady_clock::now();
+        double secs;
+        if (cmd == "poisson") {
+            Poisson pois(grid);
+            t0 = std::chrono::steady_clock::now();
+            m.multiplication(xv, yv, pois);
+            secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        } else {
+            MidpointDiffusion plug = make_plugin(grid);
+            LocalStiffnessMatricesMemoryDistribution lsm(grid, plug, 1);
+            int reps = atoi(opt("reps", "1").c_str());
+            t0 = std::chrono::steady_clock::now();
+            for (int r = 0; r < reps; ++r) m.multiplication(xv, yv, lsm);
+            secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() / reps;
+        }
+        dump("y.f64", get_vec(yv, N));
+        g_meta << "matvec_seconds " << secs << "\n";
+    } else if (cmd == "diag") {
+        MidpointDiffusion plug = make_plugin(grid);
+        LocalStiffnessMatricesMemoryDistribution lsm(grid, plug, 1);
+        VectorSparseG z(grid);
+        Preconditioning<LocalStiffnessMatricesMemoryDistribution> P(z, lsm);
+        dump("diag.f64", get_vec(z, N));
+    } else if (cmd == "cg") {
+        std::vector<double> f = read_f64(opt("f", ""), N);
+        double eps = atof(opt("eps", "1e-10").c_str());
+        MultiLevelAdaptiveSparseGrid mgrid(&grid);
+        MatrixVectorHomogen m(grid, mgrid, true, false);
+        MidpointDiffusion plug = make_plugin(grid);
+        LocalStiffnessMatricesMemoryDistribution lsm(grid, plug, 1);
+        VectorSparseG fv(grid), xv(grid), usol(grid), r(grid);
+        set_vec(fv, f);
+        xv = 0.0;
+        int it = 0;
+        double tp = 0.0;
+        auto t0 = std::chrono::steady_clock::now();
+        CG::solveHomogen(eps, xv, fv, &it, usol, m, lsm, &tp);
+        double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        m.multiplication(xv, r, lsm);
+        std::vector<double> x = get_vec(xv, N), Ax = get_vec(r, N);
+        double rr = 0.0, ff = 0.0;
+        for (unsigned long k = 0; k < N; ++k) {
+            rr += (f[k] - Ax[k]) * (f[k] - Ax[k]);
+            ff += f[k] * f[k];
+        }
+        dump("x.f64", x);
+        g_meta << "iterations " << it << "\nrelres " << sqrt(rr / ff) << "\nsolve_seconds " << secs
+               << "\nprecond_seconds " << tp << "\n";
+    } else {
+        fprintf(stderr, "unknown command %s\n", cmd.c_str());
+        return 2;
+    }
+    g_meta << "ok 1\n";
+    return 0;
+}

@@ -1,0 +1,129 @@
+"""Generate the golden fixtures in tests/golden/ from the compiled reference.
+
+Run in a container that has the reference sources (the path is given by
+--refsrc).  For every case below it builds oracle/_ref/d<d>/ref_harness (the
+unmodified LoAdSG sources compiled in place plus oracle/ref_harness.cpp), runs
+it, and packs the arrays into tests/golden/<name>.npz.  The fixtures are small
+(a few hundred KB in total) and committed; the GPU box never needs the
+reference.
+
+    python tests/golden/make_golden.py [--refsrc /path/to/library/source] [--only NAME]
+"""
+import argparse
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE = os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle")
+
+# Coefficient families (oracle/coefficient.h): params as passed to the plugin.
+SINPROD = (1, [1.0, 0.5] + [1.0] * 8)           # a = 1 + 0.5 prod sin(pi x_i)
+EXPSIN6 = (2, [0.3, -0.2, 0.25, 0.1, -0.15, 0.2, 0, 0])  # a = exp(sum c_k sin(k pi x_k))
+SINPROD_M = (1, [1.0, 0.9, 2.0, 1.0, 3.0, 2.0, 1.0, 3.0, 1.0, 2.0])
+CONST1 = (0, [1.0])
+SIN2PI = (4, [1.0, 0.5])
+
+# name, d, grid args, coefficient, commands
+CASES = [
+    ("d3_L3", 3, "level=3", SINPROD, ["tables", "matvec", "poisson", "diag", "cg"]),
+    ("d3_L5", 3, "level=5", SINPROD, ["tables", "matvec", "poisson", "diag", "cg"]),
+    ("d3_adapt", 3, "level=2 refine=3 theta=0.6 target=corner", SINPROD, ["tables", "matvec", "diag", "cg"]),
+    ("d3_plane", 3, "level=3 refine=2 theta=0.3 target=plane", SIN2PI, ["tables", "matvec", "diag"]),
+    ("d2_L6", 2, "level=6", SINPROD_M, ["tables", "matvec", "poisson", "diag", "cg"]),
+    ("d2_adapt", 2, "level=3 refine=3 theta=0.45 target=corner", SINPROD, ["tables", "matvec", "diag", "cg"]),
+    ("d4_L3", 4, "level=3", EXPSIN6, ["tables", "matvec", "diag", "cg"]),
+    ("d4_plane", 4, "level=2 refine=2 theta=0.3 target=plane", SINPROD_M, ["tables", "matvec", "diag"]),
+    ("d5_L2", 5, "level=2", EXPSIN6, ["tables", "matvec", "diag"]),
+    ("d6_L2", 6, "level=2", EXPSIN6, ["tables", "matvec", "poisson", "diag", "cg"]),
+    ("d6_L3", 6, "level=3", SINPROD_M, ["matvec", "diag"]),
+]
+
+
+def run(cmd, **kw):
+    r = subprocess.run(cmd, capture_output=True, text=True, **kw)
+    if r.returncode != 0:
+        raise RuntimeError(f"{cmd} failed:\n{r.stdout}\n{r.stderr}")
+    return r.stdout
+
+
+def read_meta(path):
+    meta, arrays = {}, []
+    for line in open(path):
+        parts = line.split()
+        if not parts:
+            continue
+        if parts[0] == "array":
+            arrays.append(parts[1])
+        else:
+            meta[parts[0]] = parts[1]
+    return meta, arrays
+
+
+DTYPES = {"i32": np.int32, "u8": np.uint8, "f64": np.float64}
+
+
+def load_arrays(outdir, names, prefix):
+    res = {}
+    for n in names:
+        stem, ext = n.rsplit(".", 1)
+        res[prefix + stem] = np.fromfile(os.path.join(outdir, n), dtype=DTYPES[ext])
+    return res
+
+
+def make_case(name, d, gridargs, coef, cmds, refsrc):
+    run(["make", "-s", "-C", ORACLE, "ref", f"D={d}", f"REFSRC={refsrc}", "-j8"])
+    exe = os.path.join(ORACLE, "_ref", f"d{d}", "ref_harness")
+    fam, params = coef
+    cp = "cp=" + ",".join(repr(float(p)) for p in params)
+    args = gridargs.split() + [f"coef={fam}", cp]
+    out = {"d": np.int32(d), "coef_family": np.int32(fam), "coef_params": np.array(params, np.float64)}
+    with tempfile.TemporaryDirectory() as tmp:
+        run([exe, "grid", tmp] + args)
+        meta, arrs = read_meta(os.path.join(tmp, "meta_grid.txt"))
+        out.update(load_arrays(tmp, arrs, ""))
+        n = int(meta["N"])
+        rng = np.random.default_rng(sum(map(ord, name)))
+        x = rng.uniform(-1.0, 1.0, n)
+        f = rng.uniform(-1.0, 1.0, n) * (out["active"] > 0)
+        x.tofile(os.path.join(tmp, "x_in.f64"))
+        f.tofile(os.path.join(tmp, "f_in.f64"))
+        out["x"] = x
+        out["f"] = f
+        for c in cmds:
+            extra = []
+            if c in ("matvec", "poisson"):
+                extra = [f"x={tmp}/x_in.f64"]
+            if c == "cg":
+                extra = [f"f={tmp}/f_in.f64", "eps=1e-20"]
+            run([exe, c, tmp] + args + extra)
+            meta, arrs = read_meta(os.path.join(tmp, f"meta_{c}.txt"))
+            got = load_arrays(tmp, arrs, c + "_")
+            out.update(got)
+            for k, v in meta.items():
+                if k not in ("ok",):
+                    try:
+                        out[f"{c}_meta_{k}"] = np.float64(float(v))
+                    except ValueError:
+                        pass
+    out["gridargs"] = np.array(gridargs)
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"{name}: N={n} -> {os.path.getsize(path)} bytes")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--refsrc", default="/root/reference/library/source")
+    ap.add_argument("--only", default=None)
+    a = ap.parse_args()
+    for case in CASES:
+        if a.only and case[0] != a.only:
+            continue
+        make_case(*case, refsrc=a.refsrc)
+
+
+if __name__ == "__main__":
+    main()
