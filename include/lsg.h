@@ -1,0 +1,153 @@
+/*
+ * lsg.h -- C-ABI of the B200 prewavelet matvec / CG library (liblsg.so).
+ *
+ * Plain pointers and sizes only.  Every function returns 0 on success and a
+ * negative LSG_E* code on failure; lsg_last_error() gives the message of the
+ * calling thread's last failure.  Nothing here calls exit() (the reference
+ * does, e.g. LocalStiffnessMatrices.cpp:267-268).
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to LoAdSG's library/source/).
+ */
+#ifndef LSG_H
+#define LSG_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSG_OK 0
+#define LSG_E_INVALID -1   /* bad argument or grid */
+#define LSG_E_CUDA -2      /* CUDA runtime failure (device missing, out of memory, ...) */
+#define LSG_E_STATE -3     /* call order (e.g. no coefficient set) */
+#define LSG_E_NOCONV -4    /* solver did not reach the tolerance */
+
+#define LSG_FP64 0
+#define LSG_FP32 1
+
+/* Coefficient families of -div(a grad u); a is sampled at each cell midpoint.
+ * Parameter layouts (p = params):
+ *   LSG_COEF_CONST     a = p[0]
+ *   LSG_COEF_SINPROD   a = p[0] + p[1] prod_i sin(pi p[2+i] x_i)
+ *   LSG_COEF_EXPSIN    a = exp(sum_{k=1..d} p[k-1] sin(k pi x_{k-1}))
+ *   LSG_COEF_LOGNORMAL a = exp(sum_{j<J} p[1+j] prod_i sin(pi p[1+J+j*d+i] x_i)), J = p[0]
+ *   LSG_COEF_SIN2PI    a = p[0] + p[1] sin(2 pi x_0) cos(2 pi x_1)              */
+#define LSG_COEF_CONST 0
+#define LSG_COEF_SINPROD 1
+#define LSG_COEF_EXPSIN 2
+#define LSG_COEF_LOGNORMAL 3
+#define LSG_COEF_SIN2PI 4
+
+typedef struct lsg_operator lsg_operator;
+
+typedef struct {
+    int32_t d;
+    int64_t n_points;     /* N (active + hanging) */
+    int64_t n_active;
+    int32_t n_depths;     /* |D| */
+    int64_t n_slab_entries;  /* sum_T N_T (multilevel entries) */
+    int64_t n_cells;      /* sum_T C_T */
+    int64_t case_slab_entries;   /* sum_c sum_{T in S(c)} N_T */
+    int64_t case_cells;          /* sum_c sum_{T in S(c)} C_T */
+    int64_t device_bytes; /* device memory held by the operator */
+    double plan_seconds;
+    double matvec_bytes_fp64;    /* algorithmic bytes of one FP64 matvec */
+    double matvec_flops;         /* algorithmic flops of one matvec (cell apply) */
+} lsg_info;
+
+/* Flattens the grid (AdaptiveSparseGrid in storage order: getIndexOfTable(k),
+ * sgrid/sparseGrid.h:566-572, and getActiveTable()) and uploads the tables.
+ * Replaces MatrixVectorHomogen(grid, mgrid, symmetry, mpi_on)
+ * (MatrixVectorMultiplication/MatrixVectorHomogen.h:72-77) together with
+ * MultiLevelAdaptiveSparseGrid and CellData construction.
+ * points: n*d 1D indices; active: n flags.  Uses the current CUDA device. */
+int lsg_operator_create(int32_t d, const int32_t *points, const uint8_t *active, int64_t n, lsg_operator **out);
+void lsg_operator_destroy(lsg_operator *op);
+int lsg_operator_info(const lsg_operator *op, lsg_info *info);
+
+/* Sets the coefficient (replaces constructing the StencilTemplate plugin,
+ * stencils/Stencil.h:740, and LocalStiffnessMatricesMemoryDistribution,
+ * localStiffnessMatrices/LocalStiffnessMatricesMemoryDistribution.h:14-159). */
+int lsg_operator_set_coefficient(lsg_operator *op, int32_t family, const double *params, int32_t nparams);
+
+/* y = A_prew x with host buffers of n doubles in storage order; y is written
+ * at active points only (hanging entries untouched), as
+ * MatrixVectorHomogen::multiplication (MatrixVectorHomogen.h:91-92,659-759). */
+int lsg_matvec(lsg_operator *op, const double *x, double *y);
+
+/* Same on device buffers of n elements (double for LSG_FP64, float for
+ * LSG_FP32), enqueued on `stream` (a cudaStream_t, 0 = legacy default). */
+int lsg_matvec_device(lsg_operator *op, const void *x, void *y, int32_t precision, void *stream);
+
+/* Exact Jacobi diagonal a(psi_i, psi_i) at active points (0 at hanging), as
+ * Preconditioning::precondLocalStiffnessMatrix (applications/cg_method.h:544-680). */
+int lsg_diag(lsg_operator *op, double *diag);
+int lsg_diag_device(lsg_operator *op, double *diag, void *stream);
+
+typedef struct {
+    double eps;          /* tolerance (meaning set by `criterion`) */
+    int32_t criterion;   /* 0: reference rule on delta = r^T D^-1 r (cg_method.h:852,871);
+                            1: true relative residual ||f - A x|| / ||f|| <= eps */
+    int32_t max_iter;    /* 0 = 500 (cg_method.h:35) */
+    int32_t precond;     /* 0 Jacobi (reference), 1 none, 2 learned diagonal (see lsg_set_learned_diag) */
+    int32_t precision;   /* LSG_FP64: plain CG; LSG_FP32: FP32 inner CG in FP64 iterative refinement */
+    int32_t inner_iter;  /* FP32+IR: inner iterations per refinement step (0 = 30) */
+    double inner_tol;    /* FP32+IR: inner relative reduction (0 = 1e-4) */
+    int32_t use_graph;   /* capture one CG iteration as a CUDA graph */
+} lsg_solver_opts;
+
+typedef struct {
+    int32_t iterations;      /* CG iterations (inner iterations summed for IR) */
+    int32_t outer_iterations;
+    double rel_residual;     /* ||f - A x|| / ||f|| recomputed in FP64 */
+    double seconds;          /* device time of the solve */
+    int32_t converged;
+    int32_t fell_back;       /* learned preconditioner stalled -> Jacobi */
+} lsg_solve_report;
+
+/* Solves A x = f (CG::solveHomogen, applications/cg_method.h:27-33,759-886).
+ * Host buffers of n doubles; x holds the initial guess on entry. */
+int lsg_cg_solve(lsg_operator *op, const double *f, double *x, const lsg_solver_opts *opts, lsg_solve_report *rep);
+/* Device-buffer variant (double arrays of n). */
+int lsg_cg_solve_device(lsg_operator *op, const double *f, double *x, const lsg_solver_opts *opts,
+                        lsg_solve_report *rep, void *stream);
+
+/* Installs a diagonal preconditioner (n doubles, host) used by precond = 2. */
+int lsg_set_learned_diag(lsg_operator *op, const double *diag);
+
+/* ---- host-only planner (no GPU needed): the flattened integer tables.
+ * lsg_plan_create builds the same tables lsg_operator_create uploads, so the
+ * tests can check them bit-exact against the reference's lookups on a CPU. */
+typedef struct lsg_plan lsg_plan;
+int lsg_plan_create(int32_t d, const int32_t *points, const uint8_t *active, int64_t n, lsg_plan **out);
+void lsg_plan_destroy(lsg_plan *plan);
+int lsg_plan_info(const lsg_plan *plan, lsg_info *info);
+/* DepthList order (iterator/depthIterator.h:14-50): n_depths*d */
+int lsg_plan_export_depths(const lsg_plan *plan, int32_t *depths);
+/* sortDepths(case c) (iterator/depthIterator.cpp:7-45) as depth ids; *count <= n_depths */
+int lsg_plan_export_sorted_depths(const lsg_plan *plan, int32_t c, int32_t *depth_ids, int32_t *count);
+/* cells of depth T+1 in the grid per depth (CellData, cells/CellStructure.h:23-61) */
+int lsg_plan_export_cell_counts(const lsg_plan *plan, int64_t *counts);
+/* corners (storage index or -1) of every cell of one depth, 2^d per cell,
+ * corner id bit k = right side in dim k; cells ordered by min corner */
+int lsg_plan_export_cells(const lsg_plan *plan, int32_t depth_id, int64_t *corners, int64_t *count);
+/* storage indices of the points with depth <= T (multilevel entries (I,T)) */
+int lsg_plan_export_slab(const lsg_plan *plan, int32_t depth_id, int64_t *storage_idx, int64_t *count);
+/* same-level neighbours nextLeft/nextRight (indices/index.h:749-789): n*d*2 storage indices or -1 */
+int lsg_plan_export_neighbors(const lsg_plan *plan, int64_t *nbr);
+/* prewavelet stencil of point k (nextFiveP, indices/index.cc:252-327) in
+ * MultiDimFiveCompass order: storage index (or -1 if absent) and weight; at most 5^d */
+int lsg_plan_export_stencil(const lsg_plan *plan, int64_t k, int64_t *idx, double *w, int32_t *count);
+
+/* Regular sparse grid AddRecursiveSonsOfPoint(center, level)
+ * (sgrid/sparseGrid.cc:557-566) in the reference's storage order; all points
+ * active.  Pass points = NULL to query *n. */
+int lsg_grid_regular(int32_t d, int32_t level, int32_t *points, int64_t capacity, int64_t *n);
+
+const char *lsg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

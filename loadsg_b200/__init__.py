@@ -1,0 +1,321 @@
+"""loadsg_b200 -- B200-native prewavelet matvec and CG for LoAdSG grids.
+
+Python mirror of the reference's interface for this path (LoAdSG,
+library/source/):
+
+  AdaptiveSparseGrid            sgrid/sparseGrid.h:86-387 (points in storage order)
+  MidpointDiffusion             the StencilTemplate::integration plugin
+                                (stencils/Stencil.h:740) with the coefficient
+                                sampled at cell midpoints
+  MatrixVectorHomogen           MatrixVectorMultiplication/MatrixVectorHomogen.h:32-652
+    .multiplication(x, Ax, p)   MatrixVectorHomogen.h:91-92
+  CG.solveHomogen(...)          applications/cg_method.h:27-33,759-886
+  Preconditioning.diagonal      applications/cg_method.h:81-754
+
+All compute runs in liblsg.so (hand-written sm_100a CUDA behind the C-ABI of
+include/lsg.h).  There is no CPU fallback: if the library is missing or no GPU
+is present, the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblsg.so")
+_LIB = None
+
+FP64, FP32 = 0, 1
+COEF_CONST, COEF_SINPROD, COEF_EXPSIN, COEF_LOGNORMAL, COEF_SIN2PI = range(5)
+
+
+class LsgError(RuntimeError):
+    pass
+
+
+class _Info(ctypes.Structure):
+    _fields_ = [
+        ("d", ctypes.c_int32),
+        ("n_points", ctypes.c_int64),
+        ("n_active", ctypes.c_int64),
+        ("n_depths", ctypes.c_int32),
+        ("n_slab_entries", ctypes.c_int64),
+        ("n_cells", ctypes.c_int64),
+        ("case_slab_entries", ctypes.c_int64),
+        ("case_cells", ctypes.c_int64),
+        ("device_bytes", ctypes.c_int64),
+        ("plan_seconds", ctypes.c_double),
+        ("matvec_bytes_fp64", ctypes.c_double),
+        ("matvec_flops", ctypes.c_double),
+    ]
+
+
+class SolverOpts(ctypes.Structure):
+    _fields_ = [
+        ("eps", ctypes.c_double),
+        ("criterion", ctypes.c_int32),
+        ("max_iter", ctypes.c_int32),
+        ("precond", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("inner_iter", ctypes.c_int32),
+        ("inner_tol", ctypes.c_double),
+        ("use_graph", ctypes.c_int32),
+    ]
+
+
+class SolveReport(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int32),
+        ("outer_iterations", ctypes.c_int32),
+        ("rel_residual", ctypes.c_double),
+        ("seconds", ctypes.c_double),
+        ("converged", ctypes.c_int32),
+        ("fell_back", ctypes.c_int32),
+    ]
+
+
+def lib():
+    """Loads liblsg.so (built in-tree by `python -m loadsg_b200.build`)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise LsgError(f"{LIB_PATH} is missing; build it with `python -m loadsg_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I32, I64, D = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+        sig = {
+            "lsg_operator_create": (ctypes.c_int, [I32, P, P, I64, P]),
+            "lsg_operator_destroy": (None, [P]),
+            "lsg_operator_info": (ctypes.c_int, [P, P]),
+            "lsg_operator_set_coefficient": (ctypes.c_int, [P, I32, P, I32]),
+            "lsg_matvec": (ctypes.c_int, [P, P, P]),
+            "lsg_matvec_device": (ctypes.c_int, [P, P, P, I32, P]),
+            "lsg_diag": (ctypes.c_int, [P, P]),
+            "lsg_diag_device": (ctypes.c_int, [P, P, P]),
+            "lsg_cg_solve": (ctypes.c_int, [P, P, P, P, P]),
+            "lsg_cg_solve_device": (ctypes.c_int, [P, P, P, P, P, P]),
+            "lsg_set_learned_diag": (ctypes.c_int, [P, P]),
+            "lsg_plan_create": (ctypes.c_int, [I32, P, P, I64, P]),
+            "lsg_plan_destroy": (None, [P]),
+            "lsg_plan_info": (ctypes.c_int, [P, P]),
+            "lsg_plan_export_depths": (ctypes.c_int, [P, P]),
+            "lsg_plan_export_sorted_depths": (ctypes.c_int, [P, I32, P, P]),
+            "lsg_plan_export_cell_counts": (ctypes.c_int, [P, P]),
+            "lsg_plan_export_cells": (ctypes.c_int, [P, I32, P, P]),
+            "lsg_plan_export_slab": (ctypes.c_int, [P, I32, P, P]),
+            "lsg_plan_export_neighbors": (ctypes.c_int, [P, P]),
+            "lsg_plan_export_stencil": (ctypes.c_int, [P, I64, P, P, P]),
+            "lsg_grid_regular": (ctypes.c_int, [I32, I32, P, I64, P]),
+            "lsg_last_error": (ctypes.c_char_p, []),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if isinstance(a, np.ndarray) else ctypes.c_void_p(a)
+
+
+def _check(rc):
+    if rc != 0:
+        raise LsgError(f"liblsg error {rc}: {lib().lsg_last_error().decode()}")
+
+
+# --------------------------------------------------------------------------- grids
+class AdaptiveSparseGrid:
+    """Grid points (1D indices, storage order) and active flags.
+
+    Mirrors the parts of the reference's AdaptiveSparseGrid this path reads:
+    getIndexOfTable(k) (sgrid/sparseGrid.h:566-572), getActiveTable() and
+    getMaximalOccupiedSecondTable()."""
+
+    def __init__(self, points, active=None):
+        self.points = np.ascontiguousarray(points, dtype=np.int32)
+        if self.points.ndim != 2:
+            raise ValueError("points must be N x d")
+        self.n, self.d = self.points.shape
+        if active is None:
+            active = np.ones(self.n, np.uint8)
+        self.active = np.ascontiguousarray(active, dtype=np.uint8)
+
+    @classmethod
+    def regular(cls, d, level):
+        """AddRecursiveSonsOfPoint(center, level) (sgrid/sparseGrid.cc:557-566)."""
+        n = ctypes.c_int64(0)
+        _check(lib().lsg_grid_regular(d, level, None, 0, ctypes.byref(n)))
+        pts = np.zeros((n.value, d), np.int32)
+        _check(lib().lsg_grid_regular(d, level, _ptr(pts), n.value, ctypes.byref(n)))
+        return cls(pts)
+
+    def getMaximalOccupiedSecondTable(self):
+        return self.n
+
+    def getDOFS(self):
+        return int(self.active.sum())
+
+    def coordinates(self):
+        """Coordinates of all points (IndexOneD::coordinate, indices/index.h:718-730)."""
+        idx = self.points.astype(np.int64)
+        t = np.floor(np.log2(idx)).astype(np.int64)
+        return (2 * (idx - (1 << t)) + 1) / (2.0 ** t)
+
+
+class MidpointDiffusion:
+    """-div(a grad u) with a sampled at cell midpoints: the local stiffness
+    entry of a cell is a(x_c) times the exact Q1 entry (the value a
+    StencilTemplate::integration plugin returns, stencils/Stencil.h:740)."""
+
+    def __init__(self, family, params):
+        self.family = int(family)
+        self.params = np.zeros(256, np.float64)
+        p = np.asarray(params, np.float64).ravel()
+        self.params[: len(p)] = p
+        self.nparams = len(p)
+
+
+class Plan:
+    """Host-only flattened tables (no GPU needed); for parity tests."""
+
+    def __init__(self, grid):
+        self.grid = grid
+        h = ctypes.c_void_p()
+        _check(lib().lsg_plan_create(grid.d, _ptr(grid.points), _ptr(grid.active), grid.n, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.lsg_plan_destroy(self._h)
+            self._h = None
+
+    def info(self):
+        i = _Info()
+        _check(lib().lsg_plan_info(self._h, ctypes.byref(i)))
+        return {k: getattr(i, k) for k, _ in _Info._fields_}
+
+    def depths(self):
+        nd = self.info()["n_depths"]
+        out = np.zeros((nd, self.grid.d), np.int32)
+        _check(lib().lsg_plan_export_depths(self._h, _ptr(out)))
+        return out
+
+    def sorted_depths(self, case):
+        nd = self.info()["n_depths"]
+        out = np.zeros(nd, np.int32)
+        cnt = ctypes.c_int32(0)
+        _check(lib().lsg_plan_export_sorted_depths(self._h, case, _ptr(out), ctypes.byref(cnt)))
+        return out[: cnt.value]
+
+    def cell_counts(self):
+        out = np.zeros(self.info()["n_depths"], np.int64)
+        _check(lib().lsg_plan_export_cell_counts(self._h, _ptr(out)))
+        return out
+
+    def cells(self, t):
+        cnt = ctypes.c_int64(0)
+        _check(lib().lsg_plan_export_cells(self._h, t, None, ctypes.byref(cnt)))
+        out = np.zeros((cnt.value, 1 << self.grid.d), np.int64)
+        _check(lib().lsg_plan_export_cells(self._h, t, _ptr(out), ctypes.byref(cnt)))
+        return out
+
+    def slab(self, t):
+        cnt = ctypes.c_int64(0)
+        _check(lib().lsg_plan_export_slab(self._h, t, None, ctypes.byref(cnt)))
+        out = np.zeros(cnt.value, np.int64)
+        _check(lib().lsg_plan_export_slab(self._h, t, _ptr(out), ctypes.byref(cnt)))
+        return out
+
+    def neighbors(self):
+        out = np.zeros((self.grid.n, self.grid.d, 2), np.int64)
+        _check(lib().lsg_plan_export_neighbors(self._h, _ptr(out)))
+        return out
+
+    def stencil(self, k):
+        m = 5 ** self.grid.d
+        idx = np.zeros(m, np.int64)
+        w = np.zeros(m, np.float64)
+        cnt = ctypes.c_int32(0)
+        _check(lib().lsg_plan_export_stencil(self._h, k, _ptr(idx), _ptr(w), ctypes.byref(cnt)))
+        return idx[: cnt.value], w[: cnt.value]
+
+
+# --------------------------------------------------------------------------- operator
+class MatrixVectorHomogen:
+    """Prewavelet stiffness operator on one grid, resident on the current GPU
+    (MatrixVectorHomogen(grid, mgrid, symmetry, mpi_on), MatrixVectorHomogen.h:72-77)."""
+
+    def __init__(self, grid, problem=None):
+        self.grid = grid
+        h = ctypes.c_void_p()
+        _check(lib().lsg_operator_create(grid.d, _ptr(grid.points), _ptr(grid.active), grid.n, ctypes.byref(h)))
+        self._h = h
+        self._problem = None
+        if problem is not None:
+            self.set_problem(problem)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.lsg_operator_destroy(self._h)
+            self._h = None
+
+    def set_problem(self, problem):
+        if problem is not self._problem:
+            _check(lib().lsg_operator_set_coefficient(self._h, problem.family, _ptr(problem.params), problem.nparams))
+            self._problem = problem
+
+    def info(self):
+        i = _Info()
+        _check(lib().lsg_operator_info(self._h, ctypes.byref(i)))
+        return {k: getattr(i, k) for k, _ in _Info._fields_}
+
+    def multiplication(self, prew, Ax, problem):
+        """Ax[active] = A_prew prew (host arrays of length N, storage order)."""
+        self.set_problem(problem)
+        x = np.ascontiguousarray(prew, np.float64)
+        if Ax.dtype != np.float64 or not Ax.flags.c_contiguous:
+            raise ValueError("Ax must be a contiguous float64 array")
+        _check(lib().lsg_matvec(self._h, _ptr(x), _ptr(Ax)))
+        return Ax
+
+    def multiplication_device(self, x_ptr, y_ptr, precision=FP64, stream=0):
+        """Device-pointer variant (torch tensors: pass t.data_ptr())."""
+        _check(lib().lsg_matvec_device(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), precision,
+                                       ctypes.c_void_p(stream)))
+
+    def diagonal(self, problem):
+        """Exact Jacobi diagonal (Preconditioning::precondLocalStiffnessMatrix)."""
+        self.set_problem(problem)
+        out = np.zeros(self.grid.n)
+        _check(lib().lsg_diag(self._h, _ptr(out)))
+        return out
+
+    def set_learned_diagonal(self, diag):
+        diag = np.ascontiguousarray(diag, np.float64)
+        _check(lib().lsg_set_learned_diag(self._h, _ptr(diag)))
+
+
+class CG:
+    @staticmethod
+    def solveHomogen(eps, x, f, matrix, problem, criterion=0, max_iter=500, precond=0, precision=FP64,
+                     inner_iter=30, inner_tol=1e-4, use_graph=True):
+        """CG::solveHomogen (applications/cg_method.h:759-886).  x (in/out) and f
+        are host float64 arrays.  criterion 0 is the reference's stopping rule on
+        r^T D^-1 r; criterion 1 stops at ||f - A x|| / ||f|| <= eps.  Returns the
+        report (iterations, rel_residual, seconds, ...)."""
+        matrix.set_problem(problem)
+        o = SolverOpts(eps, criterion, max_iter, precond, precision, inner_iter, inner_tol, int(use_graph))
+        rep = SolveReport()
+        if x.dtype != np.float64 or not x.flags.c_contiguous:
+            raise ValueError("x must be a contiguous float64 array")
+        f = np.ascontiguousarray(f, np.float64)
+        _check(lib().lsg_cg_solve(matrix._h, _ptr(f), _ptr(x), ctypes.byref(o), ctypes.byref(rep)))
+        return {k: getattr(rep, k) for k, _ in SolveReport._fields_}
+
+    @staticmethod
+    def solve_device(matrix, f_ptr, x_ptr, opts, stream=0):
+        rep = SolveReport()
+        _check(lib().lsg_cg_solve_device(matrix._h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(x_ptr),
+                                         ctypes.byref(opts), ctypes.byref(rep), ctypes.c_void_p(stream)))
+        return {k: getattr(rep, k) for k, _ in SolveReport._fields_}

@@ -1,0 +1,1389 @@
+// B200 (sm_100a) prewavelet matvec, Jacobi diagonal and CG behind the C-ABI of
+// include/lsg.h.  The host planner (lsg_plan.cpp) produces integer tables and a
+// static level schedule; this file uploads them and runs:
+//   k_nodal      prewavelet -> nodal values per depth (calcNodal,
+//                MatrixVectorHomogen.cpp:43-74), sum-factorised 3-tap stages
+//   k_pinit      P_c(T) = nodal(T)            ("P += nodal", MVH.h:1649)
+//   k_prolong    one prolongation level       (MVH.h:1655-1670, 444-474)
+//   k_phaseB     one restriction wavefront: per (case, depth) item the level-T
+//                cell operator (LocalStiffnessMatrices.cpp:555-582) applied in
+//                the Walsh-Hadamard basis where the Q1 element is diagonal,
+//                + gM bookkeeping + restrictions (MVH.h:1672-1735, 485-530)
+//                + ConvertToPrewavelet2 (MVH.h:540-562), sum-factorised 5-tap
+//   k_diag       exact Jacobi diagonal (cg_method.h:544-680)
+//   CG kernels   CG::solveHomogen vector semantics (cg_method.h:759-886)
+#include "lsg_plan.h"
+#include "lsg_coef.cuh"
+#include "../../include/lsg.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                       \
+    do {                                                                                     \
+        cudaError_t _e = (expr);                                                             \
+        if (_e != cudaSuccess)                                                               \
+            return fail(LSG_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));     \
+    } while (0)
+
+// ----------------------------------------------------------------------------- device tables
+struct DevSlab {
+    int64_t off, n, cell_off, ncell, corner_off;
+    int32_t dense, pad;
+    int32_t T[lsg::kMaxDim];
+    int32_t ext[lsg::kMaxDim];     // 2^T_k - 1 (interior points per dim)
+    int32_t stride[lsg::kMaxDim];  // slab-position stride of dim k (dense slabs)
+};
+
+struct DevPlan {
+    int d, nD;
+    int64_t n;
+    const DevSlab* slabs;
+    const int32_t* did;
+    const uint8_t* act;
+    const int64_t* exa_off;
+    const int64_t* exa;
+    const uint64_t* cell_key;   // sparse cells
+    const int32_t* cell_corner;
+    const int64_t* nodal_stage;  // nD*d+1
+    const int32_t* nodal_src;
+    const int32_t* nodal_code;
+    const int64_t* nodal_dom;    // nD*(d+1)
+    const int64_t* nodal_scr;    // per depth scratch offset
+    const int64_t* conv_stage;
+    const int32_t* conv_src;
+    const int32_t* conv_code;
+    const int64_t* conv_dom;
+    const int32_t* prol;
+    const int32_t* restr;
+    const lsg::PhaseAItem* a_items;
+    const lsg::PhaseBItem* b_items;
+    const lsg::PhaseBStep* b_steps;
+    const int32_t* pts;
+};
+
+template <typename V>
+__device__ __forceinline__ V wcode(int c) {
+    // 0: none, 1: 1.0, 2: 0.9, 3: -0.6, 4: 0.1 (nextFiveP weights, indices/index.cc:252-327)
+    switch (c) {
+    case 1: return V(1.0);
+    case 2: return V(0.9);
+    case 3: return V(-0.6);
+    case 4: return V(0.1);
+    default: return V(0.0);
+    }
+}
+
+// one sum-factorised stencil stage: out[e] = sum_s w_s in[src_s]
+template <int NS, typename V, typename VI>
+__device__ __forceinline__ void stage_gather(const int32_t* __restrict__ src, const int32_t* __restrict__ code,
+                                             int64_t nout, const VI* __restrict__ in, const int64_t* __restrict__ in_map,
+                                             V* __restrict__ out) {
+    for (int64_t e = threadIdx.x; e < nout; e += blockDim.x) {
+        int cd = code[e];
+        V acc = V(0);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            int32_t i = src[e * NS + s];
+            if (i < 0) break;
+            V v = in_map ? V(in[in_map[i]]) : V(in[i]);
+            acc += wcode<V>((cd >> (3 * s)) & 7) * v;
+        }
+        out[e] = acc;
+    }
+}
+
+// ----------------------------------------------------------------------------- nodal
+template <typename V>
+__global__ void k_nodal(DevPlan P, const V* __restrict__ x, V* __restrict__ ml, V* __restrict__ scratch) {
+    int t = blockIdx.x;
+    int d = P.d;
+    const DevSlab& s = P.slabs[t];
+    V* scr = scratch + P.nodal_scr[t];
+    const int64_t* dom = P.nodal_dom + t * (d + 1);
+    // stage buffers for domains 1..d-1 are consecutive in scr
+    int64_t off_in = 0, off_out = 0;
+    for (int j = 0; j < d; ++j) {
+        int64_t so = P.nodal_stage[t * d + j];
+        int64_t nout = dom[j + 1];
+        V* out = (j == d - 1) ? ml + s.off : scr + off_out;
+        if (j == 0) stage_gather<3, V, V>(P.nodal_src + so * 3, P.nodal_code + so, nout, x, P.exa + P.exa_off[t], out);
+        else stage_gather<3, V, V>(P.nodal_src + so * 3, P.nodal_code + so, nout, scr + off_in, nullptr, out);
+        off_in = off_out;
+        off_out += (j == d - 1) ? 0 : nout;
+        __syncthreads();
+    }
+}
+
+// ----------------------------------------------------------------------------- P init, prolongation
+template <typename V>
+__global__ void k_pinit(DevPlan P, const V* __restrict__ ml, V* __restrict__ pc, int32_t item0) {
+    const lsg::PhaseBItem it = P.b_items[item0 + blockIdx.x];
+    const DevSlab& s = P.slabs[it.t];
+    for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) pc[it.p_off + e] = ml[s.off + e];
+}
+
+template <typename V>
+__global__ void k_prolong(DevPlan P, V* __restrict__ pc, int32_t item0) {
+    const lsg::PhaseAItem it = P.a_items[item0 + blockIdx.x];
+    const int32_t* tab = P.prol + it.tab_off;
+    const V* src = pc + it.src_off;
+    V* dst = pc + it.dst_off;
+    for (int64_t e = threadIdx.x; e < it.n_dst; e += blockDim.x) {
+        int32_t a = tab[2 * e], b = tab[2 * e + 1];
+        V add;
+        if (b == -2) add = src[a];
+        else add = V(0.5) * ((b >= 0 ? src[b] : V(0)) + (a >= 0 ? src[a] : V(0)));
+        dst[e] = dst[e] + add;
+    }
+}
+
+// ----------------------------------------------------------------------------- cell operator
+// Corner positions of one level-T cell (bit k of the corner id = right side in dim k).
+template <int D>
+__device__ __forceinline__ void cell_corners(const DevPlan& P, const DevSlab& s, int64_t ci, int32_t* pos) {
+    constexpr int NC = 1 << D;
+    if (!s.dense) {
+        const int32_t* c = P.cell_corner + ((s.corner_off + ci) << D);
+#pragma unroll
+        for (int b = 0; b < NC; ++b) pos[b] = c[b];
+        return;
+    }
+    const int32_t BAD = -(1 << 27);
+    pos[0] = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        int32_t cext = s.ext[k] + 1;
+        int32_t m = (int32_t)(ci % cext);
+        ci /= cext;
+        int32_t lo = (m >= 1) ? (m - 1) * s.stride[k] : BAD;
+        int32_t hi = (m + 1 <= s.ext[k]) ? m * s.stride[k] : BAD;
+#pragma unroll
+        for (int b = 0; b < (1 << k); ++b) {
+            pos[b | (1 << k)] = pos[b] + hi;
+            pos[b] = pos[b] + lo;
+        }
+    }
+}
+
+// z += a_c K_ref u on the corners of one cell.  K_ref = H diag(lam) H with H the
+// d-fold Hadamard transform: the exact Q1 stiffness sum_i K1_i (x) M1_others is
+// diagonal in the basis (1,1),(1,-1) of every dimension.
+template <int D, typename V, bool SHARED_ATOMIC>
+__device__ __forceinline__ void apply_cell(const int32_t* pos, const V* __restrict__ u, V* z, V a, const V* lam) {
+    constexpr int NC = 1 << D;
+    V v[NC];
+#pragma unroll
+    for (int b = 0; b < NC; ++b) v[b] = pos[b] >= 0 ? u[pos[b]] : V(0);
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+#pragma unroll
+        for (int b = 0; b < NC; ++b)
+            if (!(b & (1 << k))) {
+                V p = v[b], q = v[b | (1 << k)];
+                v[b] = p + q;
+                v[b | (1 << k)] = p - q;
+            }
+#pragma unroll
+    for (int b = 0; b < NC; ++b) v[b] *= a * lam[b];
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+#pragma unroll
+        for (int b = 0; b < NC; ++b)
+            if (!(b & (1 << k))) {
+                V p = v[b], q = v[b | (1 << k)];
+                v[b] = p + q;
+                v[b | (1 << k)] = p - q;
+            }
+#pragma unroll
+    for (int b = 0; b < NC; ++b)
+        if (pos[b] >= 0) atomicAdd(&z[pos[b]], v[b]);
+}
+
+// ----------------------------------------------------------------------------- phase B item
+template <int D, typename V>
+__global__ void __launch_bounds__(256) k_phaseB(DevPlan P, const V* __restrict__ pc, V* __restrict__ gm,
+                                                 V* __restrict__ scratch, V* __restrict__ y,
+                                                 const V* __restrict__ acell, const V* __restrict__ lam_all,
+                                                 int32_t item0, int64_t smem_cap) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NC = 1 << D;
+    const lsg::PhaseBItem it = P.b_items[item0 + blockIdx.x];
+    const DevSlab& s = P.slabs[it.t];
+    V* lam = reinterpret_cast<V*>(smem_raw);
+    for (int b = threadIdx.x; b < NC; b += blockDim.x) lam[b] = lam_all[(int64_t)it.t * NC + b];
+    V* scr = scratch + it.scratch_off;
+    const V* u_g = pc + it.p_off;
+    const V* ac = acell + s.cell_off;
+    bool in_smem = (int64_t)(2 * s.n) <= smem_cap;
+    if (in_smem) {
+        V* u = lam + NC;
+        V* z = u + s.n;
+        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) {
+            u[e] = u_g[e];
+            z[e] = V(0);
+        }
+        __syncthreads();
+        int32_t pos[NC];
+        for (int64_t ci = threadIdx.x; ci < s.ncell; ci += blockDim.x) {
+            cell_corners<D>(P, s, ci, pos);
+            apply_cell<D, V, true>(pos, u, z, ac[ci], lam);
+        }
+        __syncthreads();
+        const V* g0 = gm + it.gm_off;
+        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) scr[e] = it.gm_prev ? z[e] + g0[e] : z[e];
+    } else {
+        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) scr[e] = V(0);
+        __syncthreads();
+        int32_t pos[NC];
+        for (int64_t ci = threadIdx.x; ci < s.ncell; ci += blockDim.x) {
+            cell_corners<D>(P, s, ci, pos);
+            apply_cell<D, V, false>(pos, u_g, scr, ac[ci], lam);
+        }
+        __syncthreads();
+        if (it.gm_prev) {
+            const V* g0 = gm + it.gm_off;
+            for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) scr[e] += g0[e];
+        }
+    }
+    __syncthreads();
+    // restriction steps with gM swap-add
+    V* cur = scr;
+    int64_t used = s.n;
+    for (int32_t si = it.step_begin; si < it.step_end; ++si) {
+        const lsg::PhaseBStep st = P.b_steps[si];
+        const int32_t* tab = P.restr + st.tab_off;
+        V* nxt = scr + used;
+        V* g = gm + st.gm_off;
+        for (int64_t q = threadIdx.x; q < st.n_dst; q += blockDim.x) {
+            int32_t a = tab[3 * q], l = tab[3 * q + 1], r = tab[3 * q + 2];
+            V v = cur[a];
+            if (l >= 0) v = v + V(0.5) * cur[l];
+            if (r >= 0) v = v + V(0.5) * cur[r];
+            V tmp = st.gm_prev ? g[q] : V(0);
+            g[q] = v;
+            nxt[q] = v + tmp;
+        }
+        __syncthreads();
+        cur = nxt;
+        used += st.n_dst;
+    }
+    // convert to prewavelets at Tc
+    if (it.t_conv >= 0) {
+        int tc = it.t_conv;
+        const int64_t* dom = P.conv_dom + tc * (D + 1);
+        const V* in = cur;
+        V* buf = scr + used;
+        for (int j = 0; j < D; ++j) {
+            int64_t so = P.conv_stage[tc * D + j];
+            int64_t nout = dom[j + 1];
+            if (j == D - 1) {
+                const int32_t* src = P.conv_src + so * 5;
+                const int32_t* code = P.conv_code + so;
+                const int64_t* outmap = P.exa + P.exa_off[tc];
+                for (int64_t e = threadIdx.x; e < nout; e += blockDim.x) {
+                    int cd = code[e];
+                    V acc = V(0);
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) {
+                        int32_t i = src[e * 5 + q];
+                        if (i < 0) break;
+                        acc += wcode<V>((cd >> (3 * q)) & 7) * in[i];
+                    }
+                    atomicAdd(&y[outmap[e]], acc);
+                }
+            } else {
+                stage_gather<5, V, V>(P.conv_src + so * 5, P.conv_code + so, nout, in, nullptr, buf);
+                __syncthreads();
+                in = buf;
+                buf += nout;
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------- coefficient, diag
+template <typename V>
+__global__ void k_cell_coef(DevPlan P, int64_t C, int family, const double* __restrict__ params,
+                            double* __restrict__ a64, float* __restrict__ a32, const int64_t* __restrict__ cell_slab_off) {
+    int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (gi >= C) return;
+    // slab of this cell (cell_slab_off is the prefix of cell counts)
+    int lo = 0, hi = P.nD;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) / 2;
+        if (cell_slab_off[mid] <= gi) lo = mid;
+        else hi = mid;
+    }
+    const DevSlab& s = P.slabs[lo];
+    int64_t ci = gi - s.cell_off;
+    uint64_t key = s.dense ? (uint64_t)ci : P.cell_key[s.corner_off + ci];
+    double x[lsg::kMaxDim];
+    for (int k = 0; k < P.d; ++k) {
+        uint64_t cext = (uint64_t)s.ext[k] + 1;
+        int64_t m = (int64_t)(key % cext);
+        key /= cext;
+        double lo_c = ldexp((double)m, -s.T[k]);
+        double hi_c = ldexp((double)(m + 1), -s.T[k]);
+        x[k] = 0.5 * (lo_c + hi_c);
+    }
+    double a = lsg_coef_eval_dev(family, params, P.d, x);
+    a64[gi] = a;
+    a32[gi] = (float)a;
+}
+
+// diag_i = v^T A_T v for v = psi_i on level T = Depth(i): sum over the level-T
+// cells inside the grid that touch the support of psi_i of
+// a_c * sum_k qK_k prod_{j!=k} qM_j (v is a tensor product on every such cell).
+template <int D>
+__global__ void k_diag(DevPlan P, const double* __restrict__ acell, double* __restrict__ diag) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= P.n) return;
+    if (!P.act[k]) { diag[k] = 0.0; return; }
+    const DevSlab& s = P.slabs[P.did[k]];
+    // 1D weights at the 6 candidate cells of each dim: cell m in {c-3..c+2}
+    double wl[D][6], wr[D][6], h[D];
+    int64_t mm[D][6];
+    int nm[D];
+    for (int j = 0; j < D; ++j) {
+        int32_t idx = P.pts[k * D + j];
+        int t = s.T[j];
+        int64_t c = 2 * (int64_t)(idx - (1 << t)) + 1;
+        int64_t top = (int64_t)1 << t;
+        h[j] = ldexp(1.0, -t);
+        bool lok = c - 1 > 0, rok = c + 1 < top;
+        double w[7];  // weights at c-3..c+3
+        for (int q = 0; q < 7; ++q) w[q] = 0.0;
+        w[3] = (t > 1 && (!lok || !rok)) ? 0.9 : 1.0;
+        if (lok) { w[2] = -0.6; w[1] = 0.1; }
+        if (rok) { w[4] = -0.6; w[5] = 0.1; }
+        nm[j] = 0;
+        for (int q = 0; q < 6; ++q) {
+            int64_t m = c - 3 + q;
+            if (m < 0 || m >= top) continue;
+            if (w[q] == 0.0 && w[q + 1] == 0.0) continue;
+            mm[j][nm[j]] = m;
+            wl[j][nm[j]] = w[q];
+            wr[j][nm[j]] = w[q + 1];
+            nm[j]++;
+        }
+    }
+    double acc = 0.0;
+    int ctr[D];
+    for (int j = 0; j < D; ++j) ctr[j] = 0;
+    for (;;) {
+        uint64_t key = 0, cs = 1;
+        for (int j = 0; j < D; ++j) {
+            key += (uint64_t)mm[j][ctr[j]] * cs;
+            cs *= (uint64_t)s.ext[j] + 1;
+        }
+        int64_t ci = -1;
+        if (s.dense) ci = (int64_t)key;
+        else {
+            const uint64_t* ks = P.cell_key + s.corner_off;
+            int64_t lo = 0, hi = s.ncell;
+            while (lo < hi) {
+                int64_t mid = (lo + hi) / 2;
+                if (ks[mid] < key) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo < s.ncell && ks[lo] == key) ci = lo;
+        }
+        if (ci >= 0) {
+            double qK[D], qM[D];
+            for (int j = 0; j < D; ++j) {
+                double a = wl[j][ctr[j]], b = wr[j][ctr[j]];
+                qK[j] = (a - b) * (a - b) / h[j];
+                qM[j] = h[j] * (a * a + a * b + b * b) / 3.0;
+            }
+            double sum = 0.0;
+            for (int i = 0; i < D; ++i) {
+                double prod = qK[i];
+                for (int j = 0; j < D; ++j)
+                    if (j != i) prod *= qM[j];
+                sum += prod;
+            }
+            acc += acell[s.cell_off + ci] * sum;
+        }
+        int j = 0;
+        while (j < D && ++ctr[j] == nm[j]) { ctr[j] = 0; ++j; }
+        if (j == D) break;
+    }
+    diag[k] = acc;
+}
+
+// ----------------------------------------------------------------------------- vector kernels
+template <typename V>
+__global__ void k_zero_active(const int64_t* __restrict__ exa, int64_t na, V* __restrict__ y) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e < na) y[exa[e]] = V(0);
+}
+
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    if (w == 0)
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    return v;
+}
+
+// partial dot products (FP64 accumulation), deterministic two-pass
+template <typename A, typename B>
+__global__ void k_dot_partial(const A* __restrict__ a, const B* __restrict__ b, int64_t n, double* __restrict__ part) {
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += (double)a[i] * (double)b[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+__global__ void k_dot_final(const double* __restrict__ part, int np, double* __restrict__ out) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) acc += part[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) *out = acc;
+}
+
+// scalars: s[0]=delta s[1]=dg s[2]=tau s[3]=delta_new s[4]=beta s[5]=rr s[6]=ff
+__global__ void k_tau(double* s) { s[2] = s[0] / s[1]; }
+__global__ void k_beta(double* s) { s[4] = s[3] / s[0]; s[0] = s[3]; }
+
+// r += tau g ; x -= tau d   (all entries, ET semantics of cg_method.h:862-863)
+template <typename V>
+__global__ void k_update_rx(int64_t n, const double* s, V* r, V* x, const V* g, const V* d) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    V tau = (V)s[2];
+    r[i] = r[i] + tau * g[i];
+    x[i] = x[i] - tau * d[i];
+}
+// h = r (all) ; h /= z on active entries (apply_inverse, cg_method.h:717-727)
+template <typename V>
+__global__ void k_precond(int64_t n, const uint8_t* act, const V* r, const V* z, V* h, int all) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (act[i]) h[i] = z ? r[i] / z[i] : r[i];
+    else if (all) h[i] = r[i];
+}
+// d = -h + beta d
+template <typename V>
+__global__ void k_update_d(int64_t n, const double* s, const V* h, V* d) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d[i] = V(-1.0) * h[i] + (V)s[4] * d[i];
+}
+template <typename V>
+__global__ void k_sub(int64_t n, const V* f, V* r) {  // r = f - r
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) r[i] = f[i] - r[i];
+}
+template <typename V>
+__global__ void k_neg(int64_t n, const V* h, V* d) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) d[i] = V(-1.0) * h[i];
+}
+__global__ void k_scale_to_f32(int64_t n, const double* a, double scale, float* b) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)(a[i] * scale);
+}
+__global__ void k_axpy_f32(int64_t n, double alpha, const float* e, double* x) {  // x += alpha * e
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) x[i] += alpha * (double)e[i];
+}
+__global__ void k_to_f32(int64_t n, const double* a, float* b) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+
+inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+// ----------------------------------------------------------------------------- device buffer helper
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DBuf() { if (p) cudaFree(p); }
+    int alloc(size_t b, size_t* total) {
+        if (p) { cudaFree(p); p = nullptr; }
+        bytes = b;
+        if (b == 0) return 0;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) return fail(LSG_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        *total += b;
+        return 0;
+    }
+    template <typename T>
+    int upload(const std::vector<T>& v, size_t* total) {
+        int rc = alloc(v.size() * sizeof(T), total);
+        if (rc) return rc;
+        if (!v.empty()) {
+            cudaError_t e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return fail(LSG_E_CUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+        }
+        return 0;
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+struct lsg_operator {
+    lsg::Plan plan;
+    DevPlan dp{};
+    int device = 0;
+    size_t dev_bytes = 0;
+    // tables
+    DBuf slabs, did, act, exa_off, exa, cell_key, cell_corner, nodal_stage, nodal_src, nodal_code, nodal_dom, nodal_scr,
+        conv_stage, conv_src, conv_code, conv_dom, prol, restr, a_items, b_items, b_steps, pts, cell_slab_off;
+    DBuf lam64, lam32;
+    // coefficient
+    bool have_coef = false;
+    DBuf acell64, acell32, params;
+    // work buffers per precision
+    struct Work {
+        DBuf ml, pc, gm, scratch, nscratch;
+    } w64, w32;
+    DBuf xbuf64, ybuf64;  // host-call staging
+    DBuf diag;            // Jacobi diagonal (FP64)
+    bool have_diag = false;
+    DBuf learned;
+    bool have_learned = false;
+    int64_t smem_cap64 = 0, smem_cap32 = 0;
+    std::vector<int64_t> level_maxn;  // per phase-B level: max N_T
+};
+
+namespace {
+
+int upload_plan(lsg_operator* op) {
+    const lsg::Plan& p = op->plan;
+    size_t* tot = &op->dev_bytes;
+    int d = p.d;
+    std::vector<DevSlab> ds(p.nD);
+    for (int t = 0; t < p.nD; ++t) {
+        const lsg::Slab& s = p.slabs[t];
+        DevSlab& o = ds[t];
+        memset(&o, 0, sizeof o);
+        o.off = s.off;
+        o.n = s.n;
+        o.cell_off = s.cell_off;
+        o.ncell = s.ncell;
+        o.corner_off = s.corner_off;
+        o.dense = s.dense ? 1 : 0;
+        int64_t stride = 1;
+        for (int k = 0; k < d; ++k) {
+            o.T[k] = s.T[k];
+            o.ext[k] = (1 << s.T[k]) - 1;
+            o.stride[k] = (int32_t)stride;
+            stride *= o.ext[k];
+        }
+    }
+    std::vector<int64_t> nscr(p.nD);
+    int64_t acc = 0;
+    for (int t = 0; t < p.nD; ++t) {
+        nscr[t] = acc;
+        for (int j = 1; j < d; ++j) acc += p.nodal_dom[t * (d + 1) + j];
+    }
+    std::vector<int64_t> cso(p.nD + 1);
+    for (int t = 0; t < p.nD; ++t) cso[t] = p.slabs[t].cell_off;
+    cso[p.nD] = p.C;
+    int rc = 0;
+    rc |= op->slabs.upload(ds, tot);
+    rc |= op->did.upload(p.did, tot);
+    rc |= op->act.upload(p.act, tot);
+    rc |= op->exa_off.upload(p.exa_off, tot);
+    rc |= op->exa.upload(p.exa, tot);
+    rc |= op->cell_key.upload(p.cell_key, tot);
+    rc |= op->cell_corner.upload(p.cell_corner, tot);
+    rc |= op->nodal_stage.upload(p.nodal.stage_off, tot);
+    rc |= op->nodal_src.upload(p.nodal.src, tot);
+    rc |= op->nodal_code.upload(p.nodal.code, tot);
+    rc |= op->nodal_dom.upload(p.nodal_dom, tot);
+    rc |= op->nodal_scr.upload(nscr, tot);
+    rc |= op->conv_stage.upload(p.convert.stage_off, tot);
+    rc |= op->conv_src.upload(p.convert.src, tot);
+    rc |= op->conv_code.upload(p.convert.code, tot);
+    rc |= op->conv_dom.upload(p.convert_dom, tot);
+    rc |= op->prol.upload(p.prol, tot);
+    rc |= op->restr.upload(p.restr, tot);
+    rc |= op->a_items.upload(p.a_items, tot);
+    rc |= op->b_items.upload(p.b_items, tot);
+    rc |= op->b_steps.upload(p.b_steps, tot);
+    rc |= op->pts.upload(p.pts, tot);
+    rc |= op->cell_slab_off.upload(cso, tot);
+    if (rc) return LSG_E_CUDA;
+    // Hadamard-basis eigenvalues of the Q1 element per depth, 1/2^d folded in
+    int nc = 1 << d;
+    std::vector<double> lam(p.nD * (size_t)nc);
+    std::vector<float> lamf(lam.size());
+    for (int t = 0; t < p.nD; ++t) {
+        double h[lsg::kMaxDim];
+        for (int k = 0; k < d; ++k) h[k] = std::ldexp(1.0, -p.slabs[t].T[k]);
+        for (int sgn = 0; sgn < nc; ++sgn) {
+            double l = 0.0;
+            for (int i = 0; i < d; ++i) {
+                if (!((sgn >> i) & 1)) continue;
+                double prod = 2.0 / h[i];
+                for (int j = 0; j < d; ++j)
+                    if (j != i) prod *= ((sgn >> j) & 1) ? h[j] / 6.0 : h[j] / 2.0;
+                l += prod;
+            }
+            lam[(size_t)t * nc + sgn] = l / nc;
+            lamf[(size_t)t * nc + sgn] = (float)(l / nc);
+        }
+    }
+    rc |= op->lam64.upload(lam, tot);
+    rc |= op->lam32.upload(lamf, tot);
+    if (rc) return LSG_E_CUDA;
+    DevPlan& P = op->dp;
+    P.d = d;
+    P.nD = p.nD;
+    P.n = p.n;
+    P.slabs = op->slabs.as<DevSlab>();
+    P.did = op->did.as<int32_t>();
+    P.act = op->act.as<uint8_t>();
+    P.exa_off = op->exa_off.as<int64_t>();
+    P.exa = op->exa.as<int64_t>();
+    P.cell_key = op->cell_key.as<uint64_t>();
+    P.cell_corner = op->cell_corner.as<int32_t>();
+    P.nodal_stage = op->nodal_stage.as<int64_t>();
+    P.nodal_src = op->nodal_src.as<int32_t>();
+    P.nodal_code = op->nodal_code.as<int32_t>();
+    P.nodal_dom = op->nodal_dom.as<int64_t>();
+    P.nodal_scr = op->nodal_scr.as<int64_t>();
+    P.conv_stage = op->conv_stage.as<int64_t>();
+    P.conv_src = op->conv_src.as<int32_t>();
+    P.conv_code = op->conv_code.as<int32_t>();
+    P.conv_dom = op->conv_dom.as<int64_t>();
+    P.prol = op->prol.as<int32_t>();
+    P.restr = op->restr.as<int32_t>();
+    P.a_items = op->a_items.as<lsg::PhaseAItem>();
+    P.b_items = op->b_items.as<lsg::PhaseBItem>();
+    P.b_steps = op->b_steps.as<lsg::PhaseBStep>();
+    P.pts = op->pts.as<int32_t>();
+    // per-level max slab size (dynamic shared memory of k_phaseB)
+    op->level_maxn.clear();
+    for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
+        int64_t mx = 0;
+        for (int32_t i = p.b_level_off[L]; i < p.b_level_off[L + 1]; ++i) mx = std::max(mx, p.slabs[p.b_items[i].t].n);
+        op->level_maxn.push_back(mx);
+    }
+    return 0;
+}
+
+template <typename V>
+int ensure_work(lsg_operator* op, lsg_operator::Work& w) {
+    if (w.ml.p) return 0;
+    const lsg::Plan& p = op->plan;
+    size_t* tot = &op->dev_bytes;
+    int rc = 0;
+    rc |= w.ml.alloc(p.M * sizeof(V), tot);
+    rc |= w.pc.alloc(p.p_total * sizeof(V), tot);
+    rc |= w.gm.alloc(p.gm_total * sizeof(V), tot);
+    rc |= w.scratch.alloc(std::max<int64_t>(p.scratch_total, 1) * sizeof(V), tot);
+    rc |= w.nscratch.alloc(std::max<int64_t>(p.nodal_scratch, 1) * sizeof(V), tot);
+    return rc ? LSG_E_CUDA : 0;
+}
+
+template <int D, typename V>
+int set_phaseB_smem() {
+    static bool done = false;
+    if (done) return 0;
+    CUDA_TRY(cudaFuncSetAttribute(k_phaseB<D, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    done = true;
+    return 0;
+}
+
+// The matvec: a fixed sequence of launches on one stream.
+template <int D, typename V>
+int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st) {
+    const lsg::Plan& p = op->plan;
+    lsg_operator::Work& w = std::is_same<V, double>::value ? op->w64 : op->w32;
+    int rc = ensure_work<V>(op, w);
+    if (rc) return rc;
+    rc = set_phaseB_smem<D, V>();
+    if (rc) return rc;
+    const V* acell = std::is_same<V, double>::value ? (const V*)op->acell64.p : (const V*)op->acell32.p;
+    const V* lam = std::is_same<V, double>::value ? (const V*)op->lam64.p : (const V*)op->lam32.p;
+    int64_t na = p.exa_off[p.nD];
+    if (na > 0) k_zero_active<V><<<nblk(na), 256, 0, st>>>(op->dp.exa, na, y);
+    k_nodal<V><<<p.nD, 256, 0, st>>>(op->dp, x, w.ml.as<V>(), w.nscratch.as<V>());
+    int32_t nb = (int32_t)p.b_items.size();
+    if (nb > 0) k_pinit<V><<<nb, 256, 0, st>>>(op->dp, w.ml.as<V>(), w.pc.as<V>(), 0);
+    for (size_t L = 0; L + 1 < p.a_level_off.size(); ++L) {
+        int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
+        if (e > b) k_prolong<V><<<e - b, 256, 0, st>>>(op->dp, w.pc.as<V>(), b);
+    }
+    const int64_t cap_elems = (200 * 1024) / sizeof(V) - (1 << D);
+    for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
+        int32_t b = p.b_level_off[L], e = p.b_level_off[L + 1];
+        if (e <= b) continue;
+        int64_t mx = op->level_maxn[L];
+        int64_t alloc_elems = 2 * mx <= cap_elems ? 2 * mx : 0;  // u and z of the largest slab
+        size_t smem = (size_t)((1 << D) + alloc_elems) * sizeof(V);
+        k_phaseB<D, V><<<e - b, 256, smem, st>>>(op->dp, w.pc.as<V>(), w.gm.as<V>(), w.scratch.as<V>(), y, acell, lam, b,
+                                                 alloc_elems);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <typename V>
+int matvec_dispatch(lsg_operator* op, const V* x, V* y, cudaStream_t st) {
+    switch (op->plan.d) {
+    case 1: return matvec_impl<1, V>(op, x, y, st);
+    case 2: return matvec_impl<2, V>(op, x, y, st);
+    case 3: return matvec_impl<3, V>(op, x, y, st);
+    case 4: return matvec_impl<4, V>(op, x, y, st);
+    case 5: return matvec_impl<5, V>(op, x, y, st);
+    case 6: return matvec_impl<6, V>(op, x, y, st);
+    case 7: return matvec_impl<7, V>(op, x, y, st);
+    case 8: return matvec_impl<8, V>(op, x, y, st);
+    }
+    return fail(LSG_E_INVALID, "unsupported dimension");
+}
+
+int compute_diag(lsg_operator* op, cudaStream_t st) {
+    if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
+    if (!op->diag.p) {
+        int rc = op->diag.alloc(op->plan.n * sizeof(double), &op->dev_bytes);
+        if (rc) return rc;
+    }
+    unsigned g = nblk(op->plan.n, 128);
+    const double* a = op->acell64.as<double>();
+    double* dg = op->diag.as<double>();
+    switch (op->plan.d) {
+    case 1: k_diag<1><<<g, 128, 0, st>>>(op->dp, a, dg); break;
+    case 2: k_diag<2><<<g, 128, 0, st>>>(op->dp, a, dg); break;
+    case 3: k_diag<3><<<g, 128, 0, st>>>(op->dp, a, dg); break;
+    case 4: k_diag<4><<<g, 128, 0, st>>>(op->dp, a, dg); break;
+    case 5: k_diag<5><<<g, 128, 0, st>>>(op->dp, a, dg); break;
+    case 6: k_diag<6><<<g, 128, 0, st>>>(op->dp, a, dg); break;
+    case 7: k_diag<7><<<g, 128, 0, st>>>(op->dp, a, dg); break;
+    case 8: k_diag<8><<<g, 128, 0, st>>>(op->dp, a, dg); break;
+    }
+    CUDA_TRY(cudaGetLastError());
+    op->have_diag = true;
+    return 0;
+}
+
+}  // namespace
+
+// forward helpers used by the CG section
+static int lsg_internal_matvec64(lsg_operator* op, const double* x, double* y, cudaStream_t st);
+static int lsg_internal_matvec32(lsg_operator* op, const float* x, float* y, cudaStream_t st);
+static const uint8_t* lsg_internal_active(lsg_operator* op);
+
+// ============================================================================= C-ABI
+extern "C" {
+
+const char* lsg_last_error(void) { return g_err.c_str(); }
+
+int lsg_operator_create(int32_t d, const int32_t* points, const uint8_t* active, int64_t n, lsg_operator** out) {
+    if (!out || !points || !active) return fail(LSG_E_INVALID, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(LSG_E_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    std::unique_ptr<lsg_operator> op(new lsg_operator());
+    if (!lsg::build_plan(d, n, points, active, op->plan)) return fail(LSG_E_INVALID, op->plan.error);
+    CUDA_TRY(cudaGetDevice(&op->device));
+    int rc = upload_plan(op.get());
+    if (rc) return rc;
+    *out = op.release();
+    return 0;
+}
+
+void lsg_operator_destroy(lsg_operator* op) { delete op; }
+
+int lsg_operator_info(const lsg_operator* op, lsg_info* info) {
+    if (!op || !info) return fail(LSG_E_INVALID, "null argument");
+    const lsg::Plan& p = op->plan;
+    memset(info, 0, sizeof *info);
+    info->d = p.d;
+    info->n_points = p.n;
+    info->n_active = p.exa_off[p.nD];
+    info->n_depths = p.nD;
+    info->n_slab_entries = p.M;
+    info->n_cells = p.C;
+    int64_t cse = 0, cc = 0;
+    for (int c = 0; c < p.ncase; ++c)
+        for (int t : p.sorted[c]) { cse += p.slabs[t].n; cc += p.slabs[t].ncell; }
+    info->case_slab_entries = cse;
+    info->case_cells = cc;
+    info->device_bytes = (int64_t)op->dev_bytes;
+    info->plan_seconds = p.plan_seconds;
+    // algorithmic bytes of one FP64 matvec: x in, y out, nodal slabs, per-case
+    // P/gM/z slab traffic (3 passes), per-cell coefficient, corner tables of
+    // sparse slabs (read once per case item)
+    double s = 8.0;
+    double bytes = s * 2.0 * p.n + s * p.M + s * 3.0 * cse + s * cc;
+    int64_t sparse_cells = 0;
+    for (int c = 0; c < p.ncase; ++c)
+        for (int t : p.sorted[c])
+            if (!p.slabs[t].dense) sparse_cells += p.slabs[t].ncell;
+    bytes += 4.0 * (double)(1 << p.d) * sparse_cells;
+    info->matvec_bytes_fp64 = bytes;
+    info->matvec_flops = (double)cc * ((double)(2 * p.d + 2) * (1 << p.d));
+    return 0;
+}
+
+int lsg_operator_set_coefficient(lsg_operator* op, int32_t family, const double* params, int32_t nparams) {
+    if (!op) return fail(LSG_E_INVALID, "null operator");
+    if (family < 0 || family > 4) return fail(LSG_E_INVALID, "unknown coefficient family");
+    if (nparams < 0 || nparams > LSG_MAX_COEF_PARAMS || (nparams > 0 && !params))
+        return fail(LSG_E_INVALID, "bad coefficient parameters");
+    std::vector<double> pv(LSG_MAX_COEF_PARAMS, 0.0);
+    for (int i = 0; i < nparams; ++i) pv[i] = params[i];
+    size_t* tot = &op->dev_bytes;
+    int rc = 0;
+    if (!op->params.p) rc |= op->params.alloc(pv.size() * sizeof(double), tot);
+    if (!op->acell64.p) {
+        rc |= op->acell64.alloc(std::max<int64_t>(op->plan.C, 1) * sizeof(double), tot);
+        rc |= op->acell32.alloc(std::max<int64_t>(op->plan.C, 1) * sizeof(float), tot);
+    }
+    if (rc) return LSG_E_CUDA;
+    CUDA_TRY(cudaMemcpy(op->params.p, pv.data(), pv.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (op->plan.C > 0)
+        k_cell_coef<double><<<nblk(op->plan.C), 256>>>(op->dp, op->plan.C, family, op->params.as<double>(),
+                                                       op->acell64.as<double>(), op->acell32.as<float>(),
+                                                       op->cell_slab_off.as<int64_t>());
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaDeviceSynchronize());
+    op->have_coef = true;
+    op->have_diag = false;
+    return 0;
+}
+
+int lsg_matvec_device(lsg_operator* op, const void* x, void* y, int32_t precision, void* stream) {
+    if (!op || !x || !y) return fail(LSG_E_INVALID, "null argument");
+    if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == LSG_FP64) return matvec_dispatch<double>(op, (const double*)x, (double*)y, st);
+    if (precision == LSG_FP32) return matvec_dispatch<float>(op, (const float*)x, (float*)y, st);
+    return fail(LSG_E_INVALID, "precision must be LSG_FP64 or LSG_FP32");
+}
+
+int lsg_matvec(lsg_operator* op, const double* x, double* y) {
+    if (!op || !x || !y) return fail(LSG_E_INVALID, "null argument");
+    size_t b = op->plan.n * sizeof(double);
+    int rc = 0;
+    if (!op->xbuf64.p) rc |= op->xbuf64.alloc(b, &op->dev_bytes);
+    if (!op->ybuf64.p) rc |= op->ybuf64.alloc(b, &op->dev_bytes);
+    if (rc) return LSG_E_CUDA;
+    CUDA_TRY(cudaMemcpy(op->xbuf64.p, x, b, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(op->ybuf64.p, y, b, cudaMemcpyHostToDevice));  // hanging entries stay as given
+    rc = lsg_matvec_device(op, op->xbuf64.p, op->ybuf64.p, LSG_FP64, nullptr);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpy(y, op->ybuf64.p, b, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int lsg_diag_device(lsg_operator* op, double* diag, void* stream) {
+    if (!op || !diag) return fail(LSG_E_INVALID, "null argument");
+    int rc = compute_diag(op, (cudaStream_t)stream);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(diag, op->diag.p, op->plan.n * sizeof(double), cudaMemcpyDeviceToDevice,
+                             (cudaStream_t)stream));
+    return 0;
+}
+
+int lsg_diag(lsg_operator* op, double* diag) {
+    if (!op || !diag) return fail(LSG_E_INVALID, "null argument");
+    int rc = compute_diag(op, nullptr);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpy(diag, op->diag.p, op->plan.n * sizeof(double), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int lsg_set_learned_diag(lsg_operator* op, const double* diag) {
+    if (!op || !diag) return fail(LSG_E_INVALID, "null argument");
+    if (!op->learned.p) {
+        int rc = op->learned.alloc(op->plan.n * sizeof(double), &op->dev_bytes);
+        if (rc) return rc;
+    }
+    CUDA_TRY(cudaMemcpy(op->learned.p, diag, op->plan.n * sizeof(double), cudaMemcpyHostToDevice));
+    op->have_learned = true;
+    return 0;
+}
+
+struct lsg_plan {
+    lsg::Plan plan;
+};
+
+int lsg_plan_create(int32_t d, const int32_t* points, const uint8_t* active, int64_t n, lsg_plan** out) {
+    if (!out || !points || !active) return fail(LSG_E_INVALID, "null argument");
+    *out = nullptr;
+    std::unique_ptr<lsg_plan> p(new lsg_plan());
+    if (!lsg::build_plan(d, n, points, active, p->plan)) return fail(LSG_E_INVALID, p->plan.error);
+    *out = p.release();
+    return 0;
+}
+void lsg_plan_destroy(lsg_plan* p) { delete p; }
+
+int lsg_plan_info(const lsg_plan* p, lsg_info* info) {
+    if (!p || !info) return fail(LSG_E_INVALID, "null argument");
+    lsg_operator tmp;  // info only needs the plan
+    tmp.plan = p->plan;
+    return lsg_operator_info(&tmp, info);
+}
+int lsg_plan_export_depths(const lsg_plan* p, int32_t* depths) {
+    if (!p || !depths) return fail(LSG_E_INVALID, "null argument");
+    memcpy(depths, p->plan.D.data(), p->plan.D.size() * sizeof(int32_t));
+    return 0;
+}
+int lsg_plan_export_sorted_depths(const lsg_plan* p, int32_t c, int32_t* ids, int32_t* count) {
+    if (!p || !ids || !count) return fail(LSG_E_INVALID, "null argument");
+    if (c < 0 || c >= p->plan.ncase) return fail(LSG_E_INVALID, "case out of range");
+    const auto& v = p->plan.sorted[c];
+    memcpy(ids, v.data(), v.size() * sizeof(int32_t));
+    *count = (int32_t)v.size();
+    return 0;
+}
+int lsg_plan_export_cell_counts(const lsg_plan* p, int64_t* counts) {
+    if (!p || !counts) return fail(LSG_E_INVALID, "null argument");
+    for (int t = 0; t < p->plan.nD; ++t) counts[t] = p->plan.slabs[t].ncell;
+    return 0;
+}
+int lsg_plan_export_slab(const lsg_plan* p, int32_t t, int64_t* idx, int64_t* count) {
+    if (!p || !count) return fail(LSG_E_INVALID, "null argument");
+    if (t < 0 || t >= p->plan.nD) return fail(LSG_E_INVALID, "depth id out of range");
+    const lsg::Slab& s = p->plan.slabs[t];
+    *count = s.n;
+    if (idx) memcpy(idx, p->plan.slab_pt.data() + s.off, s.n * sizeof(int64_t));
+    return 0;
+}
+int lsg_plan_export_cells(const lsg_plan* p, int32_t t, int64_t* corners, int64_t* count) {
+    if (!p || !count) return fail(LSG_E_INVALID, "null argument");
+    const lsg::Plan& P = p->plan;
+    if (t < 0 || t >= P.nD) return fail(LSG_E_INVALID, "depth id out of range");
+    const lsg::Slab& s = P.slabs[t];
+    *count = s.ncell;
+    if (!corners) return 0;
+    int d = P.d, nc = 1 << d;
+    int64_t ext[lsg::kMaxDim], stride[lsg::kMaxDim];
+    int64_t st = 1;
+    for (int k = 0; k < d; ++k) { ext[k] = ((int64_t)1 << s.T[k]) - 1; stride[k] = st; st *= ext[k]; }
+    for (int64_t ci = 0; ci < s.ncell; ++ci) {
+        for (int b = 0; b < nc; ++b) {
+            int64_t pos;
+            if (!s.dense) pos = P.cell_corner[(s.corner_off + ci) * nc + b];
+            else {
+                int64_t r = ci;
+                pos = 0;
+                for (int k = 0; k < d && pos >= 0; ++k) {
+                    int64_t m = r % (ext[k] + 1);
+                    r /= (ext[k] + 1);
+                    int64_t c = m + ((b >> k) & 1);
+                    if (c == 0 || c == ext[k] + 1) pos = -1;
+                    else pos += (c - 1) * stride[k];
+                }
+            }
+            corners[ci * nc + b] = pos < 0 ? -1 : P.slab_pt[s.off + pos];
+        }
+    }
+    return 0;
+}
+
+static int64_t plan_lookup(const lsg::Plan& P, const int32_t* idx) {
+    // a point of depth <= T lies in slab T; look it up in the slab of its own depth
+    int d = P.d;
+    int32_t T[lsg::kMaxDim];
+    for (int k = 0; k < d; ++k) {
+        if (idx[k] < 2) return -1;
+        T[k] = lsg::depth1(idx[k]);
+    }
+    int t = -1;
+    for (int u = 0; u < P.nD && t < 0; ++u) {
+        bool eq = true;
+        for (int k = 0; k < d; ++k) eq &= P.D[u * d + k] == T[k];
+        if (eq) t = u;
+    }
+    if (t < 0) return -1;
+    const lsg::Slab& s = P.slabs[t];
+    uint64_t key = 0, st = 1;
+    for (int k = 0; k < d; ++k) {
+        int64_t c = 2 * (int64_t)(idx[k] - (1 << T[k])) + 1;
+        key += (uint64_t)(c - 1) * st;
+        st *= ((uint64_t)1 << T[k]) - 1;
+    }
+    const uint64_t* ks = P.slab_key.data() + s.off;
+    const uint64_t* it = std::lower_bound(ks, ks + s.n, key);
+    if (it == ks + s.n || *it != key) return -1;
+    return P.slab_pt[s.off + (it - ks)];
+}
+
+int lsg_plan_export_neighbors(const lsg_plan* p, int64_t* nbr) {
+    if (!p || !nbr) return fail(LSG_E_INVALID, "null argument");
+    const lsg::Plan& P = p->plan;
+    int d = P.d;
+    for (int64_t k = 0; k < P.n; ++k) {
+        int32_t J[lsg::kMaxDim];
+        for (int j = 0; j < d; ++j) {
+            for (int side = 0; side < 2; ++side) {
+                memcpy(J, &P.pts[k * d], d * sizeof(int32_t));
+                int32_t i = J[j];
+                J[j] = side ? (i >> (__builtin_ctz(~(unsigned)i) + 1)) : (i >> (__builtin_ctz((unsigned)i) + 1));
+                nbr[(k * d + j) * 2 + side] = plan_lookup(P, J);
+            }
+        }
+    }
+    return 0;
+}
+
+int lsg_plan_export_stencil(const lsg_plan* p, int64_t k, int64_t* idx, double* w, int32_t* count) {
+    if (!p || !idx || !w || !count) return fail(LSG_E_INVALID, "null argument");
+    const lsg::Plan& P = p->plan;
+    if (k < 0 || k >= P.n) return fail(LSG_E_INVALID, "point out of range");
+    int d = P.d;
+    int32_t j1[lsg::kMaxDim][5];
+    double w1[lsg::kMaxDim][5];
+    int n1[lsg::kMaxDim];
+    for (int j = 0; j < d; ++j) {
+        int32_t i = P.pts[k * d + j];
+        int t = lsg::depth1(i);
+        int32_t l = i >> (__builtin_ctz((unsigned)i) + 1), r = i >> (__builtin_ctz(~(unsigned)i) + 1);
+        bool lok = l > 1, rok = r > 1;
+        int n = 0;
+        j1[j][n] = i; w1[j][n++] = (t > 1 && (!lok || !rok)) ? 0.9 : 1.0;
+        if (lok) { j1[j][n] = l; w1[j][n++] = -0.6; }
+        if (rok) { j1[j][n] = r; w1[j][n++] = -0.6; }
+        // next left/right on level t of the neighbour (index.h:834-866)
+        if (lok) { int32_t x = l << 1; for (int q = 1; q < t - lsg::depth1(l); ++q) x = (x << 1) + 1; j1[j][n] = x; w1[j][n++] = 0.1; }
+        if (rok) { int32_t x = (r << 1) + 1; for (int q = 1; q < t - lsg::depth1(r); ++q) x <<= 1; j1[j][n] = x; w1[j][n++] = 0.1; }
+        n1[j] = n;
+    }
+    int pos[lsg::kMaxDim] = {0};
+    int cnt = 0;
+    for (;;) {
+        int32_t J[lsg::kMaxDim];
+        double val = 1.0;
+        for (int j = 0; j < d; ++j) {
+            J[j] = j1[j][pos[j]];
+            double wj = w1[j][pos[j]];
+            if (wj != 1.0) val = wj * val;  // the reference scales val in dimension order
+        }
+        idx[cnt] = plan_lookup(P, J);
+        w[cnt] = val;
+        ++cnt;
+        int j = 0;
+        while (j < d && ++pos[j] == n1[j]) { pos[j] = 0; ++j; }
+        if (j == d) break;
+    }
+    *count = cnt;
+    return 0;
+}
+
+}  // extern "C"
+
+// ============================================================================= CG
+namespace {
+
+struct Pinned {
+    double* h = nullptr;
+    Pinned() { cudaMallocHost(&h, 16 * sizeof(double)); }
+    ~Pinned() { if (h) cudaFreeHost(h); }
+};
+
+struct Solver {
+    lsg_operator* op;
+    int64_t n;
+    size_t bytes = 0;
+    DBuf r, g, d, h, part, s, ones;
+    DBuf r32, g32, d32, h32, e32, z32;
+    Pinned pin;
+};
+
+int solver_init(Solver& S, bool fp32) {
+    int64_t n = S.n;
+    size_t* t = &S.bytes;
+    int rc = 0;
+    rc |= S.r.alloc(n * 8, t);
+    rc |= S.g.alloc(n * 8, t);
+    rc |= S.d.alloc(n * 8, t);
+    rc |= S.h.alloc(n * 8, t);
+    rc |= S.part.alloc(kRedBlocks * 8, t);
+    rc |= S.s.alloc(16 * 8, t);
+    if (fp32) {
+        rc |= S.r32.alloc(n * 4, t);
+        rc |= S.g32.alloc(n * 4, t);
+        rc |= S.d32.alloc(n * 4, t);
+        rc |= S.h32.alloc(n * 4, t);
+        rc |= S.e32.alloc(n * 4, t);
+        rc |= S.z32.alloc(n * 4, t);
+    }
+    if (rc) return LSG_E_CUDA;
+    // every vector starts at zero (fresh VectorSparseG), hanging entries included
+    for (DBuf* b : {&S.r, &S.g, &S.d, &S.h, &S.s, &S.r32, &S.g32, &S.d32, &S.h32, &S.e32, &S.z32})
+        if (b->p) CUDA_TRY(cudaMemset(b->p, 0, b->bytes));
+    return 0;
+}
+
+// One CG iteration (CG::solveHomogen loop body, cg_method.h:852-879) with
+// beta/d-update of the previous iteration moved to the front; the scalars
+// live on the device so the body can be captured as a CUDA graph.
+// s[0]=delta s[1]=dg s[2]=tau s[3]=delta_new s[4]=beta s[5]=rr
+template <typename V>
+int cg_body(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, bool want_rr, cudaStream_t st) {
+    int64_t n = S.n;
+    double* s = S.s.as<double>();
+    double* part = S.part.as<double>();
+    k_beta<<<1, 1, 0, st>>>(s);
+    k_update_d<V><<<nblk(n), 256, 0, st>>>(n, s, h, d);
+    int rc = std::is_same<V, double>::value
+                 ? lsg_internal_matvec64(S.op, (const double*)d, (double*)g, st)
+                 : lsg_internal_matvec32(S.op, (const float*)d, (float*)g, st);
+    if (rc) return rc;
+    k_dot_partial<V, V><<<kRedBlocks, kRedThreads, 0, st>>>(d, g, n, part);
+    k_dot_final<<<1, 1024, 0, st>>>(part, kRedBlocks, s + 1);
+    k_tau<<<1, 1, 0, st>>>(s);
+    k_update_rx<V><<<nblk(n), 256, 0, st>>>(n, s, r, x, g, d);
+    k_precond<V><<<nblk(n), 256, 0, st>>>(n, lsg_internal_active(S.op), r, z, h, 1);
+    k_dot_partial<V, V><<<kRedBlocks, kRedThreads, 0, st>>>(r, h, n, part);
+    k_dot_final<<<1, 1024, 0, st>>>(part, kRedBlocks, s + 3);
+    if (want_rr) {
+        k_dot_partial<V, V><<<kRedBlocks, kRedThreads, 0, st>>>(r, r, n, part);
+        k_dot_final<<<1, 1024, 0, st>>>(part, kRedBlocks, s + 5);
+    }
+    cudaMemcpyAsync(S.pin.h, s, 8 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// Runs CG on (x, r, ...) until the criterion holds.  r must hold f - A x and
+// h, d, s[0], s[3] the start state.  Returns iterations in *its.
+template <typename V>
+int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int crit, double rr_stop, int maxit,
+            bool use_graph, cudaStream_t st, int* its, double* last_rr) {
+    cudaGraphExec_t exec = nullptr;
+    bool want_rr = crit == 1;
+    int it = 0;
+    int rc = 0;
+    if (use_graph) {
+        cudaGraph_t graph;
+        CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        rc = cg_body<V>(S, x, r, g, d, h, z, want_rr, st);
+        cudaError_t e = cudaStreamEndCapture(st, &graph);
+        if (rc) return rc;
+        if (e != cudaSuccess) return fail(LSG_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(LSG_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    for (int i = 1; i <= maxit; ++i) {
+        if (use_graph) {
+            cudaError_t e = cudaGraphLaunch(exec, st);
+            if (e != cudaSuccess) { rc = fail(LSG_E_CUDA, cudaGetErrorString(e)); break; }
+        } else {
+            rc = cg_body<V>(S, x, r, g, d, h, z, want_rr, st);
+            if (rc) break;
+        }
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) { rc = fail(LSG_E_CUDA, cudaGetErrorString(e)); break; }
+        it = i;
+        double dn = S.pin.h[3];
+        if (want_rr) *last_rr = S.pin.h[5];
+        if (!std::isfinite(dn)) break;
+        if (crit == 0 && dn < eps * eps) break;
+        if (crit == 1 && S.pin.h[5] <= rr_stop) break;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    *its = it;
+    return rc;
+}
+
+template <typename V>
+int cg_start(Solver& S, const V* f, V* x, V* r, V* d, V* h, const V* z, cudaStream_t st) {
+    int64_t n = S.n;
+    double* s = S.s.as<double>();
+    CUDA_TRY(cudaMemsetAsync(r, 0, n * sizeof(V), st));
+    int rc = std::is_same<V, double>::value ? lsg_internal_matvec64(S.op, (const double*)x, (double*)r, st)
+                                            : lsg_internal_matvec32(S.op, (const float*)x, (float*)r, st);
+    if (rc) return rc;
+    k_sub<V><<<nblk(n), 256, 0, st>>>(n, f, r);
+    CUDA_TRY(cudaMemsetAsync(h, 0, n * sizeof(V), st));
+    k_precond<V><<<nblk(n), 256, 0, st>>>(n, lsg_internal_active(S.op), r, z, h, 0);
+    CUDA_TRY(cudaMemsetAsync(d, 0, n * sizeof(V), st));
+    k_dot_partial<V, V><<<kRedBlocks, kRedThreads, 0, st>>>(r, h, n, S.part.as<double>());
+    k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, s + 0);
+    CUDA_TRY(cudaMemcpyAsync(s + 3, s + 0, sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+double host_dot(Solver& S, const double* a, const double* b, cudaStream_t st) {
+    k_dot_partial<double, double><<<kRedBlocks, kRedThreads, 0, st>>>(a, b, S.n, S.part.as<double>());
+    k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, S.s.as<double>() + 8);
+    cudaMemcpyAsync(S.pin.h + 8, S.s.as<double>() + 8, sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return S.pin.h[8];
+}
+
+int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_opts* o, lsg_solve_report* rep,
+                 cudaStream_t user_st) {
+    if (!op || !f || !x || !o) return fail(LSG_E_INVALID, "null argument");
+    if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
+    cudaStream_t st;
+    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaEvent_t ev0, ev1, evu;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    cudaEventCreate(&evu);
+    cudaEventRecord(evu, user_st);
+    cudaStreamWaitEvent(st, evu, 0);
+    Solver S;
+    S.op = op;
+    S.n = op->plan.n;
+    int64_t n = S.n;
+    lsg_solve_report R;
+    memset(&R, 0, sizeof R);
+    int rc = solver_init(S, o->precision == LSG_FP32);
+    const double* zdiag = nullptr;
+    if (!rc && o->precond == 0) { rc = compute_diag(op, st); zdiag = op->diag.as<double>(); }
+    if (!rc && o->precond == 2) {
+        if (!op->have_learned) rc = fail(LSG_E_STATE, "no learned diagonal installed");
+        zdiag = op->learned.as<double>();
+    }
+    int maxit = o->max_iter > 0 ? o->max_iter : 500;
+    double eps = o->eps;
+    cudaEventRecord(ev0, st);
+    double ff = rc ? 0.0 : host_dot(S, f, f, st);
+    if (!rc && o->precision == LSG_FP64) {
+        rc = cg_start<double>(S, f, x, S.r.as<double>(), S.d.as<double>(), S.h.as<double>(), zdiag, st);
+        int its = 0;
+        double rr = 0.0;
+        if (!rc)
+            rc = cg_loop<double>(S, x, S.r.as<double>(), S.g.as<double>(), S.d.as<double>(), S.h.as<double>(), zdiag, eps,
+                                 o->criterion, eps * eps * ff, maxit, o->use_graph != 0, st, &its, &rr);
+        R.iterations = its;
+        R.outer_iterations = 1;
+    } else if (!rc) {
+        // FP32 inner CG inside FP64 iterative refinement
+        int inner = o->inner_iter > 0 ? o->inner_iter : 30;
+        double itol = o->inner_tol > 0 ? o->inner_tol : 1e-4;
+        float* z32 = nullptr;
+        if (zdiag) {
+            k_to_f32<<<nblk(n), 256, 0, st>>>(n, zdiag, S.z32.as<float>());
+            z32 = S.z32.as<float>();
+        }
+        double* r = S.r.as<double>();
+        int total = 0, outer = 0;
+        for (outer = 0; outer < maxit && total < maxit * 4; ++outer) {
+            CUDA_TRY(cudaMemsetAsync(r, 0, n * 8, st));
+            rc = lsg_internal_matvec64(op, x, r, st);
+            if (rc) break;
+            k_sub<double><<<nblk(n), 256, 0, st>>>(n, f, r);
+            double rr = host_dot(S, r, r, st);
+            if (!std::isfinite(rr)) { rc = fail(LSG_E_NOCONV, "non-finite residual"); break; }
+            if (rr <= eps * eps * ff) break;
+            double nr = std::sqrt(rr);
+            float* r32 = S.r32.as<float>();
+            float* e32 = S.e32.as<float>();
+            k_scale_to_f32<<<nblk(n), 256, 0, st>>>(n, r, 1.0 / nr, r32);
+            CUDA_TRY(cudaMemsetAsync(e32, 0, n * 4, st));
+            // inner start: r32 already = rhs - A*0
+            float* h32 = S.h32.as<float>();
+            float* d32 = S.d32.as<float>();
+            CUDA_TRY(cudaMemsetAsync(h32, 0, n * 4, st));
+            k_precond<float><<<nblk(n), 256, 0, st>>>(n, lsg_internal_active(op), r32, z32, h32, 0);
+            CUDA_TRY(cudaMemsetAsync(d32, 0, n * 4, st));
+            double* s = S.s.as<double>();
+            k_dot_partial<float, float><<<kRedBlocks, kRedThreads, 0, st>>>(r32, h32, n, S.part.as<double>());
+            k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, s + 0);
+            cudaMemcpyAsync(s + 3, s + 0, 8, cudaMemcpyDeviceToDevice, st);
+            int its = 0;
+            double lrr = 0.0;
+            rc = cg_loop<float>(S, e32, r32, S.g32.as<float>(), d32, h32, z32, 0.0, 1, itol * itol, inner,
+                                o->use_graph != 0, st, &its, &lrr);
+            if (rc) break;
+            total += its;
+            k_axpy_f32<<<nblk(n), 256, 0, st>>>(n, nr, e32, x);
+        }
+        R.iterations = total;
+        R.outer_iterations = outer;
+    }
+    cudaEventRecord(ev1, st);
+    if (!rc) {
+        // true relative residual in FP64
+        double* r = S.r.as<double>();
+        cudaMemsetAsync(r, 0, n * 8, st);
+        rc = lsg_internal_matvec64(op, x, r, st);
+        if (!rc) {
+            k_sub<double><<<nblk(n), 256, 0, st>>>(n, f, r);
+            double rr = host_dot(S, r, r, st);
+            R.rel_residual = ff > 0 ? std::sqrt(rr / ff) : std::sqrt(rr);
+        }
+    }
+    cudaStreamSynchronize(st);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    R.seconds = ms * 1e-3;
+    double target = o->criterion == 1 ? eps : 1e300;
+    R.converged = (!rc && R.rel_residual <= target * 1.0000001) ? 1 : 0;
+    if (o->criterion == 0 && !rc) R.converged = 1;
+    cudaEventRecord(evu, st);
+    cudaStreamWaitEvent(user_st, evu, 0);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    cudaEventDestroy(evu);
+    cudaStreamDestroy(st);
+    if (rep) *rep = R;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lsg_cg_solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_opts* opts,
+                        lsg_solve_report* rep, void* stream) {
+    return solve_device(op, f, x, opts, rep, (cudaStream_t)stream);
+}
+
+int lsg_cg_solve(lsg_operator* op, const double* f, double* x, const lsg_solver_opts* opts, lsg_solve_report* rep) {
+    if (!op || !f || !x || !opts) return fail(LSG_E_INVALID, "null argument");
+    size_t b = op->plan.n * sizeof(double);
+    DBuf fd, xd;
+    size_t dummy = 0;
+    if (fd.alloc(b, &dummy) || xd.alloc(b, &dummy)) return LSG_E_CUDA;
+    CUDA_TRY(cudaMemcpy(fd.p, f, b, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(xd.p, x, b, cudaMemcpyHostToDevice));
+    int rc = solve_device(op, fd.as<double>(), xd.as<double>(), opts, rep, nullptr);
+    CUDA_TRY(cudaDeviceSynchronize());
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpy(x, xd.p, b, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+}  // extern "C"
+
+static int lsg_internal_matvec64(lsg_operator* op, const double* x, double* y, cudaStream_t st) {
+    return matvec_dispatch<double>(op, x, y, st);
+}
+static int lsg_internal_matvec32(lsg_operator* op, const float* x, float* y, cudaStream_t st) {
+    return matvec_dispatch<float>(op, x, y, st);
+}
+static const uint8_t* lsg_internal_active(lsg_operator* op) { return op->act.as<uint8_t>(); }

@@ -1,0 +1,722 @@
+// Host planner for the prewavelet matvec (see lsg_plan.h for the reference anchors).
+#include "lsg_plan.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <numeric>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace lsg {
+
+int depth1(int32_t i) { return i == 0 ? 0 : 31 - __builtin_clz((unsigned)i); }
+
+namespace {
+
+// level-t integer coordinate of a 1D index of depth <= t (coordinate * 2^t)
+inline int64_t coord_at(int32_t idx, int t) {
+    int ti = depth1(idx);
+    int64_t c = 2 * (int64_t)(idx - (1 << ti)) + 1;
+    return c << (t - ti);
+}
+
+struct Geometry {  // level-T interior grid: coordinates 1..2^T_k-1 per dim
+    int d;
+    int64_t ext[kMaxDim];     // 2^T_k - 1
+    uint64_t stride[kMaxDim];
+    int64_t cext[kMaxDim];    // cells per dim: 2^T_k
+    uint64_t cstride[kMaxDim];
+    int32_t T[kMaxDim];
+    explicit Geometry(int d_, const int32_t* T_) : d(d_) {
+        uint64_t s = 1, cs = 1;
+        for (int k = 0; k < d; ++k) {
+            T[k] = T_[k];
+            ext[k] = ((int64_t)1 << T_[k]) - 1;
+            stride[k] = s;
+            s *= (uint64_t)ext[k];
+            cext[k] = (int64_t)1 << T_[k];
+            cstride[k] = cs;
+            cs *= (uint64_t)cext[k];
+        }
+    }
+    uint64_t key(const int64_t* c) const {
+        uint64_t k = 0;
+        for (int j = 0; j < d; ++j) k += (uint64_t)(c[j] - 1) * stride[j];
+        return k;
+    }
+    void decode(uint64_t key, int64_t* c) const {
+        for (int j = 0; j < d; ++j) {
+            c[j] = (int64_t)(key % (uint64_t)ext[j]) + 1;
+            key /= (uint64_t)ext[j];
+        }
+    }
+    uint64_t total() const {
+        uint64_t t = 1;
+        for (int j = 0; j < d; ++j) t *= (uint64_t)ext[j];
+        return t;
+    }
+};
+
+inline int64_t find_key(const uint64_t* keys, int64_t n, uint64_t k) {
+    const uint64_t* it = std::lower_bound(keys, keys + n, k);
+    if (it != keys + n && *it == k) return it - keys;
+    return -1;
+}
+
+// slab position of level-T coordinates c (interior), -1 if absent
+inline int64_t slab_pos(const Plan& p, int t, const Geometry& g, const int64_t* c) {
+    uint64_t k = g.key(c);
+    const Slab& s = p.slabs[t];
+    if (s.dense) return (int64_t)k;
+    return find_key(p.slab_key.data() + s.off, s.n, k);
+}
+
+// One-dimensional prewavelet stencil of an odd level-t coordinate c
+// (IndexDimension::nextFiveP, indices/index.cc:252-327) in level-t coordinates:
+// positions {c, c-1, c+1, c-2, c+2} in the reference's direction order
+// (Mitte, Links, Rechts, LinksLinks, RechtsRechts), weight codes
+// 1: 1.0, 2: 0.9 (next to the boundary, depth > 1), 3: -0.6, 4: 0.1.
+inline int stencil1(int64_t c, int t, int64_t* pos, int* code) {
+    int64_t top = (int64_t)1 << t;
+    int n = 0;
+    bool lok = c - 1 > 0, rok = c + 1 < top;
+    pos[n] = c;
+    code[n++] = (t > 1 && (!lok || !rok)) ? 2 : 1;
+    if (lok) { pos[n] = c - 1; code[n++] = 3; }
+    if (rok) { pos[n] = c + 1; code[n++] = 3; }
+    if (lok) { pos[n] = c - 2; code[n++] = 4; }
+    if (rok) { pos[n] = c + 2; code[n++] = 4; }
+    return n;
+}
+// weight code of stencil(i) at position q (0 if q is not in it)
+inline int stencil_code(int64_t i, int t, int64_t q) {
+    int64_t pos[5];
+    int code[5];
+    int n = stencil1(i, t, pos, code);
+    for (int s = 0; s < n; ++s)
+        if (pos[s] == q) return code[s];
+    return 0;
+}
+
+void sort_unique(std::vector<uint64_t>& v) {
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+}
+
+// Sum-factorised tensor stencil transform for one depth.
+//  nodal   (forward=true):  in = active exact-depth points, out = all slab entries;
+//          stage j maps odd coordinates in dim j to any coordinate in their stencil.
+//  convert (forward=false): in = slab entries, out = active exact-depth points;
+//          stage j gathers the stencil of an odd coordinate in dim j.
+struct StageOut {
+    std::vector<std::vector<uint64_t>> dom;  // d+1 domains (sorted keys)
+    std::vector<std::vector<int32_t>> src;   // d stages
+    std::vector<std::vector<int32_t>> code;
+};
+
+void build_transform(const Geometry& g, const std::vector<uint64_t>& in_keys, const std::vector<uint64_t>& out_keys,
+                     bool nodal, int nsrc, StageOut& so) {
+    int d = g.d;
+    so.dom.assign(d + 1, {});
+    so.src.assign(d, {});
+    so.code.assign(d, {});
+    // forward reachability
+    std::vector<std::vector<uint64_t>> fwd(d + 1);
+    fwd[0] = in_keys;
+    int64_t c[kMaxDim], pos[5];
+    int code[5];
+    for (int j = 0; j < d; ++j) {
+        std::vector<uint64_t> nxt;
+        nxt.reserve(fwd[j].size() * (nodal ? 3 : 2));
+        int64_t top = (int64_t)1 << g.T[j];
+        for (uint64_t k : fwd[j]) {
+            g.decode(k, c);
+            int64_t cj = c[j];
+            if (nodal) {  // odd cj spreads to its stencil
+                int n = stencil1(cj, g.T[j], pos, code);
+                for (int s = 0; s < n; ++s) { c[j] = pos[s]; nxt.push_back(g.key(c)); }
+            } else {      // any cj reaches the odd coordinates whose stencil contains it
+                for (int64_t o = -2; o <= 2; ++o) {
+                    int64_t i = cj + o;
+                    if (i < 1 || i >= top || !(i & 1)) continue;
+                    if (stencil_code(i, g.T[j], cj)) { c[j] = i; nxt.push_back(g.key(c)); }
+                }
+            }
+            c[j] = cj;
+        }
+        sort_unique(nxt);
+        fwd[j + 1].swap(nxt);
+    }
+    // backward need, intersected with reachability
+    so.dom[d] = out_keys;
+    for (int j = d - 1; j >= 0; --j) {
+        std::vector<uint64_t> need;
+        need.reserve(so.dom[j + 1].size() * 3);
+        int64_t top = (int64_t)1 << g.T[j];
+        for (uint64_t k : so.dom[j + 1]) {
+            g.decode(k, c);
+            int64_t cj = c[j];
+            if (nodal) {
+                for (int64_t o = -2; o <= 2; ++o) {
+                    int64_t i = cj + o;
+                    if (i < 1 || i >= top || !(i & 1)) continue;
+                    if (stencil_code(i, g.T[j], cj)) { c[j] = i; need.push_back(g.key(c)); }
+                }
+            } else {
+                int n = stencil1(cj, g.T[j], pos, code);
+                for (int s = 0; s < n; ++s) { c[j] = pos[s]; need.push_back(g.key(c)); }
+            }
+            c[j] = cj;
+        }
+        sort_unique(need);
+        if (j == 0) {
+            so.dom[0] = in_keys;  // stage-0 sources index the input list directly
+        } else {
+            std::vector<uint64_t> dom;
+            std::set_intersection(need.begin(), need.end(), fwd[j].begin(), fwd[j].end(), std::back_inserter(dom));
+            so.dom[j].swap(dom);
+        }
+    }
+    // gather tables
+    for (int j = 0; j < d; ++j) {
+        const auto& out = so.dom[j + 1];
+        const auto& in = so.dom[j];
+        auto& src = so.src[j];
+        auto& cod = so.code[j];
+        src.assign(out.size() * nsrc, -1);
+        cod.assign(out.size(), 0);
+        int64_t top = (int64_t)1 << g.T[j];
+        for (size_t e = 0; e < out.size(); ++e) {
+            g.decode(out[e], c);
+            int64_t cj = c[j];
+            int ns = 0;
+            int packed = 0;
+            if (nodal) {
+                for (int64_t o = -2; o <= 2; ++o) {
+                    int64_t i = cj + o;
+                    if (i < 1 || i >= top || !(i & 1)) continue;
+                    int cd = stencil_code(i, g.T[j], cj);
+                    if (!cd) continue;
+                    c[j] = i;
+                    int64_t at = find_key(in.data(), (int64_t)in.size(), g.key(c));
+                    if (at >= 0) {
+                        src[e * nsrc + ns] = (int32_t)at;
+                        packed |= cd << (3 * ns);
+                        ++ns;
+                    }
+                }
+            } else {
+                int n = stencil1(cj, g.T[j], pos, code);
+                for (int s = 0; s < n; ++s) {
+                    c[j] = pos[s];
+                    int64_t at = find_key(in.data(), (int64_t)in.size(), g.key(c));
+                    if (at >= 0) {
+                        src[e * nsrc + ns] = (int32_t)at;
+                        packed |= code[s] << (3 * ns);
+                        ++ns;
+                    }
+                }
+            }
+            c[j] = cj;
+            cod[e] = packed;
+        }
+    }
+}
+
+}  // namespace
+
+// DepthList::recursiveDepth (iterator/depthIterator.cpp:7-45)
+static void rec_depth(const Plan& p, const std::map<std::vector<int32_t>, int>& ids, int c, bool checkProl, int dd,
+                      std::vector<int32_t>& T, std::vector<int32_t>& out) {
+    int d = p.d;
+    if (checkProl && dd > 0) {
+        if (!((c >> dd) & 1)) {
+            for (int t = 1; t <= p.maxdep[dd]; ++t) { T[dd] = t; rec_depth(p, ids, c, checkProl, dd - 1, T, out); }
+        } else rec_depth(p, ids, c, checkProl, dd - 1, T, out);
+    }
+    if (checkProl && dd == 0) {
+        if (!(c & 1)) {
+            for (int t = 1; t <= p.maxdep[0]; ++t) { T[0] = t; rec_depth(p, ids, c, false, d - 1, T, out); }
+        } else rec_depth(p, ids, c, false, d - 1, T, out);
+    }
+    if (!checkProl && dd >= 0) {
+        if ((c >> dd) & 1) {
+            for (int t = p.maxdep[dd]; t > 1; --t) { T[dd] = t; rec_depth(p, ids, c, checkProl, dd - 1, T, out); }
+        } else rec_depth(p, ids, c, checkProl, dd - 1, T, out);
+    }
+    if (dd < 0) {
+        auto it = ids.find(T);
+        if (it != ids.end()) out.push_back(it->second);
+    }
+}
+
+static std::map<std::vector<int32_t>, int> depth_ids(const Plan& p) {
+    std::map<std::vector<int32_t>, int> ids;
+    for (int t = 0; t < p.nD; ++t) ids[std::vector<int32_t>(p.D.begin() + t * p.d, p.D.begin() + (t + 1) * p.d)] = t;
+    return ids;
+}
+
+std::vector<int32_t> sorted_depths(const Plan& p, int c) {
+    auto ids = depth_ids(p);
+    std::vector<int32_t> T(p.d, 0), out;
+    rec_depth(p, ids, c, true, p.d - 1, T, out);
+    return out;
+}
+
+bool build_plan(int d, int64_t n, const int32_t* points, const uint8_t* active, Plan& p) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (d < 1 || d > kMaxDim || n < 1) { p.error = "dimension must be 1..8 and the grid non-empty"; return false; }
+    p.d = d;
+    p.n = n;
+    p.pts.assign(points, points + n * d);
+    p.act.assign(active, active + n);
+    // ---- depths and depth list (first appearance, iterator/depthIterator.h:14-50)
+    std::map<std::vector<int32_t>, int> ids;
+    p.did.resize(n);
+    std::vector<int32_t> Tk(d);
+    for (int64_t k = 0; k < n; ++k) {
+        for (int j = 0; j < d; ++j) {
+            int32_t i = points[k * d + j];
+            if (i < 2) { p.error = "boundary points (1D index 0 or 1) are not allowed in a Dirichlet grid"; return false; }
+            if (depth1(i) > 30) { p.error = "depth too large"; return false; }
+            Tk[j] = depth1(i);
+        }
+        auto it = ids.find(Tk);
+        int t;
+        if (it == ids.end()) {
+            t = p.nD++;
+            ids[Tk] = t;
+            p.D.insert(p.D.end(), Tk.begin(), Tk.end());
+        } else t = it->second;
+        p.did[k] = t;
+    }
+    int nD = p.nD;
+    p.maxdep.assign(d, 0);
+    for (int t = 0; t < nD; ++t)
+        for (int j = 0; j < d; ++j) p.maxdep[j] = std::max(p.maxdep[j], p.D[t * d + j]);
+    p.ex_off.assign(nD + 1, 0);
+    p.exa_off.assign(nD + 1, 0);
+    for (int64_t k = 0; k < n; ++k) {
+        p.ex_off[p.did[k] + 1]++;
+        if (active[k]) p.exa_off[p.did[k] + 1]++;
+    }
+    for (int t = 0; t < nD; ++t) { p.ex_off[t + 1] += p.ex_off[t]; p.exa_off[t + 1] += p.exa_off[t]; }
+    p.ex.resize(n);
+    p.exa.resize(p.exa_off[nD]);
+    {
+        std::vector<int64_t> f(nD, 0), fa(nD, 0);
+        for (int64_t k = 0; k < n; ++k) {
+            int t = p.did[k];
+            p.ex[p.ex_off[t] + f[t]++] = k;
+            if (active[k]) p.exa[p.exa_off[t] + fa[t]++] = k;
+        }
+    }
+    // duplicate points are invalid
+    {
+        std::vector<uint64_t> h(n);
+        for (int64_t k = 0; k < n; ++k) {
+            uint64_t x = 1469598103934665603ull;
+            for (int j = 0; j < d; ++j) { x ^= (uint64_t)points[k * d + j]; x *= 1099511628211ull; }
+            h[k] = x;
+        }
+        std::vector<int64_t> ord(n);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) {
+            if (h[a] != h[b]) return h[a] < h[b];
+            return std::lexicographical_compare(points + a * d, points + a * d + d, points + b * d, points + b * d + d);
+        });
+        for (int64_t k = 1; k < n; ++k)
+            if (h[ord[k]] == h[ord[k - 1]] && std::equal(points + ord[k] * d, points + ord[k] * d + d, points + ord[k - 1] * d)) {
+                p.error = "duplicate grid point";
+                return false;
+            }
+    }
+    // ---- slabs: points of depth <= T, ordered by level-T linear key
+    p.slabs.resize(nD);
+    std::vector<std::vector<uint64_t>> skeys(nD);
+    std::vector<std::vector<int64_t>> spts(nD);
+#pragma omp parallel for schedule(dynamic)
+    for (int t = 0; t < nD; ++t) {
+        const int32_t* T = &p.D[t * d];
+        Geometry g(d, T);
+        std::vector<std::pair<uint64_t, int64_t>> v;
+        for (int u = 0; u < nD; ++u) {
+            const int32_t* U = &p.D[u * d];
+            bool le = true;
+            for (int j = 0; j < d; ++j) le &= U[j] <= T[j];
+            if (!le) continue;
+            for (int64_t e = p.ex_off[u]; e < p.ex_off[u + 1]; ++e) {
+                int64_t k = p.ex[e];
+                int64_t c[kMaxDim];
+                for (int j = 0; j < d; ++j) c[j] = coord_at(points[k * d + j], T[j]);
+                v.emplace_back(g.key(c), k);
+            }
+        }
+        std::sort(v.begin(), v.end());
+        skeys[t].resize(v.size());
+        spts[t].resize(v.size());
+        for (size_t e = 0; e < v.size(); ++e) { skeys[t][e] = v[e].first; spts[t][e] = v[e].second; }
+        Slab& s = p.slabs[t];
+        std::copy(T, T + d, s.T);
+        s.n = (int64_t)v.size();
+        s.dense = (uint64_t)s.n == g.total();
+    }
+    p.M = 0;
+    for (int t = 0; t < nD; ++t) { p.slabs[t].off = p.M; p.M += p.slabs[t].n; p.max_slab = std::max(p.max_slab, p.slabs[t].n); }
+    p.slab_key.resize(p.M);
+    p.slab_pt.resize(p.M);
+    for (int t = 0; t < nD; ++t) {
+        std::copy(skeys[t].begin(), skeys[t].end(), p.slab_key.begin() + p.slabs[t].off);
+        std::copy(spts[t].begin(), spts[t].end(), p.slab_pt.begin() + p.slabs[t].off);
+    }
+    skeys.clear();
+    spts.clear();
+    // ---- cells of depth T+1 in the grid (cells/CellStructure.h:23-61)
+    std::vector<std::vector<uint64_t>> ckeys(nD);
+    std::vector<std::vector<int32_t>> ccorn(nD);
+    int nc = 1 << d;
+#pragma omp parallel for schedule(dynamic)
+    for (int t = 0; t < nD; ++t) {
+        Slab& s = p.slabs[t];
+        Geometry g(d, s.T);
+        if (s.dense) {
+            uint64_t nc_all = 1;
+            for (int j = 0; j < d; ++j) nc_all *= (uint64_t)g.cext[j];
+            s.ncell = (int64_t)nc_all;
+            continue;
+        }
+        std::vector<uint64_t> cand;
+        cand.reserve(s.n * nc);
+        int64_t c[kMaxDim], m[kMaxDim];
+        for (int64_t e = 0; e < s.n; ++e) {
+            g.decode(p.slab_key[s.off + e], c);
+            for (int b = 0; b < nc; ++b) {
+                uint64_t ck = 0;
+                for (int j = 0; j < d; ++j) ck += (uint64_t)(c[j] - ((b >> j) & 1)) * g.cstride[j];
+                cand.push_back(ck);
+            }
+        }
+        sort_unique(cand);
+        for (uint64_t ck : cand) {
+            uint64_t r = ck;
+            for (int j = 0; j < d; ++j) { m[j] = (int64_t)(r % (uint64_t)g.cext[j]); r /= (uint64_t)g.cext[j]; }
+            int32_t corner[1 << kMaxDim];
+            bool ok = true;
+            for (int b = 0; b < nc && ok; ++b) {
+                bool bnd = false;
+                for (int j = 0; j < d; ++j) {
+                    c[j] = m[j] + ((b >> j) & 1);
+                    if (c[j] == 0 || c[j] == g.cext[j]) bnd = true;
+                }
+                if (bnd) { corner[b] = -1; continue; }
+                int64_t at = find_key(p.slab_key.data() + s.off, s.n, g.key(c));
+                if (at < 0) ok = false;
+                else corner[b] = (int32_t)at;
+            }
+            if (!ok) continue;
+            ckeys[t].push_back(ck);
+            ccorn[t].insert(ccorn[t].end(), corner, corner + nc);
+        }
+        s.ncell = (int64_t)ckeys[t].size();
+    }
+    p.C = 0;
+    int64_t ck_total = 0;
+    for (int t = 0; t < nD; ++t) {
+        Slab& s = p.slabs[t];
+        s.cell_off = p.C;
+        p.C += s.ncell;
+        if (!s.dense) { s.corner_off = ck_total; ck_total += s.ncell; }
+    }
+    p.cell_key.resize(ck_total);
+    p.cell_corner.resize(ck_total * nc);
+    for (int t = 0; t < nD; ++t) {
+        Slab& s = p.slabs[t];
+        if (s.dense) continue;
+        std::copy(ckeys[t].begin(), ckeys[t].end(), p.cell_key.begin() + s.corner_off);
+        std::copy(ccorn[t].begin(), ccorn[t].end(), p.cell_corner.begin() + s.corner_off * nc);
+    }
+    ckeys.clear();
+    ccorn.clear();
+    // ---- tensor stencil transforms (calcNodal, MatrixVectorHomogen.cpp:43-74;
+    //      ConvertToPrewavelet2, MatrixVectorHomogen.h:540-562)
+    std::vector<StageOut> nod(nD), con(nD);
+#pragma omp parallel for schedule(dynamic)
+    for (int t = 0; t < nD; ++t) {
+        Slab& s = p.slabs[t];
+        Geometry g(d, s.T);
+        std::vector<uint64_t> act_keys;
+        for (int64_t e = p.exa_off[t]; e < p.exa_off[t + 1]; ++e) {
+            int64_t k = p.exa[e];
+            int64_t c[kMaxDim];
+            for (int j = 0; j < d; ++j) c[j] = coord_at(points[k * d + j], s.T[j]);
+            act_keys.push_back(g.key(c));
+        }
+        // active exact-depth points are stored in storage order; the transforms
+        // use them sorted by key, so sort the list (exa) the same way
+        std::vector<std::pair<uint64_t, int64_t>> kv;
+        for (size_t e = 0; e < act_keys.size(); ++e) kv.emplace_back(act_keys[e], p.exa[p.exa_off[t] + e]);
+        std::sort(kv.begin(), kv.end());
+        for (size_t e = 0; e < kv.size(); ++e) { act_keys[e] = kv[e].first; p.exa[p.exa_off[t] + e] = kv[e].second; }
+        std::vector<uint64_t> slab_keys(p.slab_key.begin() + s.off, p.slab_key.begin() + s.off + s.n);
+        build_transform(g, act_keys, slab_keys, true, 3, nod[t]);
+        build_transform(g, slab_keys, act_keys, false, 5, con[t]);
+    }
+    p.nodal.nsrc = 3;
+    p.convert.nsrc = 5;
+    p.nodal_dom.assign(nD * (d + 1), 0);
+    p.convert_dom.assign(nD * (d + 1), 0);
+    for (StageSet* ss : {&p.nodal, &p.convert}) {
+        std::vector<StageOut>& so = ss == &p.nodal ? nod : con;
+        std::vector<int64_t>& dom = ss == &p.nodal ? p.nodal_dom : p.convert_dom;
+        ss->stage_off.assign(nD * d + 1, 0);
+        int64_t tot = 0;
+        for (int t = 0; t < nD; ++t) {
+            for (int j = 0; j <= d; ++j) dom[t * (d + 1) + j] = (int64_t)so[t].dom[j].size();
+            for (int j = 0; j < d; ++j) {
+                ss->stage_off[t * d + j] = tot;
+                tot += (int64_t)so[t].code[j].size();
+            }
+        }
+        ss->stage_off[nD * d] = tot;
+        ss->src.resize(tot * ss->nsrc);
+        ss->code.resize(tot);
+        for (int t = 0; t < nD; ++t)
+            for (int j = 0; j < d; ++j) {
+                int64_t o = ss->stage_off[t * d + j];
+                std::copy(so[t].src[j].begin(), so[t].src[j].end(), ss->src.begin() + o * ss->nsrc);
+                std::copy(so[t].code[j].begin(), so[t].code[j].end(), ss->code.begin() + o);
+            }
+    }
+    nod.clear();
+    con.clear();
+    // ---- prolongation tables (MatrixVectorHomogen.h:444-474 + addMultiLevelValues)
+    p.prol_tab.assign(nD * d, -1);
+    {
+        int64_t tot = 0;
+        for (int t = 0; t < nD; ++t)
+            for (int k = 0; k < d; ++k) {
+                std::vector<int32_t> T(p.D.begin() + t * d, p.D.begin() + (t + 1) * d);
+                T[k] += 1;
+                auto it = ids.find(T);
+                if (it == ids.end()) continue;
+                p.prol_tab[t * d + k] = tot;
+                tot += 2 * p.slabs[it->second].n;
+            }
+        p.prol.resize(tot);
+#pragma omp parallel for schedule(dynamic)
+        for (int tk = 0; tk < nD * d; ++tk) {
+            if (p.prol_tab[tk] < 0) continue;
+            int t = tk / d, k = tk % d;
+            std::vector<int32_t> T(p.D.begin() + t * d, p.D.begin() + (t + 1) * d);
+            Geometry gs(d, T.data());
+            T[k] += 1;
+            int tf = ids.at(T);
+            Geometry gf(d, T.data());
+            const Slab& sf = p.slabs[tf];
+            int32_t* tab = &p.prol[p.prol_tab[tk]];
+            int64_t c[kMaxDim];
+            for (int64_t e = 0; e < sf.n; ++e) {
+                gf.decode(p.slab_key[sf.off + e], c);
+                int64_t ck = c[k];
+                if (!(ck & 1)) {  // depth in dim k <= T_k: copy
+                    c[k] = ck / 2;
+                    int64_t at = slab_pos(p, t, gs, c);
+                    tab[2 * e] = (int32_t)at;
+                    tab[2 * e + 1] = -2;
+                } else {          // new point: 0.5 (right + left)
+                    int64_t top = gs.cext[k];
+                    int64_t l = (ck - 1) / 2, r = (ck + 1) / 2;
+                    c[k] = l;
+                    tab[2 * e] = (l > 0 && l < top) ? (int32_t)slab_pos(p, t, gs, c) : -1;
+                    c[k] = r;
+                    tab[2 * e + 1] = (r > 0 && r < top) ? (int32_t)slab_pos(p, t, gs, c) : -1;
+                }
+            }
+        }
+    }
+    // ---- per-case schedules
+    p.ncase = 1 << d;
+    p.sorted.resize(p.ncase);
+    {
+        std::vector<int32_t> T(d, 0);
+        for (int c = 0; c < p.ncase; ++c) {
+            std::vector<int32_t> out;
+            std::fill(T.begin(), T.end(), 0);
+            rec_depth(p, ids, c, true, d - 1, T, out);
+            p.sorted[c] = out;
+        }
+    }
+    p.p_slab_off.assign((size_t)p.ncase * nD, -1);
+    p.gm_slab_off.assign((size_t)p.ncase * nD, -1);
+    p.p_total = 0;
+    p.gm_total = 0;
+    std::map<std::tuple<int, int, int>, int64_t> restr_ids;  // (src, dst, dim) -> table offset
+    std::vector<std::tuple<int, int, int, int64_t>> restr_list;
+    int64_t restr_tot = 0;
+    struct Pend { int c, t, s; };
+    std::vector<std::vector<PhaseBItem>> blevels;
+    std::vector<std::vector<std::vector<PhaseBStep>>> bsteps;
+    int smax = 0;
+    for (int t = 0; t < nD; ++t) {
+        int s = 0;
+        for (int j = 0; j < d; ++j) s += p.D[t * d + j];
+        smax = std::max(smax, s);
+    }
+    blevels.assign(smax + 1, {});
+    bsteps.assign(smax + 1, {});
+    for (int c = 0; c < p.ncase; ++c) {
+        for (int t : p.sorted[c]) {
+            p.p_slab_off[(size_t)c * nD + t] = p.p_total;
+            p.p_total += p.slabs[t].n;
+        }
+        auto gm_of = [&](int t) {
+            int64_t& o = p.gm_slab_off[(size_t)c * nD + t];
+            if (o < 0) { o = p.gm_total; p.gm_total += p.slabs[t].n; }
+            return o;
+        };
+        for (int t : p.sorted[c]) {
+            const int32_t* T = &p.D[t * d];
+            int s = 0;
+            for (int j = 0; j < d; ++j)
+                if ((c >> j) & 1) s += T[j];
+            PhaseBItem it{};
+            it.c = c;
+            it.t = t;
+            it.p_off = p.p_slab_off[(size_t)c * nD + t];
+            it.gm_off = gm_of(t);
+            std::vector<PhaseBStep> steps;
+            std::vector<int32_t> Tc(T, T + d);
+            int cur = t;
+            bool final_ok = true;
+            for (int j = 0; j < d; ++j) {
+                if (!((c >> j) & 1)) continue;
+                Tc[j] -= 1;
+                auto f = ids.find(Tc);
+                if (f == ids.end()) { final_ok = false; continue; }
+                final_ok = true;
+                PhaseBStep st{};
+                st.t_dst = f->second;
+                st.dim = j;
+                auto key = std::make_tuple(cur, f->second, j);
+                auto rit = restr_ids.find(key);
+                if (rit == restr_ids.end()) {
+                    restr_ids[key] = restr_tot;
+                    restr_list.emplace_back(cur, f->second, j, restr_tot);
+                    st.tab_off = restr_tot;
+                    restr_tot += 3 * p.slabs[f->second].n;
+                } else st.tab_off = rit->second;
+                st.n_src = p.slabs[cur].n;
+                st.n_dst = p.slabs[f->second].n;
+                st.gm_off = gm_of(f->second);
+                steps.push_back(st);
+                cur = f->second;
+            }
+            it.t_conv = final_ok ? cur : -1;
+            if (it.t_conv >= 0 && !steps.empty() && cur != ids.at(Tc)) it.t_conv = -1;
+            blevels[s].push_back(it);
+            bsteps[s].push_back(steps);
+        }
+    }
+    // restriction tables: z'[q] = z[self] + 0.5 z[q - h e_k] + 0.5 z[q + h e_k]
+    p.restr.resize(restr_tot);
+#pragma omp parallel for schedule(dynamic)
+    for (size_t r = 0; r < restr_list.size(); ++r) {
+        int ts, td, k;
+        int64_t off;
+        std::tie(ts, td, k, off) = restr_list[r];
+        const Slab& ss = p.slabs[ts];
+        const Slab& sd = p.slabs[td];
+        Geometry gs(d, ss.T), gd(d, sd.T);
+        int32_t* tab = &p.restr[off];
+        int64_t c[kMaxDim], cs[kMaxDim];
+        for (int64_t e = 0; e < sd.n; ++e) {
+            gd.decode(p.slab_key[sd.off + e], c);
+            for (int j = 0; j < d; ++j) cs[j] = c[j] << (ss.T[j] - sd.T[j]);
+            tab[3 * e] = (int32_t)slab_pos(p, ts, gs, cs);
+            // neighbours at level Tdst_k + 1 in dim k, expressed at the source level
+            int sh = ss.T[k] - (sd.T[k] + 1);
+            int64_t base = (2 * c[k]);
+            int64_t top = gs.cext[k];
+            int64_t lpos = (base - 1) << sh, rpos = (base + 1) << sh;
+            cs[k] = lpos;
+            tab[3 * e + 1] = (lpos > 0 && lpos < top) ? (int32_t)slab_pos(p, ts, gs, cs) : -1;
+            cs[k] = rpos;
+            tab[3 * e + 2] = (rpos > 0 && rpos < top) ? (int32_t)slab_pos(p, ts, gs, cs) : -1;
+        }
+    }
+    // gM first-write flags, levels in descending restriction sum
+    {
+        std::vector<uint8_t> written((size_t)p.ncase * nD, 0);
+        p.b_level_off.clear();
+        int64_t scratch_max = 0;
+        for (int s = smax; s >= 0; --s) {
+            if (blevels[s].empty()) continue;
+            p.b_level_off.push_back((int32_t)p.b_items.size());
+            int64_t arena = 0;
+            std::vector<std::pair<size_t, int>> writes;
+            for (size_t i = 0; i < blevels[s].size(); ++i) {
+                PhaseBItem it = blevels[s][i];
+                it.gm_prev = written[(size_t)it.c * nD + it.t];
+                it.step_begin = (int32_t)p.b_steps.size();
+                int64_t scr = p.slabs[it.t].n;
+                for (PhaseBStep st : bsteps[s][i]) {
+                    st.gm_prev = written[(size_t)it.c * nD + st.t_dst];
+                    writes.emplace_back((size_t)it.c * nD + st.t_dst, 1);
+                    scr += st.n_dst;
+                    p.b_steps.push_back(st);
+                }
+                it.step_end = (int32_t)p.b_steps.size();
+                if (it.t_conv >= 0)
+                    for (int j = 1; j < d; ++j) scr += p.convert_dom[it.t_conv * (d + 1) + j];
+                it.scratch_off = arena;
+                arena += scr;
+                p.b_items.push_back(it);
+            }
+            for (auto& w : writes) written[w.first] = 1;
+            scratch_max = std::max(scratch_max, arena);
+        }
+        p.b_level_off.push_back((int32_t)p.b_items.size());
+        p.scratch_total = scratch_max;
+    }
+    // phase A: prolongation levels (dim k ascending, then T_k ascending)
+    p.a_level_off.clear();
+    for (int k = 0; k < d; ++k) {
+        for (int tv = 1; tv <= p.maxdep[k]; ++tv) {
+            size_t before = p.a_items.size();
+            for (int c = 0; c < p.ncase; ++c) {
+                if ((c >> k) & 1) continue;
+                for (int t : p.sorted[c]) {
+                    if (p.D[t * d + k] != tv) continue;
+                    int64_t tab = p.prol_tab[t * d + k];
+                    if (tab < 0) continue;
+                    std::vector<int32_t> T(p.D.begin() + t * d, p.D.begin() + (t + 1) * d);
+                    T[k] += 1;
+                    int tf = ids.at(T);
+                    PhaseAItem a{};
+                    a.c = c;
+                    a.t_src = t;
+                    a.t_dst = tf;
+                    a.dim = k;
+                    a.src_off = p.p_slab_off[(size_t)c * nD + t];
+                    a.dst_off = p.p_slab_off[(size_t)c * nD + tf];
+                    a.n_dst = p.slabs[tf].n;
+                    a.tab_off = tab;
+                    p.a_items.push_back(a);
+                }
+            }
+            if (p.a_items.size() > before) p.a_level_off.push_back((int32_t)before);
+        }
+    }
+    p.a_level_off.push_back((int32_t)p.a_items.size());
+    // nodal scratch: stage domains 1..d-1 of every depth
+    p.nodal_scratch = 0;
+    for (int t = 0; t < nD; ++t)
+        for (int j = 1; j < d; ++j) p.nodal_scratch += p.nodal_dom[t * (d + 1) + j];
+    p.plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return true;
+}
+
+}  // namespace lsg

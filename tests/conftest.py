@@ -1,0 +1,30 @@
+import glob
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); run with -m gpu")
+
+
+def load_golden(path):
+    z = np.load(path)
+    d = int(z["d"])
+    out = {k: z[k] for k in z.files}
+    out["points"] = z["points"].reshape(-1, d)
+    out["name"] = os.path.basename(path)[:-4]
+    return out
+
+
+@pytest.fixture(params=GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def golden(request):
+    return load_golden(request.param)
