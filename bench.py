@@ -1,0 +1,273 @@
+"""Benchmark: time to relative residual 1e-10 of the prewavelet stiffness solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference] [--workload NAME]
+
+One step = one solve of A x = f from x = 0 to ||f - A x|| / ||f|| <= 1e-10
+(FP32 matvec inside FP64 iterative refinement, Jacobi or learned diagonal
+preconditioner), inputs resident in HBM.  The JSON line also carries the plain
+FP64 CG time on the same instance, the matvec GB/s, the roofline of the
+restriction-wavefront kernel (the dominant one), the end-to-end time through
+the C-ABI with host buffers, and the reference's CPU time on a bounded sample.
+Multi-GPU runs (torchrun) solve one independent instance per rank (weak
+scaling, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-1e-10 residual: learned-precond FP32+IR vs plain FP64 CG; matvec GB/s"
+
+
+def workload(name, rank):
+    """Seeded synthetic instance: (grid, coefficient family, params, f, description)."""
+    import loadsg_b200 as lsg
+    rng = np.random.default_rng(1000 + rank)
+    if name.startswith("d6_regular_L"):
+        level = int(name.split("L")[1])
+        g = lsg.AdaptiveSparseGrid.regular(6, level)
+        c = rng.normal(0.0, 0.3, 6)
+        fam, params = lsg.COEF_EXPSIN, list(c)
+        desc = f"d=6 regular sparse grid level {level}, a=exp(sum_k c_k sin(k pi x_k)), c_k~N(0,0.3^2)"
+    elif name == "d3_regular_L7":
+        g = lsg.AdaptiveSparseGrid.regular(3, 7)
+        fam, params = lsg.COEF_SINPROD, [1.0, 0.5, 1.0, 1.0, 1.0]
+        desc = "d=3 regular sparse grid level 7, a=1+0.5 prod sin(pi x_i)"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    f = rng.uniform(-1.0, 1.0, g.n) * g.active
+    return g, fam, params, f, desc
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_reference_sample(args):
+    """The reference's own CG (oracle/_ref, compiled from the LoAdSG sources) on
+    the largest instance of the workload family it handles in seconds."""
+    d = 6 if args.workload.startswith("d6") else 3
+    exe = os.path.join(ROOT, "oracle", "_ref", f"d{d}", "ref_harness")
+    level = 3 if d == 6 else 5
+    if not os.path.exists(exe):
+        return {"value": None, "unit": "s", "cores": 0, "kind": "reference", "sample": f"{exe} missing"}
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    rng = np.random.default_rng(0)
+    with tempfile.TemporaryDirectory() as tmp:
+        subprocess.run([exe, "grid", tmp, f"level={level}"], check=True, capture_output=True, env=env)
+        n = int([l.split()[1] for l in open(os.path.join(tmp, "meta_grid.txt")) if l.startswith("N ")][0])
+        act = np.fromfile(os.path.join(tmp, "active.u8"), np.uint8)
+        f = rng.uniform(-1, 1, n) * act
+        f.tofile(os.path.join(tmp, "f.f64"))
+        coef = ["coef=2", "cp=" + ",".join(str(v) for v in rng.normal(0, 0.3, 6))] if d == 6 else \
+               ["coef=1", "cp=1,0.5,1,1,1"]
+        # eps on r^T D^-1 r chosen as 1e-20 * f^T D^-1 f ~ 1e-10 relative residual
+        t0 = time.perf_counter()
+        subprocess.run([exe, "cg", tmp, f"level={level}", f"f={tmp}/f.f64", "eps=1e-20"] + coef, check=True,
+                       capture_output=True, env=env)
+        wall = time.perf_counter() - t0
+        meta = dict(l.split()[:2] for l in open(os.path.join(tmp, "meta_cg.txt")) if len(l.split()) >= 2)
+    secs = float(meta.get("solve_seconds", wall))
+    return {"value": secs, "unit": "s", "cores": cores, "kind": "reference",
+            "sample": f"reference CG::solveHomogen (Jacobi) on d={d} regular level {level} (N={n}), "
+                      f"{meta.get('iterations')} iterations, rel.res {meta.get('relres')}; full workload infeasible "
+                      "for the reference (fixed hash capacities, O(N^2) grid completion)",
+            "per_dof_us": secs / n * 1e6}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--workload", default="d6_regular_L8")
+    ap.add_argument("--precond", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        res = cpu_reference_sample(args)
+        line = {"metric": METRIC, "value": res["value"], "unit": "s", "impl": "reference", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload}, "cpu_baseline": res,
+                "e2e": {"value": res["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import loadsg_b200 as lsg
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    g, fam, params, f_host, desc = workload(args.workload, rank)
+    prob = lsg.MidpointDiffusion(fam, params)
+    t0 = time.perf_counter()
+    m = lsg.MatrixVectorHomogen(g, prob)
+    setup_s = time.perf_counter() - t0
+    info = m.info()
+    dev = torch.device("cuda", local)
+    f = torch.tensor(f_host, dtype=torch.float64, device=dev)
+    x = torch.zeros(g.n, dtype=torch.float64, device=dev)
+
+    def opts(precision, precond):
+        return lsg.SolverOpts(1e-10, 1, 20000, precond, precision, 40, 1e-3, 1)
+
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def solve(precision, precond):
+        x.zero_()
+        return lsg.CG.solve_device(m, f.data_ptr(), x.data_ptr(), opts(precision, precond), stream)
+
+    for _ in range(args.warmup):
+        rep = solve(lsg.FP32, args.precond)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            reps.append(solve(lsg.FP32, args.precond))
+        ev1.record()
+        torch.cuda.synchronize()
+    step_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
+    if dist:
+        t = torch.tensor([step_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_s = float(t.item())
+
+    # plain FP64 CG on the same instance (the comparison the metric names)
+    rep64 = solve(lsg.FP64, 0)
+    # end to end through the C-ABI with host buffers
+    xh = np.zeros(g.n)
+    torch.cuda.synchronize()
+    te = time.perf_counter()
+    for _ in range(args.steps):
+        xh[:] = 0.0
+        lsg.CG.solveHomogen(1e-10, xh, f_host, m, prob, criterion=1, precision=lsg.FP32, max_iter=20000,
+                            precond=args.precond, inner_iter=40, inner_tol=1e-3)
+    e2e_s = (time.perf_counter() - te) / args.steps
+
+    # matvec bandwidth and the phase-B roofline (CUDA events inside the library)
+    x32 = torch.randn(g.n, dtype=torch.float32, device=dev)
+    y32 = torch.zeros(g.n, dtype=torch.float32, device=dev)
+    x64 = x32.double()
+    y64 = torch.zeros(g.n, dtype=torch.float64, device=dev)
+    m.profile(x32.data_ptr(), y32.data_ptr(), lsg.FP32, 2)
+    ms32, by32, flops = m.profile(x32.data_ptr(), y32.data_ptr(), lsg.FP32, 5)
+    ms64, by64, _ = m.profile(x64.data_ptr(), y64.data_ptr(), lsg.FP64, 3)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        hbm, peak_src = 6650.0, "fallback"
+    achieved = by32[3] / (ms32[3] * 1e-3) / 1e9
+
+    if rank != 0:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    cpu = None if args.no_cpu_baseline or world > 1 else cpu_reference_sample(args)
+    line = {
+        "metric": METRIC, "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 matvec / f64 refinement", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc, "n_points": g.n, "n_active": g.getDOFS(),
+                   "tolerance": 1e-10, "precond": ["jacobi", "none", "learned"][args.precond],
+                   "parallelism": f"replicas x{world}", "l2": "working set larger than L2 (126 MB)"},
+        "iterations": reps[-1]["iterations"], "outer_iterations": reps[-1]["outer_iterations"],
+        "rel_residual": reps[-1]["rel_residual"],
+        "fp64_cg": {"seconds": rep64["seconds"], "iterations": rep64["iterations"],
+                    "rel_residual": rep64["rel_residual"]},
+        "speedup_vs_fp64_cg": rep64["seconds"] / step_s if step_s > 0 else None,
+        "matvec": {"fp32_ms": ms32[4], "fp64_ms": ms64[4], "fp32_gbs": by32[4] / (ms32[4] * 1e-3) / 1e9,
+                   "fp64_gbs": by64[4] / (ms64[4] * 1e-3) / 1e9, "phase_ms_fp32": list(ms32[:4]),
+                   "cell_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9},
+        "roofline": {"bound": "hbm", "kernel": "k_phaseB (restriction wavefronts + cell operator)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": peak_src, "traffic": None},
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16 * g.n, "d2h_bytes_per_step": 8 * g.n},
+        "setup_seconds": setup_s, "plan_seconds": info["plan_seconds"], "device_bytes": info["device_bytes"],
+        "clocks": clk.summary(),
+        "gpu_launches": int(sum(r["kernel_launches"] for r in reps)),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

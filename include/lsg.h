@@ -80,6 +80,14 @@ int lsg_matvec(lsg_operator *op, const double *x, double *y);
  * LSG_FP32), enqueued on `stream` (a cudaStream_t, 0 = legacy default). */
 int lsg_matvec_device(lsg_operator *op, const void *x, void *y, int32_t precision, void *stream);
 
+/* Times `iters` matvecs on device buffers with CUDA events between the
+ * phases; phase_ms[0..3] = mean ms of (nodal transform, P init, prolongation
+ * levels, restriction wavefronts incl. the cell operator), phase_ms[4] = whole
+ * matvec.  bytes[0..4] = algorithmic bytes of the same phases for this
+ * precision (see the design notes); flops = cell-operator flops per matvec. */
+int lsg_matvec_profile(lsg_operator *op, const void *x, void *y, int32_t precision, int32_t iters, double *phase_ms,
+                       double *bytes, double *flops);
+
 /* Exact Jacobi diagonal a(psi_i, psi_i) at active points (0 at hanging), as
  * Preconditioning::precondLocalStiffnessMatrix (applications/cg_method.h:544-680). */
 int lsg_diag(lsg_operator *op, double *diag);
@@ -104,6 +112,7 @@ typedef struct {
     double seconds;          /* device time of the solve */
     int32_t converged;
     int32_t fell_back;       /* learned preconditioner stalled -> Jacobi */
+    int64_t kernel_launches; /* kernels of this library launched by the solve */
 } lsg_solve_report;
 
 /* Solves A x = f (CG::solveHomogen, applications/cg_method.h:27-33,759-886).

@@ -71,6 +71,7 @@ class SolveReport(ctypes.Structure):
         ("seconds", ctypes.c_double),
         ("converged", ctypes.c_int32),
         ("fell_back", ctypes.c_int32),
+        ("kernel_launches", ctypes.c_int64),
     ]
 
 
@@ -90,6 +91,7 @@ def lib():
             "lsg_matvec": (ctypes.c_int, [P, P, P]),
             "lsg_matvec_device": (ctypes.c_int, [P, P, P, I32, P]),
             "lsg_diag": (ctypes.c_int, [P, P]),
+            "lsg_matvec_profile": (ctypes.c_int, [P, P, P, I32, I32, P, P, P]),
             "lsg_diag_device": (ctypes.c_int, [P, P, P]),
             "lsg_cg_solve": (ctypes.c_int, [P, P, P, P, P]),
             "lsg_cg_solve_device": (ctypes.c_int, [P, P, P, P, P, P]),
@@ -283,6 +285,17 @@ class MatrixVectorHomogen:
         """Device-pointer variant (torch tensors: pass t.data_ptr())."""
         _check(lib().lsg_matvec_device(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), precision,
                                        ctypes.c_void_p(stream)))
+
+    def profile(self, x_ptr, y_ptr, precision=FP32, iters=5):
+        """Mean ms per matvec phase (nodal, P init, prolongation, restriction
+        wavefronts with the cell operator, total) plus algorithmic bytes per
+        phase and cell-operator flops."""
+        ms = np.zeros(5)
+        by = np.zeros(5)
+        fl = np.zeros(1)
+        _check(lib().lsg_matvec_profile(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), precision, iters,
+                                        _ptr(ms), _ptr(by), _ptr(fl)))
+        return ms, by, float(fl[0])
 
     def diagonal(self, problem):
         """Exact Jacobi diagonal (Preconditioning::precondLocalStiffnessMatrix)."""

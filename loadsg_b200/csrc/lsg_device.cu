@@ -154,71 +154,143 @@ __global__ void k_prolong(DevPlan P, V* __restrict__ pc, int32_t item0) {
     }
 }
 
-// ----------------------------------------------------------------------------- cell operator
-// Corner positions of one level-T cell (bit k of the corner id = right side in dim k).
+// ----------------------------------------------------------------------------- cell operator, lane groups
+// A cell's 2^D corner values are spread over a group of G = 2^(D-DL) lanes:
+// lane g of the group holds the NL = 2^DL corners whose high bits (dims
+// DL..D-1) equal g.  The Walsh-Hadamard butterflies of dims < DL are
+// register-local, those of dims >= DL use warp shuffles inside the group.
 template <int D>
-__device__ __forceinline__ void cell_corners(const DevPlan& P, const DevSlab& s, int64_t ci, int32_t* pos) {
-    constexpr int NC = 1 << D;
-    if (!s.dense) {
-        const int32_t* c = P.cell_corner + ((s.corner_off + ci) << D);
+struct CellCfg {
+    static constexpr int DL = D <= 4 ? D : 4;
+    static constexpr int G = 1 << (D - DL);
+    static constexpr int NL = 1 << DL;
+    static constexpr int NH = NL / 2;  // corners per dim-0 face held by one lane
+};
+
+template <int D, typename V>
+__device__ __forceinline__ void wht_group(V* v, int g) {
+    constexpr int DL = CellCfg<D>::DL, NL = CellCfg<D>::NL;
 #pragma unroll
-        for (int b = 0; b < NC; ++b) pos[b] = c[b];
-        return;
-    }
-    const int32_t BAD = -(1 << 27);
-    pos[0] = 0;
+    for (int k = 0; k < DL; ++k)
 #pragma unroll
-    for (int k = 0; k < D; ++k) {
-        int32_t cext = s.ext[k] + 1;
-        int32_t m = (int32_t)(ci % cext);
-        ci /= cext;
-        int32_t lo = (m >= 1) ? (m - 1) * s.stride[k] : BAD;
-        int32_t hi = (m + 1 <= s.ext[k]) ? m * s.stride[k] : BAD;
+        for (int b = 0; b < NL; ++b)
+            if (!(b & (1 << k))) {
+                V p = v[b], q = v[b | (1 << k)];
+                v[b] = p + q;
+                v[b | (1 << k)] = p - q;
+            }
 #pragma unroll
-        for (int b = 0; b < (1 << k); ++b) {
-            pos[b | (1 << k)] = pos[b] + hi;
-            pos[b] = pos[b] + lo;
+    for (int k = DL; k < D; ++k) {
+        int m = 1 << (k - DL);
+        bool hi = (g & m) != 0;
+#pragma unroll
+        for (int b = 0; b < NL; ++b) {
+            V p = __shfl_xor_sync(0xffffffffu, v[b], m);
+            v[b] = hi ? p - v[b] : v[b] + p;
         }
     }
 }
 
-// z += a_c K_ref u on the corners of one cell.  K_ref = H diag(lam) H with H the
-// d-fold Hadamard transform: the exact Q1 stiffness sum_i K1_i (x) M1_others is
-// diagonal in the basis (1,1),(1,-1) of every dimension.
-template <int D, typename V, bool SHARED_ATOMIC>
-__device__ __forceinline__ void apply_cell(const int32_t* pos, const V* __restrict__ u, V* z, V a, const V* lam) {
-    constexpr int NC = 1 << D;
-    V v[NC];
+// z += sum over the slab's cells of a_c H diag(lam) H u_c.  Dense slab: the
+// group walks one column of cells along dim 0 and carries the shared face, so
+// each node of the column is gathered and scattered once per column.
+// All lanes of a warp run the same number of rounds (shuffles need them).
+template <int D, typename V>
+__device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, const V* __restrict__ ac, const V* lamg) {
+    constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NL = CellCfg<D>::NL, NH = CellCfg<D>::NH;
+    const int g = threadIdx.x & (G - 1);
+    const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
+    const int32_t c0 = s.ext[0] + 1;  // cells along dim 0
+    const int64_t ncols = s.ncell / c0;
+    const int64_t rounds = (ncols + ngroups - 1) / ngroups;
+    for (int64_t r = 0; r < rounds; ++r) {
+        int64_t col = r * ngroups + group;
+        bool live = col < ncols;
+        // min corner of the column in dims 1..D-1
+        int32_t m[D];
+        int64_t rem = live ? col : 0;
 #pragma unroll
-    for (int b = 0; b < NC; ++b) v[b] = pos[b] >= 0 ? u[pos[b]] : V(0);
+        for (int k = 1; k < D; ++k) {
+            int32_t ck = s.ext[k] + 1;
+            m[k] = (int32_t)(rem % ck);
+            rem /= ck;
+        }
+        int32_t off[NH];
+        bool ok[NH];
 #pragma unroll
-    for (int k = 0; k < D; ++k)
+        for (int j = 0; j < NH; ++j) {
+            int32_t o = 0;
+            bool good = live;
 #pragma unroll
-        for (int b = 0; b < NC; ++b)
-            if (!(b & (1 << k))) {
-                V p = v[b], q = v[b | (1 << k)];
-                v[b] = p + q;
-                v[b | (1 << k)] = p - q;
+            for (int k = 1; k < D; ++k) {
+                int bit = k < DL ? (j >> (k - 1)) & 1 : (g >> (k - DL)) & 1;
+                int32_t c = m[k] + bit;
+                good = good && c >= 1 && c <= s.ext[k];
+                o += (c - 1) * s.stride[k];
             }
+            off[j] = o;
+            ok[j] = good;
+        }
+        V uc[NH], vc[NH];
 #pragma unroll
-    for (int b = 0; b < NC; ++b) v[b] *= a * lam[b];
+        for (int j = 0; j < NH; ++j) { uc[j] = V(0); vc[j] = V(0); }
+        const V* acol = ac + col * c0;
+        for (int32_t m0 = 0; m0 < c0; ++m0) {
+            V v[NL];
+            bool rin = m0 + 1 <= s.ext[0];
 #pragma unroll
-    for (int k = 0; k < D; ++k)
-#pragma unroll
-        for (int b = 0; b < NC; ++b)
-            if (!(b & (1 << k))) {
-                V p = v[b], q = v[b | (1 << k)];
-                v[b] = p + q;
-                v[b | (1 << k)] = p - q;
+            for (int j = 0; j < NH; ++j) {
+                v[2 * j] = uc[j];
+                V x = (ok[j] && rin) ? u[off[j] + m0] : V(0);
+                v[2 * j + 1] = x;
+                uc[j] = x;
             }
+            wht_group<D, V>(v, g);
+            V a = live ? acol[m0] : V(0);
 #pragma unroll
-    for (int b = 0; b < NC; ++b)
-        if (pos[b] >= 0) atomicAdd(&z[pos[b]], v[b]);
+            for (int b = 0; b < NL; ++b) v[b] *= a * lamg[b];
+            wht_group<D, V>(v, g);
+#pragma unroll
+            for (int j = 0; j < NH; ++j) {
+                if (ok[j] && m0 >= 1) atomicAdd(&z[off[j] + m0 - 1], v[2 * j] + vc[j]);
+                vc[j] = v[2 * j + 1];
+            }
+        }
+    }
+}
+
+template <int D, typename V>
+__device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __restrict__ u, V* z,
+                             const V* __restrict__ ac, const V* lamg) {
+    constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NL = CellCfg<D>::NL;
+    const int g = threadIdx.x & (G - 1);
+    const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
+    const int64_t rounds = (s.ncell + ngroups - 1) / ngroups;
+    for (int64_t r = 0; r < rounds; ++r) {
+        int64_t ci = r * ngroups + group;
+        bool live = ci < s.ncell;
+        const int32_t* cp = P.cell_corner + ((s.corner_off + (live ? ci : 0)) << D) + (g << DL);
+        int32_t pos[NL];
+        V v[NL];
+#pragma unroll
+        for (int b = 0; b < NL; ++b) {
+            pos[b] = live ? cp[b] : -1;
+            v[b] = pos[b] >= 0 ? u[pos[b]] : V(0);
+        }
+        wht_group<D, V>(v, g);
+        V a = live ? ac[ci] : V(0);
+#pragma unroll
+        for (int b = 0; b < NL; ++b) v[b] *= a * lamg[b];
+        wht_group<D, V>(v, g);
+#pragma unroll
+        for (int b = 0; b < NL; ++b)
+            if (pos[b] >= 0) atomicAdd(&z[pos[b]], v[b]);
+    }
 }
 
 // ----------------------------------------------------------------------------- phase B item
 template <int D, typename V>
-__global__ void __launch_bounds__(256) k_phaseB(DevPlan P, const V* __restrict__ pc, V* __restrict__ gm,
+__global__ void __launch_bounds__(256, 2) k_phaseB(DevPlan P, const V* __restrict__ pc, V* __restrict__ gm,
                                                  V* __restrict__ scratch, V* __restrict__ y,
                                                  const V* __restrict__ acell, const V* __restrict__ lam_all,
                                                  int32_t item0, int64_t smem_cap) {
@@ -228,6 +300,8 @@ __global__ void __launch_bounds__(256) k_phaseB(DevPlan P, const V* __restrict__
     const DevSlab& s = P.slabs[it.t];
     V* lam = reinterpret_cast<V*>(smem_raw);
     for (int b = threadIdx.x; b < NC; b += blockDim.x) lam[b] = lam_all[(int64_t)it.t * NC + b];
+    // this lane's Hadamard-basis eigenvalues (high bits = lane position in its group)
+    const V* lamg = lam + ((threadIdx.x & (CellCfg<D>::G - 1)) << CellCfg<D>::DL);
     V* scr = scratch + it.scratch_off;
     const V* u_g = pc + it.p_off;
     const V* ac = acell + s.cell_off;
@@ -240,22 +314,16 @@ __global__ void __launch_bounds__(256) k_phaseB(DevPlan P, const V* __restrict__
             z[e] = V(0);
         }
         __syncthreads();
-        int32_t pos[NC];
-        for (int64_t ci = threadIdx.x; ci < s.ncell; ci += blockDim.x) {
-            cell_corners<D>(P, s, ci, pos);
-            apply_cell<D, V, true>(pos, u, z, ac[ci], lam);
-        }
+        if (s.dense) cells_dense<D, V>(s, u, z, ac, lamg);
+        else cells_sparse<D, V>(P, s, u, z, ac, lamg);
         __syncthreads();
         const V* g0 = gm + it.gm_off;
         for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) scr[e] = it.gm_prev ? z[e] + g0[e] : z[e];
     } else {
         for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) scr[e] = V(0);
         __syncthreads();
-        int32_t pos[NC];
-        for (int64_t ci = threadIdx.x; ci < s.ncell; ci += blockDim.x) {
-            cell_corners<D>(P, s, ci, pos);
-            apply_cell<D, V, false>(pos, u_g, scr, ac[ci], lam);
-        }
+        if (s.dense) cells_dense<D, V>(s, u_g, scr, ac, lamg);
+        else cells_sparse<D, V>(P, s, u_g, scr, ac, lamg);
         __syncthreads();
         if (it.gm_prev) {
             const V* g0 = gm + it.gm_off;
@@ -718,7 +786,7 @@ int set_phaseB_smem() {
 
 // The matvec: a fixed sequence of launches on one stream.
 template <int D, typename V>
-int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st) {
+int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t* ev = nullptr) {
     const lsg::Plan& p = op->plan;
     lsg_operator::Work& w = std::is_same<V, double>::value ? op->w64 : op->w32;
     int rc = ensure_work<V>(op, w);
@@ -728,14 +796,18 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st) {
     const V* acell = std::is_same<V, double>::value ? (const V*)op->acell64.p : (const V*)op->acell32.p;
     const V* lam = std::is_same<V, double>::value ? (const V*)op->lam64.p : (const V*)op->lam32.p;
     int64_t na = p.exa_off[p.nD];
+    if (ev) cudaEventRecord(ev[0], st);
     if (na > 0) k_zero_active<V><<<nblk(na), 256, 0, st>>>(op->dp.exa, na, y);
     k_nodal<V><<<p.nD, 256, 0, st>>>(op->dp, x, w.ml.as<V>(), w.nscratch.as<V>());
+    if (ev) cudaEventRecord(ev[1], st);
     int32_t nb = (int32_t)p.b_items.size();
     if (nb > 0) k_pinit<V><<<nb, 256, 0, st>>>(op->dp, w.ml.as<V>(), w.pc.as<V>(), 0);
+    if (ev) cudaEventRecord(ev[2], st);
     for (size_t L = 0; L + 1 < p.a_level_off.size(); ++L) {
         int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
         if (e > b) k_prolong<V><<<e - b, 256, 0, st>>>(op->dp, w.pc.as<V>(), b);
     }
+    if (ev) cudaEventRecord(ev[3], st);
     const int64_t cap_elems = (200 * 1024) / sizeof(V) - (1 << D);
     for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
         int32_t b = p.b_level_off[L], e = p.b_level_off[L + 1];
@@ -746,21 +818,46 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st) {
         k_phaseB<D, V><<<e - b, 256, smem, st>>>(op->dp, w.pc.as<V>(), w.gm.as<V>(), w.scratch.as<V>(), y, acell, lam, b,
                                                  alloc_elems);
     }
+    if (ev) cudaEventRecord(ev[4], st);
     CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
+template <int D, typename V>
+int prepare_impl(lsg_operator* op) {
+    lsg_operator::Work& w = std::is_same<V, double>::value ? op->w64 : op->w32;
+    int rc = ensure_work<V>(op, w);
+    if (rc) return rc;
+    return set_phaseB_smem<D, V>();
+}
+
+// allocations and function attributes that must not happen during graph capture
 template <typename V>
-int matvec_dispatch(lsg_operator* op, const V* x, V* y, cudaStream_t st) {
+int prepare(lsg_operator* op) {
     switch (op->plan.d) {
-    case 1: return matvec_impl<1, V>(op, x, y, st);
-    case 2: return matvec_impl<2, V>(op, x, y, st);
-    case 3: return matvec_impl<3, V>(op, x, y, st);
-    case 4: return matvec_impl<4, V>(op, x, y, st);
-    case 5: return matvec_impl<5, V>(op, x, y, st);
-    case 6: return matvec_impl<6, V>(op, x, y, st);
-    case 7: return matvec_impl<7, V>(op, x, y, st);
-    case 8: return matvec_impl<8, V>(op, x, y, st);
+    case 1: return prepare_impl<1, V>(op);
+    case 2: return prepare_impl<2, V>(op);
+    case 3: return prepare_impl<3, V>(op);
+    case 4: return prepare_impl<4, V>(op);
+    case 5: return prepare_impl<5, V>(op);
+    case 6: return prepare_impl<6, V>(op);
+    case 7: return prepare_impl<7, V>(op);
+    case 8: return prepare_impl<8, V>(op);
+    }
+    return fail(LSG_E_INVALID, "unsupported dimension");
+}
+
+template <typename V>
+int matvec_dispatch(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+    switch (op->plan.d) {
+    case 1: return matvec_impl<1, V>(op, x, y, st, ev);
+    case 2: return matvec_impl<2, V>(op, x, y, st, ev);
+    case 3: return matvec_impl<3, V>(op, x, y, st, ev);
+    case 4: return matvec_impl<4, V>(op, x, y, st, ev);
+    case 5: return matvec_impl<5, V>(op, x, y, st, ev);
+    case 6: return matvec_impl<6, V>(op, x, y, st, ev);
+    case 7: return matvec_impl<7, V>(op, x, y, st, ev);
+    case 8: return matvec_impl<8, V>(op, x, y, st, ev);
     }
     return fail(LSG_E_INVALID, "unsupported dimension");
 }
@@ -885,6 +982,74 @@ int lsg_matvec_device(lsg_operator* op, const void* x, void* y, int32_t precisio
     if (precision == LSG_FP64) return matvec_dispatch<double>(op, (const double*)x, (double*)y, st);
     if (precision == LSG_FP32) return matvec_dispatch<float>(op, (const float*)x, (float*)y, st);
     return fail(LSG_E_INVALID, "precision must be LSG_FP64 or LSG_FP32");
+}
+
+// Algorithmic bytes per phase of one matvec (value size sv): every array the
+// phase must touch, counted once per item that touches it.
+static int64_t matvec_launches(const lsg::Plan& p) {
+    return 3 + (int64_t)(p.a_level_off.size() - 1) + (int64_t)(p.b_level_off.size() - 1);
+}
+
+static void phase_bytes(const lsg::Plan& p, double sv, double* b) {
+    int d = p.d;
+    double nodal = sv * (double)p.exa_off[p.nD] + sv * (double)p.M;  // x gathered, nodal slabs written
+    for (size_t i = 0; i < p.nodal.code.size(); ++i) nodal += 4.0 * (1 + p.nodal.nsrc);  // stage tables
+    double pinit = 0, prol = 0, phb = 0;
+    for (const auto& it : p.b_items) pinit += 2.0 * sv * p.slabs[it.t].n;
+    for (const auto& a : p.a_items) prol += a.n_dst * (3.0 * sv + 8.0) + sv * p.slabs[a.t_src].n;
+    for (const auto& it : p.b_items) {
+        const lsg::Slab& s = p.slabs[it.t];
+        phb += sv * s.n * (it.gm_prev ? 3.0 : 2.0);            // P read, z written (+ gM read)
+        phb += sv * s.ncell;                                    // cell coefficient
+        if (!s.dense) phb += 4.0 * (1 << d) * s.ncell;          // corner table
+        for (int32_t k = it.step_begin; k < it.step_end; ++k) {
+            const lsg::PhaseBStep& st = p.b_steps[k];
+            phb += st.n_dst * (12.0 + sv * (st.gm_prev ? 3.0 : 2.0)) + sv * st.n_src;
+        }
+        if (it.t_conv >= 0) {
+            const int64_t* dom = &p.convert_dom[it.t_conv * (d + 1)];
+            for (int j = 1; j <= d; ++j) phb += dom[j] * (24.0 + sv);
+            phb += sv * dom[d];                                 // y update
+        }
+    }
+    b[0] = nodal;
+    b[1] = pinit;
+    b[2] = prol;
+    b[3] = phb;
+    b[4] = nodal + pinit + prol + phb;
+}
+
+int lsg_matvec_profile(lsg_operator* op, const void* x, void* y, int32_t precision, int32_t iters, double* phase_ms,
+                       double* bytes, double* flops) {
+    if (!op || !x || !y || !phase_ms || iters < 1) return fail(LSG_E_INVALID, "bad argument");
+    if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
+    cudaEvent_t ev[5];
+    for (auto& e : ev) cudaEventCreate(&e);
+    double acc[5] = {0, 0, 0, 0, 0};
+    int rc = 0;
+    for (int i = 0; i < iters && !rc; ++i) {
+        rc = precision == LSG_FP64 ? matvec_dispatch<double>(op, (const double*)x, (double*)y, nullptr, ev)
+                                   : matvec_dispatch<float>(op, (const float*)x, (float*)y, nullptr, ev);
+        if (rc) break;
+        cudaEventSynchronize(ev[4]);
+        float ms;
+        for (int k = 0; k < 4; ++k) {
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            acc[k] += ms;
+        }
+        cudaEventElapsedTime(&ms, ev[0], ev[4]);
+        acc[4] += ms;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    for (int k = 0; k < 5; ++k) phase_ms[k] = acc[k] / iters;
+    if (bytes) phase_bytes(op->plan, precision == LSG_FP64 ? 8.0 : 4.0, bytes);
+    if (flops) {
+        int64_t cc = 0;
+        for (const auto& it : op->plan.b_items) cc += op->plan.slabs[it.t].ncell;
+        *flops = (double)cc * ((2.0 * op->plan.d + 1.0) * (1 << op->plan.d));
+    }
+    return 0;
 }
 
 int lsg_matvec(lsg_operator* op, const double* x, double* y) {
@@ -1177,7 +1342,7 @@ int cg_body(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, bool want_rr, c
 // h, d, s[0], s[3] the start state.  Returns iterations in *its.
 template <typename V>
 int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int crit, double rr_stop, int maxit,
-            bool use_graph, cudaStream_t st, int* its, double* last_rr) {
+            bool use_graph, cudaStream_t st, int* its, double* last_rr, int64_t* launches) {
     cudaGraphExec_t exec = nullptr;
     bool want_rr = crit == 1;
     int it = 0;
@@ -1193,6 +1358,10 @@ int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return fail(LSG_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     }
+    // loop condition of the first iteration (delta > eps, or the residual test)
+    CUDA_TRY(cudaMemcpyAsync(S.pin.h, S.s.as<double>(), 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if ((crit == 0 && !(S.pin.h[0] > eps)) || (crit == 1 && S.pin.h[5] <= rr_stop)) maxit = 0;
     for (int i = 1; i <= maxit; ++i) {
         if (use_graph) {
             cudaError_t e = cudaGraphLaunch(exec, st);
@@ -1207,11 +1376,14 @@ int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int
         double dn = S.pin.h[3];
         if (want_rr) *last_rr = S.pin.h[5];
         if (!std::isfinite(dn)) break;
-        if (crit == 0 && dn < eps * eps) break;
+        // reference: break when delta' < eps^2, and the loop runs while delta > eps
+        // (cg_method.h:852,871) -- so it ends as soon as delta' <= eps as well
+        if (crit == 0 && (dn < eps * eps || dn <= eps)) break;
         if (crit == 1 && S.pin.h[5] <= rr_stop) break;
     }
     if (exec) cudaGraphExecDestroy(exec);
     *its = it;
+    *launches += (int64_t)it * (matvec_launches(S.op->plan) + 9 + (want_rr ? 2 : 0));
     return rc;
 }
 
@@ -1230,6 +1402,8 @@ int cg_start(Solver& S, const V* f, V* x, V* r, V* d, V* h, const V* z, cudaStre
     k_dot_partial<V, V><<<kRedBlocks, kRedThreads, 0, st>>>(r, h, n, S.part.as<double>());
     k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, s + 0);
     CUDA_TRY(cudaMemcpyAsync(s + 3, s + 0, sizeof(double), cudaMemcpyDeviceToDevice, st));
+    k_dot_partial<V, V><<<kRedBlocks, kRedThreads, 0, st>>>(r, r, n, S.part.as<double>());
+    k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, s + 5);
     CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -1261,6 +1435,8 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
     lsg_solve_report R;
     memset(&R, 0, sizeof R);
     int rc = solver_init(S, o->precision == LSG_FP32);
+    if (!rc) rc = prepare<double>(op);
+    if (!rc && o->precision == LSG_FP32) rc = prepare<float>(op);
     const double* zdiag = nullptr;
     if (!rc && o->precond == 0) { rc = compute_diag(op, st); zdiag = op->diag.as<double>(); }
     if (!rc && o->precond == 2) {
@@ -1277,7 +1453,8 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
         double rr = 0.0;
         if (!rc)
             rc = cg_loop<double>(S, x, S.r.as<double>(), S.g.as<double>(), S.d.as<double>(), S.h.as<double>(), zdiag, eps,
-                                 o->criterion, eps * eps * ff, maxit, o->use_graph != 0, st, &its, &rr);
+                                 o->criterion, eps * eps * ff, maxit, o->use_graph != 0, st, &its, &rr,
+                                 &R.kernel_launches);
         R.iterations = its;
         R.outer_iterations = 1;
     } else if (!rc) {
@@ -1314,10 +1491,13 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             k_dot_partial<float, float><<<kRedBlocks, kRedThreads, 0, st>>>(r32, h32, n, S.part.as<double>());
             k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, s + 0);
             cudaMemcpyAsync(s + 3, s + 0, 8, cudaMemcpyDeviceToDevice, st);
+            k_dot_partial<float, float><<<kRedBlocks, kRedThreads, 0, st>>>(r32, r32, n, S.part.as<double>());
+            k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, s + 5);
             int its = 0;
             double lrr = 0.0;
             rc = cg_loop<float>(S, e32, r32, S.g32.as<float>(), d32, h32, z32, 0.0, 1, itol * itol, inner,
-                                o->use_graph != 0, st, &its, &lrr);
+                                o->use_graph != 0, st, &its, &lrr, &R.kernel_launches);
+            R.kernel_launches += matvec_launches(op->plan) + 12;
             if (rc) break;
             total += its;
             k_axpy_f32<<<nblk(n), 256, 0, st>>>(n, nr, e32, x);
