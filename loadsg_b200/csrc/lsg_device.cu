@@ -182,31 +182,63 @@ __device__ __forceinline__ void wht_group(V* v, int g) {
 #pragma unroll
     for (int k = DL; k < D; ++k) {
         int m = 1 << (k - DL);
-        bool hi = (g & m) != 0;
+        V sgn = (g & m) ? V(-1) : V(1);  // low lane: v + p, high lane: p - v
 #pragma unroll
         for (int b = 0; b < NL; ++b) {
             V p = __shfl_xor_sync(0xffffffffu, v[b], m);
-            v[b] = hi ? p - v[b] : v[b] + p;
+            v[b] = fma(sgn, v[b], p);
         }
     }
 }
 
-// z += sum over the slab's cells of a_c H diag(lam) H u_c.  Dense slab: the
-// group walks one column of cells along dim 0 and carries the shared face, so
-// each node of the column is gathered and scattered once per column.
+// Hadamard butterflies over dims 1..D-1 of one dim-0 face: NH values per lane,
+// local dims 1..DL-1 (bit k-1 of the local index), dims DL..D-1 across lanes.
+template <int D, typename V>
+__device__ __forceinline__ void wht_face(V* v, int g) {
+    constexpr int DL = CellCfg<D>::DL, NH = CellCfg<D>::NH;
+#pragma unroll
+    for (int k = 0; k < DL - 1; ++k)
+#pragma unroll
+        for (int b = 0; b < NH; ++b)
+            if (!(b & (1 << k))) {
+                V p = v[b], q = v[b | (1 << k)];
+                v[b] = p + q;
+                v[b | (1 << k)] = p - q;
+            }
+#pragma unroll
+    for (int k = DL; k < D; ++k) {
+        int m = 1 << (k - DL);
+        V sgn = (g & m) ? V(-1) : V(1);
+#pragma unroll
+        for (int b = 0; b < NH; ++b) {
+            V p = __shfl_xor_sync(0xffffffffu, v[b], m);
+            v[b] = fma(sgn, v[b], p);
+        }
+    }
+}
+
+// z += sum over the slab's cells of a_c H diag(lam) H u_c on a dense slab.
+// A lane group walks one column of cells along dim 0.  The Hadamard transform
+// factorises as H = H_0 (x) H_rest; the H_rest transform of a face is shared
+// by the two cells on either side of it, so per cell only the new (right)
+// face is transformed forward, and the left-face outputs of this cell and
+// the right-face outputs of the previous one are summed before one inverse
+// H_rest.  Faces on the boundary (m0 = 0 left, m0 = 2^T_0 - 1 right) drop out.
 // All lanes of a warp run the same number of rounds (shuffles need them).
 template <int D, typename V>
 __device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, const V* __restrict__ ac, const V* lamg) {
-    constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NL = CellCfg<D>::NL, NH = CellCfg<D>::NH;
+    constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NH = CellCfg<D>::NH;
     const int g = threadIdx.x & (G - 1);
     const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
     const int32_t c0 = s.ext[0] + 1;  // cells along dim 0
     const int64_t ncols = s.ncell / c0;
     const int64_t rounds = (ncols + ngroups - 1) / ngroups;
+    V lp[NH], lm[NH];  // eigenvalues for s_0 = + (bit 0 clear) and s_0 = - (bit 0 set)
+#pragma unroll
+    for (int j = 0; j < NH; ++j) { lp[j] = lamg[2 * j]; lm[j] = lamg[2 * j + 1]; }
     for (int64_t r = 0; r < rounds; ++r) {
         int64_t col = r * ngroups + group;
         bool live = col < ncols;
-        // min corner of the column in dims 1..D-1
         int32_t m[D];
         int64_t rem = live ? col : 0;
 #pragma unroll
@@ -231,30 +263,30 @@ __device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, con
             off[j] = o;
             ok[j] = good;
         }
-        V uc[NH], vc[NH];
+        V lh[NH], cr[NH];  // transformed left face, carried right-face output
 #pragma unroll
-        for (int j = 0; j < NH; ++j) { uc[j] = V(0); vc[j] = V(0); }
+        for (int j = 0; j < NH; ++j) { lh[j] = V(0); cr[j] = V(0); }
         const V* acol = ac + col * c0;
         for (int32_t m0 = 0; m0 < c0; ++m0) {
-            V v[NL];
+            V rh[NH];
             bool rin = m0 + 1 <= s.ext[0];
 #pragma unroll
-            for (int j = 0; j < NH; ++j) {
-                v[2 * j] = uc[j];
-                V x = (ok[j] && rin) ? u[off[j] + m0] : V(0);
-                v[2 * j + 1] = x;
-                uc[j] = x;
-            }
-            wht_group<D, V>(v, g);
+            for (int j = 0; j < NH; ++j) rh[j] = (ok[j] && rin) ? u[off[j] + m0] : V(0);
+            wht_face<D, V>(rh, g);
             V a = live ? acol[m0] : V(0);
-#pragma unroll
-            for (int b = 0; b < NL; ++b) v[b] *= a * lamg[b];
-            wht_group<D, V>(v, g);
+            V outl[NH];
 #pragma unroll
             for (int j = 0; j < NH; ++j) {
-                if (ok[j] && m0 >= 1) atomicAdd(&z[off[j] + m0 - 1], v[2 * j] + vc[j]);
-                vc[j] = v[2 * j + 1];
+                V sp = (lh[j] + rh[j]) * (a * lp[j]);
+                V sm = (lh[j] - rh[j]) * (a * lm[j]);
+                lh[j] = rh[j];
+                outl[j] = sp + sm + cr[j];
+                cr[j] = sp - sm;
             }
+            wht_face<D, V>(outl, g);
+#pragma unroll
+            for (int j = 0; j < NH; ++j)
+                if (ok[j] && m0 >= 1) atomicAdd(&z[off[j] + m0 - 1], outl[j]);
         }
     }
 }
