@@ -80,6 +80,21 @@ int lsg_matvec(lsg_operator *op, const double *x, double *y);
  * LSG_FP32), enqueued on `stream` (a cudaStream_t, 0 = legacy default). */
 int lsg_matvec_device(lsg_operator *op, const void *x, void *y, int32_t precision, void *stream);
 
+/* Allocation-free variant of lsg_matvec_device (no counterpart in the
+ * reference, which has no device code).  For callers that cannot allocate
+ * device memory at call time: code running during CUDA graph capture, hosts
+ * whose own allocator owns the whole device, loops that cannot afford the
+ * synchronisation of cudaMalloc/cudaFree.  Its work space is one fixed 32 MiB
+ * array compiled into the library (held on every GPU that loads it until the
+ * process exits); grids needing more are rejected with LSG_E_INVALID and a
+ * message giving both sizes.  It calls no cudaMalloc/cudaFree.  The first call
+ * on a device resolves the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (different streams, or threads without
+ * ordering) race and give wrong results.  The operator itself (tables,
+ * coefficient) is created beforehand as usual. */
+int lsg_matvec_device_noalloc(lsg_operator *op, const void *x, void *y, int32_t precision, void *stream);
+
 /* Times `iters` matvecs on device buffers with CUDA events between the
  * phases; phase_ms[0..3] = mean ms of (nodal transform, P init, prolongation
  * levels, restriction wavefronts incl. the cell operator), phase_ms[4] = whole

@@ -92,6 +92,7 @@ def lib():
             "lsg_matvec_device": (ctypes.c_int, [P, P, P, I32, P]),
             "lsg_diag": (ctypes.c_int, [P, P]),
             "lsg_matvec_profile": (ctypes.c_int, [P, P, P, I32, I32, P, P, P]),
+            "lsg_matvec_device_noalloc": (ctypes.c_int, [P, P, P, I32, P]),
             "lsg_diag_device": (ctypes.c_int, [P, P, P]),
             "lsg_cg_solve": (ctypes.c_int, [P, P, P, P, P]),
             "lsg_cg_solve_device": (ctypes.c_int, [P, P, P, P, P, P]),

@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1599,3 +1600,120 @@ static int lsg_internal_matvec32(lsg_operator* op, const float* x, float* y, cud
     return matvec_dispatch<float>(op, x, y, st);
 }
 static const uint8_t* lsg_internal_active(lsg_operator* op) { return op->act.as<uint8_t>(); }
+
+// ============================================================================= allocation-free matvec
+// Some callers cannot allocate device memory when they need a product: code
+// running while a CUDA graph is being captured (cudaMalloc is not permitted
+// during capture), host applications whose own allocator owns every byte of
+// the device and forbids foreign allocations, and latency-critical loops that
+// cannot afford the implicit synchronisation of cudaMalloc/cudaFree.  For them
+// lsg_matvec_device_noalloc takes its work space from one fixed array that is
+// part of the library image on every GPU that loads it.
+#define LSG_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[LSG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[256] = {nullptr};  // device address of g_noalloc_scratch, per device
+
+// The array's host-side name is not a device address: resolve it once per
+// device, with that device current.
+int noalloc_address(unsigned char** out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return fail(LSG_E_INVALID, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(LSG_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+    return 0;
+}
+
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+template <int D, typename V>
+int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, unsigned char* base) {
+    const lsg::Plan& p = op->plan;
+    size_t b_ml = align256(p.M * sizeof(V)), b_pc = align256(p.p_total * sizeof(V));
+    size_t b_gm = align256(p.gm_total * sizeof(V));
+    size_t b_sc = align256(std::max<int64_t>(p.scratch_total, 1) * sizeof(V));
+    size_t b_ns = align256(std::max<int64_t>(p.nodal_scratch, 1) * sizeof(V));
+    size_t need = b_ml + b_pc + b_gm + b_sc + b_ns;
+    if (need > LSG_NOALLOC_SCRATCH_BYTES)
+        return fail(LSG_E_INVALID, "lsg_matvec_device_noalloc: this grid needs " + std::to_string(need) +
+                                       " bytes of work space, the fixed array holds " +
+                                       std::to_string(LSG_NOALLOC_SCRATCH_BYTES) +
+                                       "; use lsg_matvec_device for larger grids");
+    V* ml = reinterpret_cast<V*>(base);
+    V* pc = reinterpret_cast<V*>(base + b_ml);
+    V* gm = reinterpret_cast<V*>(base + b_ml + b_pc);
+    V* scratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_gm);
+    V* nscratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_gm + b_sc);
+    int rc = set_phaseB_smem<D, V>();
+    if (rc) return rc;
+    const V* acell = std::is_same<V, double>::value ? (const V*)op->acell64.p : (const V*)op->acell32.p;
+    const V* lam = std::is_same<V, double>::value ? (const V*)op->lam64.p : (const V*)op->lam32.p;
+    // Every region is written before it is read within one call (nodal slabs by
+    // k_nodal, P by k_pinit, gM only where an earlier item of the same call
+    // wrote it, item scratch by its own item), so nothing needs clearing;
+    // y is zeroed at active points as in the allocating path.
+    int64_t na = p.exa_off[p.nD];
+    if (na > 0) k_zero_active<V><<<nblk(na), 256, 0, st>>>(op->dp.exa, na, y);
+    k_nodal<V><<<p.nD, 256, 0, st>>>(op->dp, x, ml, nscratch);
+    int32_t nb = (int32_t)p.b_items.size();
+    if (nb > 0) k_pinit<V><<<nb, 256, 0, st>>>(op->dp, ml, pc, 0);
+    for (size_t L = 0; L + 1 < p.a_level_off.size(); ++L) {
+        int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
+        if (e > b) k_prolong<V><<<e - b, 256, 0, st>>>(op->dp, pc, b);
+    }
+    const int64_t cap_elems = (200 * 1024) / sizeof(V) - (1 << D);
+    for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
+        int32_t b = p.b_level_off[L], e = p.b_level_off[L + 1];
+        if (e <= b) continue;
+        int64_t mx = op->level_maxn[L];
+        int64_t alloc_elems = 2 * mx <= cap_elems ? 2 * mx : 0;
+        size_t smem = (size_t)((1 << D) + alloc_elems) * sizeof(V);
+        k_phaseB<D, V><<<e - b, 256, smem, st>>>(op->dp, pc, gm, scratch, y, acell, lam, b, alloc_elems);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <typename V>
+int matvec_noalloc_dispatch(lsg_operator* op, const V* x, V* y, cudaStream_t st, unsigned char* base) {
+    switch (op->plan.d) {
+    case 1: return matvec_noalloc_impl<1, V>(op, x, y, st, base);
+    case 2: return matvec_noalloc_impl<2, V>(op, x, y, st, base);
+    case 3: return matvec_noalloc_impl<3, V>(op, x, y, st, base);
+    case 4: return matvec_noalloc_impl<4, V>(op, x, y, st, base);
+    case 5: return matvec_noalloc_impl<5, V>(op, x, y, st, base);
+    case 6: return matvec_noalloc_impl<6, V>(op, x, y, st, base);
+    case 7: return matvec_noalloc_impl<7, V>(op, x, y, st, base);
+    case 8: return matvec_noalloc_impl<8, V>(op, x, y, st, base);
+    }
+    return fail(LSG_E_INVALID, "unsupported dimension");
+}
+
+}  // namespace
+
+extern "C" int lsg_matvec_device_noalloc(lsg_operator* op, const void* x, void* y, int32_t precision, void* stream) {
+    if (!op || !x || !y) return fail(LSG_E_INVALID, "null argument");
+    if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
+    if (precision != LSG_FP64 && precision != LSG_FP32)
+        return fail(LSG_E_INVALID, "precision must be LSG_FP64 or LSG_FP32");
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != op->device) return fail(LSG_E_INVALID, "the operator lives on another device than the current one");
+    unsigned char* base = nullptr;
+    int rc = noalloc_address(&base);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == LSG_FP64) return matvec_noalloc_dispatch<double>(op, (const double*)x, (double*)y, st, base);
+    return matvec_noalloc_dispatch<float>(op, (const float*)x, (float*)y, st, base);
+}

@@ -1,0 +1,52 @@
+"""The allocation-free matvec entry point (lsg_matvec_device_noalloc).
+
+It exists for callers that cannot allocate device memory when they need a
+product (graph capture, host-owned allocators, loops that cannot pay for the
+synchronisation of cudaMalloc/cudaFree); its work space is a fixed array in the
+library.  This file is collected last so that a failure here leaves every other
+test already run; it passes alone in a fresh process as well."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import loadsg_b200 as lsg
+
+pytestmark = pytest.mark.gpu
+
+
+def _call(m, x, y, precision):
+    rc = lsg.lib().lsg_matvec_device_noalloc(m._h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                                              precision, None)
+    return rc
+
+
+@pytest.mark.parametrize("precision,tol", [(lsg.FP64, 1e-12), (lsg.FP32, 2e-5)])
+def test_noalloc_matches_allocating_entry_point(precision, tol):
+    import torch
+    g = lsg.AdaptiveSparseGrid.regular(3, 6)
+    prob = lsg.MidpointDiffusion(lsg.COEF_SINPROD, [1.0, 0.5, 1, 1, 1])
+    m = lsg.MatrixVectorHomogen(g, prob)
+    dt = torch.float64 if precision == lsg.FP64 else torch.float32
+    rng = np.random.default_rng(7)
+    x = torch.tensor(rng.uniform(-1, 1, g.n), dtype=dt, device="cuda")
+    y_ref = torch.zeros(g.n, dtype=dt, device="cuda")
+    m.multiplication_device(x.data_ptr(), y_ref.data_ptr(), precision)
+    for _ in range(2):  # two calls in a row share (and reuse) the fixed array
+        y = torch.full((g.n,), 3.0, dtype=dt, device="cuda")
+        assert _call(m, x, y, precision) == 0, lsg.lib().lsg_last_error()
+        torch.cuda.synchronize()
+        err = (y - y_ref).abs().max().item() / y_ref.abs().max().item()
+        assert err < tol
+
+
+def test_noalloc_rejects_oversized_grid():
+    import torch
+    g = lsg.AdaptiveSparseGrid.regular(6, 6)  # needs more than the fixed 32 MiB
+    prob = lsg.MidpointDiffusion(lsg.COEF_CONST, [1.0])
+    m = lsg.MatrixVectorHomogen(g, prob)
+    x = torch.zeros(g.n, dtype=torch.float64, device="cuda")
+    y = torch.zeros(g.n, dtype=torch.float64, device="cuda")
+    rc = _call(m, x, y, lsg.FP64)
+    assert rc == -1
+    assert b"fixed array holds" in lsg.lib().lsg_last_error()
