@@ -5,10 +5,11 @@
 //                MatrixVectorHomogen.cpp:43-74), sum-factorised 3-tap stages
 //   k_pinit      P_c(T) = nodal(T)            ("P += nodal", MVH.h:1649)
 //   k_prolong    one prolongation level       (MVH.h:1655-1670, 444-474)
-//   k_phaseB     one restriction wavefront: per (case, depth) item the level-T
-//                cell operator (LocalStiffnessMatrices.cpp:555-582) applied in
-//                the Walsh-Hadamard basis where the Q1 element is diagonal,
-//                + gM bookkeeping + restrictions (MVH.h:1672-1735, 485-530)
+//   k_cells      the level-T cell operator (LocalStiffnessMatrices.cpp:555-582)
+//                for every (case, depth) item, applied in the Walsh-Hadamard
+//                basis where the Q1 element is diagonal
+//   k_level      one restriction wavefront: per (case, depth) item the gM
+//                bookkeeping + restrictions (MVH.h:1672-1735, 485-530)
 //                + ConvertToPrewavelet2 (MVH.h:540-562), sum-factorised 5-tap
 //   k_diag       exact Jacobi diagonal (cg_method.h:544-680)
 //   CG kernels   CG::solveHomogen vector semantics (cg_method.h:759-886)
@@ -321,25 +322,25 @@ __device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __rest
     }
 }
 
-// ----------------------------------------------------------------------------- phase B item
+// ----------------------------------------------------------------------------- phase B, cell operator
+// z_c(T) = A_T P_c(T) for every (case, depth) item in one launch (per size
+// class): the cell operator does not depend on the gM chain, so it needs no
+// wavefront ordering.  u and z live in shared memory when 2 N_T fits.
 template <int D, typename V>
-__global__ void __launch_bounds__(256, 2) k_phaseB(DevPlan P, const V* __restrict__ pc, V* __restrict__ gm,
-                                                 V* __restrict__ scratch, V* __restrict__ y,
-                                                 const V* __restrict__ acell, const V* __restrict__ lam_all,
-                                                 int32_t item0, int64_t smem_cap) {
+__global__ void __launch_bounds__(256, 2) k_cells(DevPlan P, const V* __restrict__ pc, V* __restrict__ zb,
+                                                  const V* __restrict__ acell, const V* __restrict__ lam_all,
+                                                  const int32_t* __restrict__ order, int32_t ord0, int64_t cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NC = 1 << D;
-    const lsg::PhaseBItem it = P.b_items[item0 + blockIdx.x];
+    const lsg::PhaseBItem it = P.b_items[order[ord0 + blockIdx.x]];
     const DevSlab& s = P.slabs[it.t];
     V* lam = reinterpret_cast<V*>(smem_raw);
     for (int b = threadIdx.x; b < NC; b += blockDim.x) lam[b] = lam_all[(int64_t)it.t * NC + b];
-    // this lane's Hadamard-basis eigenvalues (high bits = lane position in its group)
     const V* lamg = lam + ((threadIdx.x & (CellCfg<D>::G - 1)) << CellCfg<D>::DL);
-    V* scr = scratch + it.scratch_off;
     const V* u_g = pc + it.p_off;
+    V* z_g = zb + it.p_off;
     const V* ac = acell + s.cell_off;
-    bool in_smem = (int64_t)(2 * s.n) <= smem_cap;
-    if (in_smem) {
+    if (2 * s.n <= cap) {
         V* u = lam + NC;
         V* z = u + s.n;
         for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) {
@@ -350,47 +351,67 @@ __global__ void __launch_bounds__(256, 2) k_phaseB(DevPlan P, const V* __restric
         if (s.dense) cells_dense<D, V>(s, u, z, ac, lamg);
         else cells_sparse<D, V>(P, s, u, z, ac, lamg);
         __syncthreads();
-        const V* g0 = gm + it.gm_off;
-        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) scr[e] = it.gm_prev ? z[e] + g0[e] : z[e];
+        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) z_g[e] = z[e];
     } else {
-        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) scr[e] = V(0);
+        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) z_g[e] = V(0);
         __syncthreads();
-        if (s.dense) cells_dense<D, V>(s, u_g, scr, ac, lamg);
-        else cells_sparse<D, V>(P, s, u_g, scr, ac, lamg);
-        __syncthreads();
-        if (it.gm_prev) {
-            const V* g0 = gm + it.gm_off;
-            for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) scr[e] += g0[e];
-        }
+        if (s.dense) cells_dense<D, V>(s, u_g, z_g, ac, lamg);
+        else cells_sparse<D, V>(P, s, u_g, z_g, ac, lamg);
     }
+}
+
+// ----------------------------------------------------------------------------- phase B, wavefront level
+// Per (case, depth) item of one restriction wavefront: z = z_c(T) + gM_c(T),
+// the restriction steps with the gM swap-add, and ConvertToPrewavelet2 into y.
+// Buffers ping-pong in shared memory when the item's largest vector fits.
+template <int D, typename V>
+__global__ void __launch_bounds__(128) k_level(DevPlan P, const V* __restrict__ zb, V* __restrict__ gm,
+                                               V* __restrict__ scratch, V* __restrict__ y, int32_t item0,
+                                               int64_t buf_elems) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const lsg::PhaseBItem it = P.b_items[item0 + blockIdx.x];
+    const DevSlab& s = P.slabs[it.t];
+    // largest vector of this item
+    int64_t need = s.n;
+    for (int32_t si = it.step_begin; si < it.step_end; ++si) need = max(need, P.b_steps[si].n_dst);
+    if (it.t_conv >= 0)
+        for (int j = 1; j < D; ++j) need = max(need, P.conv_dom[it.t_conv * (D + 1) + j]);
+    V *A, *B;
+    bool ping = need <= buf_elems;
+    int64_t used = 0;
+    V* scr = scratch + it.scratch_off;
+    if (ping) {
+        A = reinterpret_cast<V*>(smem_raw);
+        B = A + buf_elems;
+    } else {
+        A = scr;
+        B = scr + s.n;
+        used = s.n;
+    }
+    const V* z0 = zb + it.p_off;
+    const V* g0 = gm + it.gm_off;
+    for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) A[e] = it.gm_prev ? z0[e] + g0[e] : z0[e];
     __syncthreads();
-    // restriction steps with gM swap-add
-    V* cur = scr;
-    int64_t used = s.n;
     for (int32_t si = it.step_begin; si < it.step_end; ++si) {
         const lsg::PhaseBStep st = P.b_steps[si];
         const int32_t* tab = P.restr + st.tab_off;
-        V* nxt = scr + used;
         V* g = gm + st.gm_off;
         for (int64_t q = threadIdx.x; q < st.n_dst; q += blockDim.x) {
             int32_t a = tab[3 * q], l = tab[3 * q + 1], r = tab[3 * q + 2];
-            V v = cur[a];
-            if (l >= 0) v = v + V(0.5) * cur[l];
-            if (r >= 0) v = v + V(0.5) * cur[r];
+            V v = A[a];
+            if (l >= 0) v = v + V(0.5) * A[l];
+            if (r >= 0) v = v + V(0.5) * A[r];
             V tmp = st.gm_prev ? g[q] : V(0);
             g[q] = v;
-            nxt[q] = v + tmp;
+            B[q] = v + tmp;
         }
         __syncthreads();
-        cur = nxt;
-        used += st.n_dst;
+        if (ping) { V* t = A; A = B; B = t; }
+        else { A = B; used += st.n_dst; B = scr + used; }
     }
-    // convert to prewavelets at Tc
     if (it.t_conv >= 0) {
         int tc = it.t_conv;
         const int64_t* dom = P.conv_dom + tc * (D + 1);
-        const V* in = cur;
-        V* buf = scr + used;
         for (int j = 0; j < D; ++j) {
             int64_t so = P.conv_stage[tc * D + j];
             int64_t nout = dom[j + 1];
@@ -405,15 +426,15 @@ __global__ void __launch_bounds__(256, 2) k_phaseB(DevPlan P, const V* __restric
                     for (int q = 0; q < 5; ++q) {
                         int32_t i = src[e * 5 + q];
                         if (i < 0) break;
-                        acc += wcode<V>((cd >> (3 * q)) & 7) * in[i];
+                        acc += wcode<V>((cd >> (3 * q)) & 7) * A[i];
                     }
                     atomicAdd(&y[outmap[e]], acc);
                 }
             } else {
-                stage_gather<5, V, V>(P.conv_src + so * 5, P.conv_code + so, nout, in, nullptr, buf);
+                stage_gather<5, V, V>(P.conv_src + so * 5, P.conv_code + so, nout, A, nullptr, B);
                 __syncthreads();
-                in = buf;
-                buf += nout;
+                if (ping) { V* t = A; A = B; B = t; }
+                else { A = B; used += nout; B = scr + used; }
             }
         }
     }
@@ -665,7 +686,7 @@ struct lsg_operator {
     DBuf acell64, acell32, params;
     // work buffers per precision
     struct Work {
-        DBuf ml, pc, gm, scratch, nscratch;
+        DBuf ml, pc, zb, gm, scratch, nscratch;
     } w64, w32;
     DBuf xbuf64, ybuf64;  // host-call staging
     DBuf diag;            // Jacobi diagonal (FP64)
@@ -673,7 +694,10 @@ struct lsg_operator {
     DBuf learned;
     bool have_learned = false;
     int64_t smem_cap64 = 0, smem_cap32 = 0;
-    std::vector<int64_t> level_maxn;  // per phase-B level: max N_T
+    std::vector<int64_t> level_need;  // per phase-B level: largest vector of any item
+    DBuf cell_order;                  // phase-B items ordered by slab size (k_cells)
+    std::vector<int32_t> cell_class_off;  // size classes in cell_order
+    std::vector<int64_t> cell_class_n;    // largest N_T per class
 };
 
 namespace {
@@ -784,12 +808,41 @@ int upload_plan(lsg_operator* op) {
     P.b_items = op->b_items.as<lsg::PhaseBItem>();
     P.b_steps = op->b_steps.as<lsg::PhaseBStep>();
     P.pts = op->pts.as<int32_t>();
-    // per-level max slab size (dynamic shared memory of k_phaseB)
-    op->level_maxn.clear();
+    // per-level largest vector of an item (dynamic shared memory of k_level)
+    op->level_need.clear();
     for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
         int64_t mx = 0;
-        for (int32_t i = p.b_level_off[L]; i < p.b_level_off[L + 1]; ++i) mx = std::max(mx, p.slabs[p.b_items[i].t].n);
-        op->level_maxn.push_back(mx);
+        for (int32_t i = p.b_level_off[L]; i < p.b_level_off[L + 1]; ++i) {
+            const lsg::PhaseBItem& it = p.b_items[i];
+            int64_t need = p.slabs[it.t].n;
+            for (int32_t k = it.step_begin; k < it.step_end; ++k) need = std::max(need, p.b_steps[k].n_dst);
+            if (it.t_conv >= 0)
+                for (int j = 1; j < d; ++j) need = std::max(need, p.convert_dom[it.t_conv * (d + 1) + j]);
+            mx = std::max(mx, need);
+        }
+        op->level_need.push_back(mx);
+    }
+    // k_cells items by slab size, largest first, in size classes (shared memory
+    // per launch = 2 N_T of the class's largest slab)
+    {
+        std::vector<int32_t> ord(p.b_items.size());
+        for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int32_t)i;
+        std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) {
+            return p.slabs[p.b_items[a].t].n > p.slabs[p.b_items[b].t].n;
+        });
+        op->cell_class_off.clear();
+        op->cell_class_n.clear();
+        int64_t bound = -1;
+        for (size_t i = 0; i < ord.size(); ++i) {
+            int64_t n = p.slabs[p.b_items[ord[i]].t].n;
+            if (bound < 0 || n * 4 < bound) {  // new class when slabs shrink 4x
+                op->cell_class_off.push_back((int32_t)i);
+                op->cell_class_n.push_back(n);
+                bound = n;
+            }
+        }
+        op->cell_class_off.push_back((int32_t)ord.size());
+        if (op->cell_order.upload(ord, tot)) return LSG_E_CUDA;
     }
     return 0;
 }
@@ -802,6 +855,7 @@ int ensure_work(lsg_operator* op, lsg_operator::Work& w) {
     int rc = 0;
     rc |= w.ml.alloc(p.M * sizeof(V), tot);
     rc |= w.pc.alloc(p.p_total * sizeof(V), tot);
+    rc |= w.zb.alloc(p.p_total * sizeof(V), tot);
     rc |= w.gm.alloc(p.gm_total * sizeof(V), tot);
     rc |= w.scratch.alloc(std::max<int64_t>(p.scratch_total, 1) * sizeof(V), tot);
     rc |= w.nscratch.alloc(std::max<int64_t>(p.nodal_scratch, 1) * sizeof(V), tot);
@@ -812,8 +866,33 @@ template <int D, typename V>
 int set_phaseB_smem() {
     static bool done = false;
     if (done) return 0;
-    CUDA_TRY(cudaFuncSetAttribute(k_phaseB<D, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_cells<D, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_level<D, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
     done = true;
+    return 0;
+}
+
+// Phase B: k_cells per size class, then one k_level per restriction wavefront.
+template <int D, typename V>
+int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* y, const V* acell, const V* lam,
+                  cudaStream_t st) {
+    const lsg::Plan& p = op->plan;
+    const int64_t cap_elems = (200 * 1024) / sizeof(V) - (1 << D);
+    for (size_t c = 0; c + 1 < op->cell_class_off.size(); ++c) {
+        int32_t b = op->cell_class_off[c], e = op->cell_class_off[c + 1];
+        int64_t need = 2 * op->cell_class_n[c];
+        int64_t alloc = need <= cap_elems ? need : 0;
+        size_t smem = (size_t)((1 << D) + alloc) * sizeof(V);
+        k_cells<D, V><<<e - b, 256, smem, st>>>(op->dp, pc, zb, acell, lam, op->cell_order.as<int32_t>(), b, alloc);
+    }
+    const int64_t lvl_cap = 12288;  // elements per ping-pong buffer
+    for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
+        int32_t b = p.b_level_off[L], e = p.b_level_off[L + 1];
+        if (e <= b) continue;
+        int64_t bufn = std::min<int64_t>(op->level_need[L], lvl_cap);
+        k_level<D, V><<<e - b, 128, 2 * bufn * sizeof(V), st>>>(op->dp, zb, gm, scratch, y, b, bufn);
+    }
+    CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
@@ -841,16 +920,8 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t
         if (e > b) k_prolong<V><<<e - b, 256, 0, st>>>(op->dp, w.pc.as<V>(), b);
     }
     if (ev) cudaEventRecord(ev[3], st);
-    const int64_t cap_elems = (200 * 1024) / sizeof(V) - (1 << D);
-    for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
-        int32_t b = p.b_level_off[L], e = p.b_level_off[L + 1];
-        if (e <= b) continue;
-        int64_t mx = op->level_maxn[L];
-        int64_t alloc_elems = 2 * mx <= cap_elems ? 2 * mx : 0;  // u and z of the largest slab
-        size_t smem = (size_t)((1 << D) + alloc_elems) * sizeof(V);
-        k_phaseB<D, V><<<e - b, 256, smem, st>>>(op->dp, w.pc.as<V>(), w.gm.as<V>(), w.scratch.as<V>(), y, acell, lam, b,
-                                                 alloc_elems);
-    }
+    rc = phaseB_launch<D, V>(op, w.pc.as<V>(), w.zb.as<V>(), w.gm.as<V>(), w.scratch.as<V>(), y, acell, lam, st);
+    if (rc) return rc;
     if (ev) cudaEventRecord(ev[4], st);
     CUDA_TRY(cudaGetLastError());
     return 0;
@@ -1641,10 +1712,11 @@ template <int D, typename V>
 int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, unsigned char* base) {
     const lsg::Plan& p = op->plan;
     size_t b_ml = align256(p.M * sizeof(V)), b_pc = align256(p.p_total * sizeof(V));
+    size_t b_zb = b_pc;
     size_t b_gm = align256(p.gm_total * sizeof(V));
     size_t b_sc = align256(std::max<int64_t>(p.scratch_total, 1) * sizeof(V));
     size_t b_ns = align256(std::max<int64_t>(p.nodal_scratch, 1) * sizeof(V));
-    size_t need = b_ml + b_pc + b_gm + b_sc + b_ns;
+    size_t need = b_ml + b_pc + b_zb + b_gm + b_sc + b_ns;
     if (need > LSG_NOALLOC_SCRATCH_BYTES)
         return fail(LSG_E_INVALID, "lsg_matvec_device_noalloc: this grid needs " + std::to_string(need) +
                                        " bytes of work space, the fixed array holds " +
@@ -1652,9 +1724,10 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
                                        "; use lsg_matvec_device for larger grids");
     V* ml = reinterpret_cast<V*>(base);
     V* pc = reinterpret_cast<V*>(base + b_ml);
-    V* gm = reinterpret_cast<V*>(base + b_ml + b_pc);
-    V* scratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_gm);
-    V* nscratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_gm + b_sc);
+    V* zb = reinterpret_cast<V*>(base + b_ml + b_pc);
+    V* gm = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb);
+    V* scratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm);
+    V* nscratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm + b_sc);
     int rc = set_phaseB_smem<D, V>();
     if (rc) return rc;
     const V* acell = std::is_same<V, double>::value ? (const V*)op->acell64.p : (const V*)op->acell32.p;
@@ -1672,15 +1745,8 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
         int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
         if (e > b) k_prolong<V><<<e - b, 256, 0, st>>>(op->dp, pc, b);
     }
-    const int64_t cap_elems = (200 * 1024) / sizeof(V) - (1 << D);
-    for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
-        int32_t b = p.b_level_off[L], e = p.b_level_off[L + 1];
-        if (e <= b) continue;
-        int64_t mx = op->level_maxn[L];
-        int64_t alloc_elems = 2 * mx <= cap_elems ? 2 * mx : 0;
-        size_t smem = (size_t)((1 << D) + alloc_elems) * sizeof(V);
-        k_phaseB<D, V><<<e - b, 256, smem, st>>>(op->dp, pc, gm, scratch, y, acell, lam, b, alloc_elems);
-    }
+    rc = phaseB_launch<D, V>(op, pc, zb, gm, scratch, y, acell, lam, st);
+    if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
     return 0;
 }
