@@ -220,29 +220,38 @@ __device__ __forceinline__ void wht_face(V* v, int g) {
 }
 
 // z += sum over the slab's cells of a_c H diag(lam) H u_c on a dense slab.
-// A lane group walks one column of cells along dim 0.  The Hadamard transform
-// factorises as H = H_0 (x) H_rest; the H_rest transform of a face is shared
-// by the two cells on either side of it, so per cell only the new (right)
-// face is transformed forward, and the left-face outputs of this cell and
-// the right-face outputs of the previous one are summed before one inverse
-// H_rest.  Faces on the boundary (m0 = 0 left, m0 = 2^T_0 - 1 right) drop out.
-// All lanes of a warp run the same number of rounds (shuffles need them).
+// Work unit = a segment of at most 8 consecutive cells of one dim-0 column.
+// The Hadamard transform factorises as H = H_0 (x) H_rest; the H_rest
+// transform of a face is shared by the two cells on either side of it, so per
+// cell only the new (right) face is transformed forward, and the left-face
+// outputs of this cell and the right-face outputs of the previous one are
+// summed before one inverse H_rest.  A segment transforms its first left face
+// itself and scatters its last right face; faces on the boundary drop out.
+// Segments (instead of whole columns) keep all lanes busy when dim 0 is long
+// and the other dims short.  All lanes of a warp run the same number of
+// rounds and iterations (the group shuffles need them).
 template <int D, typename V>
 __device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, const V* __restrict__ ac, const V* lamg) {
     constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NH = CellCfg<D>::NH;
     const int g = threadIdx.x & (G - 1);
     const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
     const int32_t c0 = s.ext[0] + 1;  // cells along dim 0
+    const int32_t seg = c0 < 8 ? c0 : 8;
+    const int32_t nseg = (c0 + seg - 1) / seg;
     const int64_t ncols = s.ncell / c0;
-    const int64_t rounds = (ncols + ngroups - 1) / ngroups;
+    const int64_t units = ncols * nseg;
+    const int64_t rounds = (units + ngroups - 1) / ngroups;
     V lp[NH], lm[NH];  // eigenvalues for s_0 = + (bit 0 clear) and s_0 = - (bit 0 set)
 #pragma unroll
     for (int j = 0; j < NH; ++j) { lp[j] = lamg[2 * j]; lm[j] = lamg[2 * j + 1]; }
     for (int64_t r = 0; r < rounds; ++r) {
-        int64_t col = r * ngroups + group;
-        bool live = col < ncols;
+        int64_t unit = r * ngroups + group;
+        bool live = unit < units;
+        int64_t col = live ? unit / nseg : 0;
+        int32_t m0s = live ? (int32_t)(unit % nseg) * seg : 0;
+        int32_t m0e = min(m0s + seg, c0);
         int32_t m[D];
-        int64_t rem = live ? col : 0;
+        int64_t rem = col;
 #pragma unroll
         for (int k = 1; k < D; ++k) {
             int32_t ck = s.ext[k] + 1;
@@ -267,29 +276,42 @@ __device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, con
         }
         V lh[NH], cr[NH];  // transformed left face, carried right-face output
 #pragma unroll
-        for (int j = 0; j < NH; ++j) { lh[j] = V(0); cr[j] = V(0); }
+        for (int j = 0; j < NH; ++j) {
+            lh[j] = (ok[j] && m0s >= 1) ? u[off[j] + m0s - 1] : V(0);
+            cr[j] = V(0);
+        }
+        wht_face<D, V>(lh, g);
         const V* acol = ac + col * c0;
-        for (int32_t m0 = 0; m0 < c0; ++m0) {
+        for (int32_t i = 0; i < seg; ++i) {
+            int32_t m0 = m0s + i;
+            bool cv = live && m0 < m0e;
             V rh[NH];
-            bool rin = m0 + 1 <= s.ext[0];
+            bool rin = cv && m0 + 1 <= s.ext[0];
 #pragma unroll
             for (int j = 0; j < NH; ++j) rh[j] = (ok[j] && rin) ? u[off[j] + m0] : V(0);
             wht_face<D, V>(rh, g);
-            V a = live ? acol[m0] : V(0);
+            V a = cv ? acol[m0] : V(0);
             V outl[NH];
 #pragma unroll
             for (int j = 0; j < NH; ++j) {
                 V sp = (lh[j] + rh[j]) * (a * lp[j]);
                 V sm = (lh[j] - rh[j]) * (a * lm[j]);
-                lh[j] = rh[j];
                 outl[j] = sp + sm + cr[j];
-                cr[j] = sp - sm;
+                if (cv) {
+                    lh[j] = rh[j];
+                    cr[j] = sp - sm;
+                }
             }
             wht_face<D, V>(outl, g);
 #pragma unroll
             for (int j = 0; j < NH; ++j)
-                if (ok[j] && m0 >= 1) atomicAdd(&z[off[j] + m0 - 1], outl[j]);
+                if (cv && ok[j] && m0 >= 1) atomicAdd(&z[off[j] + m0 - 1], outl[j]);
         }
+        // right face of the segment's last cell, unless it lies on the boundary
+        wht_face<D, V>(cr, g);
+#pragma unroll
+        for (int j = 0; j < NH; ++j)
+            if (ok[j] && m0e < c0) atomicAdd(&z[off[j] + m0e - 1], cr[j]);
     }
 }
 
