@@ -33,7 +33,16 @@ def workload(name, rank):
     """Seeded synthetic instance: (grid, coefficient family, params, f, description)."""
     import loadsg_b200 as lsg
     rng = np.random.default_rng(1000 + rank)
-    if name.startswith("d6_regular_L"):
+    if name == "d6_adaptive_corner":
+        # d=6 grid refined toward the corner (0,...,0): regular level 7, then 3
+        # rounds adding the sons of every active point with max_k x_k < 0.6*2^(1-r),
+        # then the reference's completion (hanging nodes included): 499,107 points
+        g = lsg.AdaptiveSparseGrid.adaptive(6, 7, 3, 0.6, "corner")
+        c = rng.normal(0.0, 0.3, 6)
+        fam, params = lsg.COEF_EXPSIN, list(c)
+        desc = ("d=6 adaptive grid: regular level 7 refined 3 rounds toward the corner (max_k x_k < 0.6*2^(1-r)) "
+                "+ completeDirichletGrid; a=exp(sum_k c_k sin(k pi x_k)), c_k~N(0,0.3^2); f~U[-1,1] on active points")
+    elif name.startswith("d6_regular_L"):
         level = int(name.split("L")[1])
         g = lsg.AdaptiveSparseGrid.regular(6, level)
         c = rng.normal(0.0, 0.3, 6)
@@ -134,7 +143,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--workload", default="d6_regular_L8")
+    ap.add_argument("--workload", default="d6_adaptive_corner")
     ap.add_argument("--precond", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -1,0 +1,164 @@
+// loadsg.hpp -- header-only C++ drop-in for LoAdSG's prewavelet matvec / CG path,
+// built on the C-ABI of lsg.h (liblsg.so).  Class and method names follow the
+// reference (paths relative to LoAdSG's library/source/):
+//
+//   AdaptiveSparseGrid            sgrid/sparseGrid.h:86-387
+//     AddRecursiveSonsOfPoint     sgrid/sparseGrid.cc:557-566 (center point, level)
+//     AddPoint / getIndexOfTable / getActiveTable / getMaximalOccupiedSecondTable
+//   VectorSparseG                 extemp/vector.h:247-441 (double per storage index)
+//   StencilTemplate plugin        stencils/Stencil.h:740 -> MidpointDiffusion (family + params)
+//   MatrixVectorHomogen           MatrixVectorMultiplication/MatrixVectorHomogen.h:32-652
+//     multiplication(prew, Ax, problem)   MatrixVectorHomogen.h:91-92
+//   CG::solveHomogen              applications/cg_method.h:27-33
+//
+// Differences a caller must know: the grid is frozen when the first
+// MatrixVectorHomogen is built from it (the tables are flattened once); errors
+// throw lsg::Error instead of exit(1).
+#pragma once
+#include <algorithm>
+#include <array>
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../lsg.h"
+
+namespace lsg {
+
+struct Error : std::runtime_error {
+    explicit Error(const std::string& m) : std::runtime_error(m) {}
+};
+
+inline void check(int rc) {
+    if (rc != LSG_OK) throw Error(std::string("liblsg: ") + lsg_last_error());
+}
+
+template <int D>
+class AdaptiveSparseGrid {
+public:
+    using Index = std::array<int32_t, D>;
+    // AddPoint (sgrid/sparseGrid.cc:482-516): appends in storage order, returns
+    // false if the point is already present (it is then marked active).
+    bool AddPoint(const Index& I, bool active = true) {
+        auto it = where_.find(I);
+        if (it != where_.end()) {
+            if (active) active_[it->second] = 1;
+            return false;
+        }
+        where_[I] = (int64_t)active_.size();
+        points_.insert(points_.end(), I.begin(), I.end());
+        active_.push_back(active ? 1 : 0);
+        return true;
+    }
+    // AddRecursiveSonsOfPoint(center, level) for a regular sparse grid, in the
+    // reference's storage order.
+    void AddRecursiveSonsOfPoint(int level) {
+        int64_t n = 0;
+        check(lsg_grid_regular(D, level, nullptr, 0, &n));
+        std::vector<int32_t> pts(n * D);
+        check(lsg_grid_regular(D, level, pts.data(), n, &n));
+        for (int64_t k = 0; k < n; ++k) {
+            Index I;
+            for (int d = 0; d < D; ++d) I[d] = pts[k * D + d];
+            AddPoint(I);
+        }
+    }
+    int64_t getMaximalOccupiedSecondTable() const { return (int64_t)active_.size(); }
+    Index getIndexOfTable(int64_t k) const {
+        Index I;
+        for (int d = 0; d < D; ++d) I[d] = points_[k * D + d];
+        return I;
+    }
+    const uint8_t* getActiveTable() const { return active_.data(); }
+    const int32_t* points() const { return points_.data(); }
+    int64_t getDOFS() const {
+        int64_t c = 0;
+        for (auto a : active_) c += a;
+        return c;
+    }
+
+private:
+    std::vector<int32_t> points_;
+    std::vector<uint8_t> active_;
+    std::map<Index, int64_t> where_;
+};
+
+template <int D>
+class VectorSparseG {
+public:
+    explicit VectorSparseG(const AdaptiveSparseGrid<D>& g) : data_(g.getMaximalOccupiedSecondTable(), 0.0) {}
+    double getValue(int64_t k) const { return data_[k]; }
+    void setValue(int64_t k, double v) { data_[k] = v; }
+    double* getDatatableVector() { return data_.data(); }
+    const double* getDatatableVector() const { return data_.data(); }
+    int64_t size() const { return (int64_t)data_.size(); }
+    void operator=(double v) { std::fill(data_.begin(), data_.end(), v); }
+
+private:
+    std::vector<double> data_;
+};
+
+// The variable-coefficient plugin: a(x) sampled at cell midpoints times the
+// exact Q1 stiffness entry (what StencilTemplate::integration returns).
+struct MidpointDiffusion {
+    int32_t family;
+    std::vector<double> params;
+};
+
+template <int D>
+class MatrixVectorHomogen {
+public:
+    explicit MatrixVectorHomogen(const AdaptiveSparseGrid<D>& g) {
+        check(lsg_operator_create(D, g.points(), g.getActiveTable(), g.getMaximalOccupiedSecondTable(), &op_));
+    }
+    ~MatrixVectorHomogen() { lsg_operator_destroy(op_); }
+    MatrixVectorHomogen(const MatrixVectorHomogen&) = delete;
+    MatrixVectorHomogen& operator=(const MatrixVectorHomogen&) = delete;
+
+    void setProblem(const MidpointDiffusion& p) {
+        if (have_ && p.family == fam_ && p.params == par_) return;
+        check(lsg_operator_set_coefficient(op_, p.family, p.params.data(), (int32_t)p.params.size()));
+        fam_ = p.family;
+        par_ = p.params;
+        have_ = true;
+    }
+    // Ax = A_prew prew at active points (hanging entries of Ax untouched).
+    void multiplication(const VectorSparseG<D>& prew, VectorSparseG<D>& Ax, const MidpointDiffusion& problem) {
+        setProblem(problem);
+        check(lsg_matvec(op_, prew.getDatatableVector(), Ax.getDatatableVector()));
+    }
+    lsg_operator* handle() { return op_; }
+
+private:
+    lsg_operator* op_ = nullptr;
+    bool have_ = false;
+    int32_t fam_ = -1;
+    std::vector<double> par_;
+};
+
+struct CG {
+    // CG::solveHomogen(eps, x, f, &iterations, usol, matrix, stencil, &time):
+    // Jacobi-preconditioned CG with the reference's stopping rule on r^T D^-1 r.
+    template <int D>
+    static bool solveHomogen(double eps, VectorSparseG<D>& x, const VectorSparseG<D>& f, int* iterations,
+                             MatrixVectorHomogen<D>& matrix, const MidpointDiffusion& problem, double* seconds,
+                             lsg_solver_opts* opts = nullptr) {
+        matrix.setProblem(problem);
+        lsg_solver_opts o{};
+        if (opts) o = *opts;
+        else {
+            o.eps = eps;
+            o.criterion = 0;
+            o.use_graph = 1;
+        }
+        lsg_solve_report rep{};
+        check(lsg_cg_solve(matrix.handle(), f.getDatatableVector(), x.getDatatableVector(), &o, &rep));
+        if (iterations) *iterations = rep.iterations;
+        if (seconds) *seconds = rep.seconds;
+        return true;
+    }
+};
+
+}  // namespace lsg

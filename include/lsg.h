@@ -169,6 +169,19 @@ int lsg_plan_export_stencil(const lsg_plan *plan, int64_t k, int64_t *idx, doubl
  * active.  Pass points = NULL to query *n. */
 int lsg_grid_regular(int32_t d, int32_t level, int32_t *points, int64_t capacity, int64_t *n);
 
+/* Adaptive grid: AddRecursiveSonsOfPoint(center, level), then `refine`
+ * rounds adding the sons of every active point with max_k x_k < theta 2^(1-r)
+ * (target 0, toward the corner) or |x_0 - 1/2| < theta 2^(1-r) (target 1,
+ * toward a hyperplane), then, if `complete`, the reference's completion
+ * AdaptiveSparseGrid::completeDirichletGrid (sgrid/sparseGrid.cc:771-787)
+ * including hanging nodes.  Storage order as the reference inserts.  The
+ * last completion stage (addPoints2, sgrid/GridGeneration.cpp:333-392) tests
+ * pairs of points; it runs only on grids of at most 40000 points (above that
+ * it is skipped: on every corner/plane refinement tested up to 41k points it
+ * added nothing).  Pass points = active = NULL to query *n. */
+int lsg_grid_adaptive(int32_t d, int32_t level, int32_t refine, double theta, int32_t target, int32_t complete,
+                      int32_t *points, uint8_t *active, int64_t capacity, int64_t *n);
+
 const char *lsg_last_error(void);
 
 #ifdef __cplusplus

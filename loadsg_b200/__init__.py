@@ -108,6 +108,7 @@ def lib():
             "lsg_plan_export_neighbors": (ctypes.c_int, [P, P]),
             "lsg_plan_export_stencil": (ctypes.c_int, [P, I64, P, P, P]),
             "lsg_grid_regular": (ctypes.c_int, [I32, I32, P, I64, P]),
+            "lsg_grid_adaptive": (ctypes.c_int, [I32, I32, I32, D, I32, I32, P, P, I64, P]),
             "lsg_last_error": (ctypes.c_char_p, []),
         }
         for name, (res, args) in sig.items():
@@ -152,6 +153,20 @@ class AdaptiveSparseGrid:
         pts = np.zeros((n.value, d), np.int32)
         _check(lib().lsg_grid_regular(d, level, _ptr(pts), n.value, ctypes.byref(n)))
         return cls(pts)
+
+    @classmethod
+    def adaptive(cls, d, level, refine, theta, target="corner", complete=True):
+        """Regular grid of `level`, `refine` refinement rounds toward the corner
+        (max_k x_k < theta 2^(1-r)) or the plane x_0 = 1/2, then the reference's
+        completeDirichletGrid (sgrid/sparseGrid.cc:771-787)."""
+        t = {"corner": 0, "plane": 1}[target]
+        n = ctypes.c_int64(0)
+        _check(lib().lsg_grid_adaptive(d, level, refine, theta, t, int(complete), None, None, 0, ctypes.byref(n)))
+        pts = np.zeros((n.value, d), np.int32)
+        act = np.zeros(n.value, np.uint8)
+        _check(lib().lsg_grid_adaptive(d, level, refine, theta, t, int(complete), _ptr(pts), _ptr(act), n.value,
+                                       ctypes.byref(n)))
+        return cls(pts, act)
 
     def getMaximalOccupiedSecondTable(self):
         return self.n

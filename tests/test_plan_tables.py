@@ -127,3 +127,16 @@ def test_invalid_grids_rejected():
         lsg.Plan(lsg.AdaptiveSparseGrid(np.array([[0, 2]], np.int32)))  # boundary point
     with pytest.raises(lsg.LsgError):
         lsg.Plan(lsg.AdaptiveSparseGrid(np.array([[2, 2], [2, 2]], np.int32)))  # duplicate
+
+
+def test_adaptive_generator_reproduces_reference(golden):
+    """Refinement + completeDirichletGrid restated in lsg_gridgen.cpp gives the
+    reference's grid: same points, same storage order, same hanging nodes."""
+    args = str(golden["gridargs"])
+    if "refine" not in args:
+        pytest.skip("regular grid")
+    kv = dict(a.split("=") for a in args.split())
+    g = lsg.AdaptiveSparseGrid.adaptive(int(golden["d"]), int(kv["level"]), int(kv["refine"]), float(kv["theta"]),
+                                        kv.get("target", "corner"))
+    assert np.array_equal(g.points, golden["points"])
+    assert np.array_equal(g.active, golden["active"])
