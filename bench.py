@@ -262,7 +262,7 @@ def main():
         "matvec": {"fp32_ms": ms32[4], "fp64_ms": ms64[4], "fp32_gbs": by32[4] / (ms32[4] * 1e-3) / 1e9,
                    "fp64_gbs": by64[4] / (ms64[4] * 1e-3) / 1e9, "phase_ms_fp32": list(ms32[:4]),
                    "cell_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9},
-        "roofline": {"bound": "hbm", "kernel": "k_phaseB (restriction wavefronts + cell operator)",
+        "roofline": {"bound": "hbm", "kernel": "phase B: k_cells (cell operator) + k_level (restriction wavefronts)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": peak_src, "traffic": None},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16 * g.n, "d2h_bytes_per_step": 8 * g.n},
