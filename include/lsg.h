@@ -140,6 +140,36 @@ int lsg_cg_solve_device(lsg_operator *op, const double *f, double *x, const lsg_
 /* Installs a diagonal preconditioner (n doubles, host) used by precond = 2. */
 int lsg_set_learned_diag(lsg_operator *op, const double *diag);
 
+/* ---- learned diagonal preconditioner (precond = 2).  A small MLP maps
+ * per-point features to a positive scaling s = softplus(o) of a cheap
+ * constant-coefficient diagonal b (exact for constant a on a complete grid):
+ * D = b * s.  No counterpart in the reference (its CG always uses the exact
+ * Jacobi diagonal, applications/cg_method.h:805); solves that stall with D
+ * fall back to the exact diagonal (lsg_solve_report.fell_back).
+ * Features (F = 5d + 2 floats per point, storage order): t_j / 8, x_j,
+ * next-to-boundary flags, log a(x), sum_j t_j / (8d), and
+ * log a(x +- h_j e_j) - log a(x) with h_j = 2^-t_j. */
+typedef struct lsg_mlp lsg_mlp;
+/* params: lsg_mlp_num_params(F) floats, layout W1[64][F] b1[64] W2[64][64] b2
+ * W3[64][64] b3 W4[64] b4; BF16-rounded weights, FP32 accumulation. */
+int64_t lsg_mlp_num_params(int32_t n_features);
+int lsg_mlp_create(int32_t n_features, const float *params, lsg_mlp **out);
+void lsg_mlp_destroy(lsg_mlp *m);
+int lsg_mlp_get_params(const lsg_mlp *m, float *params);
+/* out[r] = network output o for rows r < rows (device buffers, X rows x F) */
+int lsg_mlp_forward(lsg_mlp *m, const float *X, int64_t rows, float *out, void *stream);
+/* gradient of mean_r (log softplus(o_r) - Y_r)^2 w.r.t. the FP32 parameters (host
+ * copy; may be NULL) and the loss (host; may be NULL); X, Y device buffers */
+int lsg_mlp_gradient(lsg_mlp *m, const float *X, const float *Y, int64_t rows, float *grad, float *loss);
+/* one Adam step (beta 0.9/0.999) on that loss */
+int lsg_mlp_train_step(lsg_mlp *m, const float *X, const float *Y, int64_t rows, float lr, float *loss);
+const char *lsg_mlp_last_error(void);
+/* features (device, n x (5d+2) floats) and the cheap base diagonal (device, n doubles) */
+int lsg_operator_features(lsg_operator *op, float *feat, void *stream);
+int lsg_operator_base_diag(lsg_operator *op, double *base, void *stream);
+/* D = base * softplus(mlp(features)) at active points, installed for precond = 2 */
+int lsg_operator_install_learned(lsg_operator *op, lsg_mlp *m, void *stream);
+
 /* ---- host-only planner (no GPU needed): the flattened integer tables.
  * lsg_plan_create builds the same tables lsg_operator_create uploads, so the
  * tests can check them bit-exact against the reference's lookups on a CPU. */

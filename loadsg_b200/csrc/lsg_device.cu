@@ -572,6 +572,94 @@ __global__ void k_diag(DevPlan P, const double* __restrict__ acell, double* __re
     diag[k] = acc;
 }
 
+
+// ----------------------------------------------------------------------------- learned diagonal
+// Features of point k for the diagonal MLP (F = 5d + 2): depths t_j / 8,
+// coordinates x_j, next-to-boundary flags, log a(x), sum_j t_j / (8 d), and the
+// log-coefficient differences log a(x +- h_j e_j) - log a(x), h_j = 2^-t_j.
+__global__ void k_features(DevPlan P, int family, const double* __restrict__ params, float* __restrict__ feat) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= P.n) return;
+    int d = P.d, F = 5 * d + 2;
+    float* f = feat + k * F;
+    double x[lsg::kMaxDim], h[lsg::kMaxDim];
+    int tsum = 0;
+    for (int j = 0; j < d; ++j) {
+        int32_t idx = P.pts[k * d + j];
+        int t = 31 - __clz(idx);
+        int64_t c = 2 * (int64_t)(idx - (1 << t)) + 1;
+        h[j] = ldexp(1.0, -t);
+        x[j] = (double)c * h[j];
+        bool nb = (c - 1 == 0) || (c + 1 == ((int64_t)1 << t));
+        f[j] = t / 8.0f;
+        f[d + j] = (float)x[j];
+        f[2 * d + j] = nb ? 1.f : 0.f;
+        tsum += t;
+    }
+    double la = log(fmax(lsg_coef_eval_dev(family, params, d, x), 1e-300));
+    f[3 * d] = (float)la;
+    f[3 * d + 1] = tsum / (8.0f * d);
+    for (int j = 0; j < d; ++j) {
+        double xs = x[j];
+        x[j] = xs + h[j];
+        f[3 * d + 2 + 2 * j] = (float)(log(fmax(lsg_coef_eval_dev(family, params, d, x), 1e-300)) - la);
+        x[j] = xs - h[j];
+        f[3 * d + 3 + 2 * j] = (float)(log(fmax(lsg_coef_eval_dev(family, params, d, x), 1e-300)) - la);
+        x[j] = xs;
+    }
+}
+
+// Cheap diagonal a(x_k) * psi_k^T K_ref psi_k for a constant coefficient on a
+// complete level-T grid: per dimension the 1D sums over the six cells of the
+// prewavelet support factorise the tensor sum (exact when a is constant and
+// every cell exists).
+__global__ void k_base_diag(DevPlan P, int family, const double* __restrict__ params, double* __restrict__ base) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= P.n) return;
+    int d = P.d;
+    if (!P.act[k]) { base[k] = 0.0; return; }
+    double x[lsg::kMaxDim], sK[lsg::kMaxDim], sM[lsg::kMaxDim];
+    for (int j = 0; j < d; ++j) {
+        int32_t idx = P.pts[k * d + j];
+        int t = 31 - __clz(idx);
+        int64_t c = 2 * (int64_t)(idx - (1 << t)) + 1, top = (int64_t)1 << t;
+        double h = ldexp(1.0, -t);
+        x[j] = (double)c * h;
+        bool lok = c - 1 > 0, rok = c + 1 < top;
+        double w[7] = {0, 0, 0, 0, 0, 0, 0};
+        w[3] = (t > 1 && (!lok || !rok)) ? 0.9 : 1.0;
+        if (lok) { w[2] = -0.6; w[1] = 0.1; }
+        if (rok) { w[4] = -0.6; w[5] = 0.1; }
+        double a = 0, b = 0;
+        for (int q = 0; q < 6; ++q) {
+            int64_t m = c - 3 + q;
+            if (m < 0 || m >= top) continue;
+            double l = w[q], r = w[q + 1];
+            a += (l - r) * (l - r) / h;
+            b += h * (l * l + l * r + r * r) / 3.0;
+        }
+        sK[j] = a;
+        sM[j] = b;
+    }
+    double sum = 0.0;
+    for (int i = 0; i < d; ++i) {
+        double prod = sK[i];
+        for (int j = 0; j < d; ++j)
+            if (j != i) prod *= sM[j];
+        sum += prod;
+    }
+    base[k] = lsg_coef_eval_dev(family, params, d, x) * sum;
+}
+
+__global__ void k_install_learned(int64_t n, const uint8_t* __restrict__ act, const double* __restrict__ base,
+                                  const float* __restrict__ out, double* __restrict__ diag) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double o = out[k];
+    double sp = o > 30.0 ? o : log1p(exp(o));
+    diag[k] = act[k] ? base[k] * sp : 0.0;
+}
+
 // ----------------------------------------------------------------------------- vector kernels
 template <typename V>
 __global__ void k_zero_active(const int64_t* __restrict__ exa, int64_t na, V* __restrict__ y) {
@@ -705,7 +793,9 @@ struct lsg_operator {
     DBuf lam64, lam32;
     // coefficient
     bool have_coef = false;
+    int32_t family = 0;
     DBuf acell64, acell32, params;
+    DBuf feat, mlp_out, base;  // learned-diagonal work buffers
     // work buffers per precision
     struct Work {
         DBuf ml, pc, zb, gm, scratch, nscratch;
@@ -1097,6 +1187,7 @@ int lsg_operator_set_coefficient(lsg_operator* op, int32_t family, const double*
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaDeviceSynchronize());
     op->have_coef = true;
+    op->family = family;
     op->have_diag = false;
     return 0;
 }
@@ -1574,7 +1665,13 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
     cudaEventRecord(ev0, st);
     double ff = rc ? 0.0 : host_dot(S, f, f, st);
     if (!rc && o->precision == LSG_FP64) {
-        rc = cg_start<double>(S, f, x, S.r.as<double>(), S.d.as<double>(), S.h.as<double>(), zdiag, st);
+        DBuf x0;  // initial guess, kept for the fallback of a learned diagonal
+        if (!rc && o->precond == 2) {
+            size_t dummy = 0;
+            rc = x0.alloc(n * sizeof(double), &dummy);
+            if (!rc) CUDA_TRY(cudaMemcpyAsync(x0.p, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        }
+        if (!rc) rc = cg_start<double>(S, f, x, S.r.as<double>(), S.d.as<double>(), S.h.as<double>(), zdiag, st);
         int its = 0;
         double rr = 0.0;
         if (!rc)
@@ -1583,6 +1680,24 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
                                  &R.kernel_launches);
         R.iterations = its;
         R.outer_iterations = 1;
+        // learned diagonal that stalled (not converged, or non-finite): continue
+        // from the current iterate with the exact Jacobi diagonal
+        bool stalled = !rc && o->precond == 2 &&
+                       (o->criterion == 1 ? !(rr <= eps * eps * ff) : (its >= maxit || !std::isfinite(S.pin.h[3])));
+        if (stalled) {
+            R.fell_back = 1;
+            // restart from the initial guess if the iterate was spoiled by non-finite values
+            if (!std::isfinite(S.pin.h[3]) || !std::isfinite(rr))
+                CUDA_TRY(cudaMemcpyAsync(x, x0.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            rc = compute_diag(op, st);
+            const double* zj = op->diag.as<double>();
+            if (!rc) rc = cg_start<double>(S, f, x, S.r.as<double>(), S.d.as<double>(), S.h.as<double>(), zj, st);
+            if (!rc)
+                rc = cg_loop<double>(S, x, S.r.as<double>(), S.g.as<double>(), S.d.as<double>(), S.h.as<double>(), zj,
+                                     eps, o->criterion, eps * eps * ff, maxit, o->use_graph != 0, st, &its, &rr,
+                                     &R.kernel_launches);
+            R.iterations += its;
+        }
     } else if (!rc) {
         // FP32 inner CG inside FP64 iterative refinement
         int inner = o->inner_iter > 0 ? o->inner_iter : 30;
@@ -1594,6 +1709,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
         }
         double* r = S.r.as<double>();
         int total = 0, outer = 0;
+        double rr_prev = -1.0;
         for (outer = 0; outer < maxit && total < maxit * 4; ++outer) {
             CUDA_TRY(cudaMemsetAsync(r, 0, n * 8, st));
             rc = lsg_internal_matvec64(op, x, r, st);
@@ -1602,6 +1718,16 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             double rr = host_dot(S, r, r, st);
             if (!std::isfinite(rr)) { rc = fail(LSG_E_NOCONV, "non-finite residual"); break; }
             if (rr <= eps * eps * ff) break;
+            // a refinement step that did not halve the residual with the learned
+            // diagonal: switch to the exact Jacobi diagonal
+            if (o->precond == 2 && !R.fell_back && rr_prev > 0 && rr > 0.25 * rr_prev) {
+                R.fell_back = 1;
+                rc = compute_diag(op, st);
+                if (rc) break;
+                k_to_f32<<<nblk(n), 256, 0, st>>>(n, op->diag.as<double>(), S.z32.as<float>());
+                z32 = S.z32.as<float>();
+            }
+            rr_prev = rr;
             double nr = std::sqrt(rr);
             float* r32 = S.r32.as<float>();
             float* e32 = S.e32.as<float>();
@@ -1626,6 +1752,20 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             R.kernel_launches += matvec_launches(op->plan) + 12;
             if (rc) break;
             total += its;
+            if (!std::isfinite(lrr) || !std::isfinite(S.pin.h[3])) {
+                // the correction is unusable: drop it; with a learned diagonal switch to Jacobi
+                if (o->precond == 2 && !R.fell_back) {
+                    R.fell_back = 1;
+                    rc = compute_diag(op, st);
+                    if (rc) break;
+                    k_to_f32<<<nblk(n), 256, 0, st>>>(n, op->diag.as<double>(), S.z32.as<float>());
+                    z32 = S.z32.as<float>();
+                    rr_prev = -1.0;
+                    continue;
+                }
+                rc = fail(LSG_E_NOCONV, "non-finite inner residual");
+                break;
+            }
             k_axpy_f32<<<nblk(n), 256, 0, st>>>(n, nr, e32, x);
         }
         R.iterations = total;
@@ -1804,4 +1944,47 @@ extern "C" int lsg_matvec_device_noalloc(lsg_operator* op, const void* x, void* 
     cudaStream_t st = (cudaStream_t)stream;
     if (precision == LSG_FP64) return matvec_noalloc_dispatch<double>(op, (const double*)x, (double*)y, st, base);
     return matvec_noalloc_dispatch<float>(op, (const float*)x, (float*)y, st, base);
+}
+
+// ============================================================================= learned diagonal C-ABI
+struct lsg_mlp;
+extern "C" int lsg_mlp_forward(lsg_mlp* m, const float* X, int64_t rows, float* out, void* stream);
+
+extern "C" int lsg_operator_features(lsg_operator* op, float* feat, void* stream) {
+    if (!op || !feat) return fail(LSG_E_INVALID, "null argument");
+    if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
+    k_features<<<nblk(op->plan.n, 128), 128, 0, (cudaStream_t)stream>>>(op->dp, op->family, op->params.as<double>(), feat);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int lsg_operator_base_diag(lsg_operator* op, double* base, void* stream) {
+    if (!op || !base) return fail(LSG_E_INVALID, "null argument");
+    if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
+    k_base_diag<<<nblk(op->plan.n, 128), 128, 0, (cudaStream_t)stream>>>(op->dp, op->family, op->params.as<double>(), base);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int lsg_operator_install_learned(lsg_operator* op, lsg_mlp* m, void* stream) {
+    if (!op || !m) return fail(LSG_E_INVALID, "null argument");
+    if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
+    int64_t n = op->plan.n;
+    int F = 5 * op->plan.d + 2;
+    size_t* tot = &op->dev_bytes;
+    int rc = 0;
+    if (!op->feat.p) rc |= op->feat.alloc((size_t)n * F * sizeof(float), tot);
+    if (!op->mlp_out.p) rc |= op->mlp_out.alloc((size_t)n * sizeof(float), tot);
+    if (!op->base.p) rc |= op->base.alloc((size_t)n * sizeof(double), tot);
+    if (!op->learned.p) rc |= op->learned.alloc((size_t)n * sizeof(double), tot);
+    if (rc) return LSG_E_CUDA;
+    rc = lsg_operator_features(op, op->feat.as<float>(), stream);
+    if (!rc) rc = lsg_operator_base_diag(op, op->base.as<double>(), stream);
+    if (!rc) rc = lsg_mlp_forward(m, op->feat.as<float>(), n, op->mlp_out.as<float>(), stream);
+    if (rc) return rc;
+    k_install_learned<<<nblk(n), 256, 0, (cudaStream_t)stream>>>(n, op->act.as<uint8_t>(), op->base.as<double>(),
+                                                                 op->mlp_out.as<float>(), op->learned.as<double>());
+    CUDA_TRY(cudaGetLastError());
+    op->have_learned = true;
+    return 0;
 }
