@@ -115,8 +115,8 @@ typedef struct {
     int32_t max_iter;    /* 0 = 500 (cg_method.h:35) */
     int32_t precond;     /* 0 Jacobi (reference), 1 none, 2 learned diagonal (see lsg_set_learned_diag) */
     int32_t precision;   /* LSG_FP64: plain CG; LSG_FP32: FP32 inner CG in FP64 iterative refinement */
-    int32_t inner_iter;  /* FP32+IR: inner iterations per refinement step (0 = 30) */
-    double inner_tol;    /* FP32+IR: inner relative reduction (0 = 1e-4) */
+    int32_t inner_iter;  /* FP32+IR: inner iterations per refinement step (0 = 1000) */
+    double inner_tol;    /* FP32+IR: inner relative reduction (0 = 1e-5) */
     int32_t use_graph;   /* capture one CG iteration as a CUDA graph */
 } lsg_solver_opts;
 
@@ -169,6 +169,34 @@ int lsg_operator_features(lsg_operator *op, float *feat, void *stream);
 int lsg_operator_base_diag(lsg_operator *op, double *base, void *stream);
 /* D = base * softplus(mlp(features)) at active points, installed for precond = 2 */
 int lsg_operator_install_learned(lsg_operator *op, lsg_mlp *m, void *stream);
+
+/* ---- batched operators and solves: many grids of uneven size (any mix of
+ * dimensions), each with its own coefficient and right-hand side, applied and
+ * solved together.  Grids of one dimension are concatenated into one
+ * operator, so a matvec of the whole group is one launch per level step; the
+ * batched CG keeps per-grid scalars and convergence, and one iteration of the
+ * whole batch is captured as one CUDA graph.  A batch vector holds the grids'
+ * vectors side by side: grid i occupies [offsets[i], offsets[i+1]) in storage
+ * order (lsg_batch_offsets; grids are grouped by dimension, so the order of
+ * the ranges can differ from the input order).  No counterpart in the
+ * reference, which builds one MatrixVectorHomogen per grid
+ * (MatrixVectorMultiplication/MatrixVectorHomogen.h:72-77). */
+typedef struct lsg_batch lsg_batch;
+int lsg_batch_create(int32_t count, const int32_t *dims, const int32_t *const *points, const uint8_t *const *active,
+                     const int64_t *n, lsg_batch **out);
+void lsg_batch_destroy(lsg_batch *b);
+int64_t lsg_batch_size(const lsg_batch *b);
+/* offsets[i] = start of grid i in a batch vector; offsets[count] = total size */
+int lsg_batch_offsets(const lsg_batch *b, int64_t *offsets);
+int lsg_batch_set_coefficient(lsg_batch *b, int32_t grid, int32_t family, const double *params, int32_t nparams);
+/* y = A x for every grid (device batch vectors; inactive entries untouched) */
+int lsg_batch_matvec_device(lsg_batch *b, const void *x, void *y, int32_t precision, void *stream);
+/* CG of every grid (precond 0 or 1; FP64 or FP32+IR); reports[count] per grid
+ * and *total for the batch (may be NULL).  Device / host batch vectors. */
+int lsg_batch_cg_solve_device(lsg_batch *b, const double *f, double *x, const lsg_solver_opts *opts,
+                              lsg_solve_report *reports, lsg_solve_report *total, void *stream);
+int lsg_batch_cg_solve(lsg_batch *b, const double *f, double *x, const lsg_solver_opts *opts,
+                       lsg_solve_report *reports, lsg_solve_report *total);
 
 /* ---- host-only planner (no GPU needed): the flattened integer tables.
  * lsg_plan_create builds the same tables lsg_operator_create uploads, so the

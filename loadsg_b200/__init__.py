@@ -109,6 +109,14 @@ def lib():
             "lsg_plan_export_stencil": (ctypes.c_int, [P, I64, P, P, P]),
             "lsg_grid_regular": (ctypes.c_int, [I32, I32, P, I64, P]),
             "lsg_grid_adaptive": (ctypes.c_int, [I32, I32, I32, D, I32, I32, P, P, I64, P]),
+            "lsg_batch_create": (ctypes.c_int, [I32, P, P, P, P, P]),
+            "lsg_batch_destroy": (None, [P]),
+            "lsg_batch_size": (I64, [P]),
+            "lsg_batch_offsets": (ctypes.c_int, [P, P]),
+            "lsg_batch_set_coefficient": (ctypes.c_int, [P, I32, I32, P, I32]),
+            "lsg_batch_matvec_device": (ctypes.c_int, [P, P, P, I32, P]),
+            "lsg_batch_cg_solve_device": (ctypes.c_int, [P, P, P, P, P, P, P]),
+            "lsg_batch_cg_solve": (ctypes.c_int, [P, P, P, P, P, P]),
             "lsg_last_error": (ctypes.c_char_p, []),
         }
         for name, (res, args) in sig.items():
@@ -328,7 +336,7 @@ class MatrixVectorHomogen:
 class CG:
     @staticmethod
     def solveHomogen(eps, x, f, matrix, problem, criterion=0, max_iter=500, precond=0, precision=FP64,
-                     inner_iter=30, inner_tol=1e-4, use_graph=True):
+                     inner_iter=1000, inner_tol=1e-5, use_graph=True):
         """CG::solveHomogen (applications/cg_method.h:759-886).  x (in/out) and f
         are host float64 arrays.  criterion 0 is the reference's stopping rule on
         r^T D^-1 r; criterion 1 stops at ||f - A x|| / ||f|| <= eps.  Returns the
@@ -348,3 +356,76 @@ class CG:
         _check(lib().lsg_cg_solve_device(matrix._h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(x_ptr),
                                          ctypes.byref(opts), ctypes.byref(rep), ctypes.c_void_p(stream)))
         return {k: getattr(rep, k) for k, _ in SolveReport._fields_}
+
+
+# --------------------------------------------------------------------------- batches
+def _report(rep):
+    return {k: getattr(rep, k) for k, _ in SolveReport._fields_}
+
+
+class Batch:
+    """Many grids (any mix of dimensions and sizes), each with its own
+    coefficient, applied and solved together (lsg_batch_* in include/lsg.h).
+    Batch vectors hold the grids' vectors side by side: grid i is
+    ``v[offsets[i]:offsets[i+1]]`` in its own storage order."""
+
+    def __init__(self, grids, problems=None):
+        self.grids = list(grids)
+        k = len(self.grids)
+        dims = np.array([g.d for g in self.grids], np.int32)
+        pts = (ctypes.c_void_p * k)(*[g.points.ctypes.data for g in self.grids])
+        act = (ctypes.c_void_p * k)(*[g.active.ctypes.data for g in self.grids])
+        ns = np.array([g.n for g in self.grids], np.int64)
+        h = ctypes.c_void_p()
+        _check(lib().lsg_batch_create(k, _ptr(dims), pts, act, _ptr(ns), ctypes.byref(h)))
+        self._h = h
+        self._destroy = lib().lsg_batch_destroy
+        off = np.zeros(k + 1, np.int64)
+        _check(lib().lsg_batch_offsets(self._h, _ptr(off)))
+        self.offsets = off[:-1]
+        self.size = int(off[-1])
+        if problems is not None:
+            for i, p in enumerate(problems):
+                self.set_problem(i, p)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._destroy(self._h)
+            self._h = None
+
+    def set_problem(self, i, problem):
+        _check(lib().lsg_batch_set_coefficient(self._h, i, problem.family, _ptr(problem.params), problem.nparams))
+
+    def gather(self, parts):
+        """Batch vector from per-grid host arrays."""
+        v = np.zeros(self.size)
+        for i, a in enumerate(parts):
+            v[self.offsets[i]:self.offsets[i] + self.grids[i].n] = a
+        return v
+
+    def split(self, v):
+        return [v[self.offsets[i]:self.offsets[i] + self.grids[i].n] for i in range(len(self.grids))]
+
+    def matvec_device(self, x_ptr, y_ptr, precision=FP64, stream=0):
+        _check(lib().lsg_batch_matvec_device(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), precision,
+                                             ctypes.c_void_p(stream)))
+
+    def solve(self, eps, x, f, criterion=1, max_iter=500, precond=0, precision=FP64, inner_iter=1000,
+              inner_tol=1e-5, use_graph=True):
+        """CG of every grid; x (in/out) and f are host batch vectors.  Returns
+        (per-grid reports, batch report)."""
+        if x.dtype != np.float64 or not x.flags.c_contiguous:
+            raise ValueError("x must be a contiguous float64 array")
+        f = np.ascontiguousarray(f, np.float64)
+        o = SolverOpts(eps, criterion, max_iter, precond, precision, inner_iter, inner_tol, int(use_graph))
+        reps = (SolveReport * len(self.grids))()
+        tot = SolveReport()
+        _check(lib().lsg_batch_cg_solve(self._h, _ptr(f), _ptr(x), ctypes.byref(o), reps, ctypes.byref(tot)))
+        return [_report(r) for r in reps], _report(tot)
+
+    def solve_device(self, f_ptr, x_ptr, opts, stream=0):
+        reps = (SolveReport * len(self.grids))()
+        tot = SolveReport()
+        _check(lib().lsg_batch_cg_solve_device(self._h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(x_ptr),
+                                               ctypes.byref(opts), reps, ctypes.byref(tot), ctypes.c_void_p(stream)))
+        return [_report(r) for r in reps], _report(tot)

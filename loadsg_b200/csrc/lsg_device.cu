@@ -15,6 +15,7 @@
 //   CG kernels   CG::solveHomogen vector semantics (cg_method.h:759-886)
 #include "lsg_plan.h"
 #include "lsg_coef.cuh"
+#include "lsg_internal.h"
 #include "../../include/lsg.h"
 
 #include <cuda_runtime.h>
@@ -463,13 +464,15 @@ __global__ void __launch_bounds__(128) k_level(DevPlan P, const V* __restrict__ 
 }
 
 // ----------------------------------------------------------------------------- coefficient, diag
-template <typename V>
-__global__ void k_cell_coef(DevPlan P, int64_t C, int family, const double* __restrict__ params,
-                            double* __restrict__ a64, float* __restrict__ a32, const int64_t* __restrict__ cell_slab_off) {
-    int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (gi >= C) return;
+// a(x_c) at the midpoint of every cell of one part of the plan (cells
+// [c_lo, c_hi) on slabs [t_lo, t_hi)); the part's family and parameters
+__global__ void k_cell_coef(DevPlan P, int64_t c_lo, int64_t c_hi, int t_lo, int t_hi, int family,
+                            const double* __restrict__ params, double* __restrict__ a64, float* __restrict__ a32,
+                            const int64_t* __restrict__ cell_slab_off) {
+    int64_t gi = c_lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (gi >= c_hi) return;
     // slab of this cell (cell_slab_off is the prefix of cell counts)
-    int lo = 0, hi = P.nD;
+    int lo = t_lo, hi = t_hi;
     while (hi - lo > 1) {
         int mid = (lo + hi) / 2;
         if (cell_slab_off[mid] <= gi) lo = mid;
@@ -791,9 +794,10 @@ struct lsg_operator {
     DBuf slabs, did, act, exa_off, exa, cell_key, cell_corner, nodal_stage, nodal_src, nodal_code, nodal_dom, nodal_scr,
         conv_stage, conv_src, conv_code, conv_dom, prol, restr, a_items, b_items, b_steps, pts, cell_slab_off;
     DBuf lam64, lam32;
-    // coefficient
+    // coefficient (one family and parameter set per part of a concatenated plan)
     bool have_coef = false;
     int32_t family = 0;
+    std::vector<uint8_t> part_coef;
     DBuf acell64, acell32, params;
     DBuf feat, mlp_out, base;  // learned-diagonal work buffers
     // work buffers per precision
@@ -1110,6 +1114,79 @@ static int lsg_internal_matvec32(lsg_operator* op, const float* x, float* y, cud
 static const uint8_t* lsg_internal_active(lsg_operator* op);
 
 // ============================================================================= C-ABI
+namespace lsg_internal {
+
+int create_from_plan(lsg::Plan&& plan, lsg_operator** out) {
+    *out = nullptr;
+    std::unique_ptr<lsg_operator> op(new lsg_operator());
+    op->plan = std::move(plan);
+    CUDA_TRY(cudaGetDevice(&op->device));
+    op->part_coef.assign(op->plan.inst_n_off.size() - 1, 0);
+    int rc = upload_plan(op.get());
+    if (rc) return rc;
+    *out = op.release();
+    return 0;
+}
+
+int set_part_coefficient(lsg_operator* op, int part, int32_t family, const double* params, int32_t nparams) {
+    if (!op) return fail(LSG_E_INVALID, "null operator");
+    const lsg::Plan& p = op->plan;
+    int nparts = (int)p.inst_n_off.size() - 1;
+    if (part < 0 || part >= nparts) return fail(LSG_E_INVALID, "part index out of range");
+    if (family < 0 || family > 4) return fail(LSG_E_INVALID, "unknown coefficient family");
+    if (nparams < 0 || nparams > LSG_MAX_COEF_PARAMS || (nparams > 0 && !params))
+        return fail(LSG_E_INVALID, "bad coefficient parameters");
+    std::vector<double> pv(LSG_MAX_COEF_PARAMS, 0.0);
+    for (int i = 0; i < nparams; ++i) pv[i] = params[i];
+    size_t* tot = &op->dev_bytes;
+    int rc = 0;
+    if (!op->params.p) rc |= op->params.alloc((size_t)nparts * LSG_MAX_COEF_PARAMS * sizeof(double), tot);
+    if (!op->acell64.p) {
+        rc |= op->acell64.alloc(std::max<int64_t>(p.C, 1) * sizeof(double), tot);
+        rc |= op->acell32.alloc(std::max<int64_t>(p.C, 1) * sizeof(float), tot);
+    }
+    if (rc) return LSG_E_CUDA;
+    double* pp = op->params.as<double>() + (size_t)part * LSG_MAX_COEF_PARAMS;
+    CUDA_TRY(cudaMemcpy(pp, pv.data(), pv.size() * sizeof(double), cudaMemcpyHostToDevice));
+    int64_t c_lo = p.inst_c_off[part], c_hi = p.inst_c_off[part + 1];
+    if (c_hi > c_lo)
+        k_cell_coef<<<nblk(c_hi - c_lo), 256>>>(op->dp, c_lo, c_hi, p.inst_t_off[part], p.inst_t_off[part + 1], family,
+                                                pp, op->acell64.as<double>(), op->acell32.as<float>(),
+                                                op->cell_slab_off.as<int64_t>());
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaDeviceSynchronize());
+    op->part_coef[part] = 1;
+    op->have_coef = std::all_of(op->part_coef.begin(), op->part_coef.end(), [](uint8_t v) { return v != 0; });
+    op->family = family;
+    op->have_diag = false;
+    return 0;
+}
+
+int matvec64(lsg_operator* op, const double* x, double* y, cudaStream_t st) { return matvec_dispatch<double>(op, x, y, st); }
+int matvec32(lsg_operator* op, const float* x, float* y, cudaStream_t st) { return matvec_dispatch<float>(op, x, y, st); }
+int prepare_precision(lsg_operator* op, bool fp32) {
+    int rc = prepare<double>(op);
+    if (!rc && fp32) rc = prepare<float>(op);
+    return rc;
+}
+const uint8_t* active(lsg_operator* op) { return op->act.as<uint8_t>(); }
+int jacobi_diag(lsg_operator* op, cudaStream_t st, const double** diag) {
+    int rc = op->have_diag ? 0 : compute_diag(op, st);
+    *diag = op->diag.as<double>();
+    return rc;
+}
+bool has_coefficient(const lsg_operator* op) { return op->have_coef; }
+const lsg::Plan& plan(const lsg_operator* op) { return op->plan; }
+size_t device_bytes(const lsg_operator* op) { return op->dev_bytes; }
+int64_t matvec_launch_count(const lsg_operator* op) {
+    const lsg::Plan& p = op->plan;
+    return 3 + (int64_t)(p.a_level_off.size() - 1) + (int64_t)op->cell_class_off.size() - 1 +
+           (int64_t)(p.b_level_off.size() - 1);
+}
+int fail_msg(int code, const char* msg) { return fail(code, msg); }
+
+}  // namespace lsg_internal
+
 extern "C" {
 
 const char* lsg_last_error(void) { return g_err.c_str(); }
@@ -1121,13 +1198,9 @@ int lsg_operator_create(int32_t d, const int32_t* points, const uint8_t* active,
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0)
         return fail(LSG_E_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
-    std::unique_ptr<lsg_operator> op(new lsg_operator());
-    if (!lsg::build_plan(d, n, points, active, op->plan)) return fail(LSG_E_INVALID, op->plan.error);
-    CUDA_TRY(cudaGetDevice(&op->device));
-    int rc = upload_plan(op.get());
-    if (rc) return rc;
-    *out = op.release();
-    return 0;
+    lsg::Plan plan;
+    if (!lsg::build_plan(d, n, points, active, plan)) return fail(LSG_E_INVALID, plan.error);
+    return lsg_internal::create_from_plan(std::move(plan), out);
 }
 
 void lsg_operator_destroy(lsg_operator* op) { delete op; }
@@ -1166,29 +1239,11 @@ int lsg_operator_info(const lsg_operator* op, lsg_info* info) {
 
 int lsg_operator_set_coefficient(lsg_operator* op, int32_t family, const double* params, int32_t nparams) {
     if (!op) return fail(LSG_E_INVALID, "null operator");
-    if (family < 0 || family > 4) return fail(LSG_E_INVALID, "unknown coefficient family");
-    if (nparams < 0 || nparams > LSG_MAX_COEF_PARAMS || (nparams > 0 && !params))
-        return fail(LSG_E_INVALID, "bad coefficient parameters");
-    std::vector<double> pv(LSG_MAX_COEF_PARAMS, 0.0);
-    for (int i = 0; i < nparams; ++i) pv[i] = params[i];
-    size_t* tot = &op->dev_bytes;
-    int rc = 0;
-    if (!op->params.p) rc |= op->params.alloc(pv.size() * sizeof(double), tot);
-    if (!op->acell64.p) {
-        rc |= op->acell64.alloc(std::max<int64_t>(op->plan.C, 1) * sizeof(double), tot);
-        rc |= op->acell32.alloc(std::max<int64_t>(op->plan.C, 1) * sizeof(float), tot);
+    int nparts = (int)op->plan.inst_n_off.size() - 1;
+    for (int b = 0; b < nparts; ++b) {
+        int rc = lsg_internal::set_part_coefficient(op, b, family, params, nparams);
+        if (rc) return rc;
     }
-    if (rc) return LSG_E_CUDA;
-    CUDA_TRY(cudaMemcpy(op->params.p, pv.data(), pv.size() * sizeof(double), cudaMemcpyHostToDevice));
-    if (op->plan.C > 0)
-        k_cell_coef<double><<<nblk(op->plan.C), 256>>>(op->dp, op->plan.C, family, op->params.as<double>(),
-                                                       op->acell64.as<double>(), op->acell32.as<float>(),
-                                                       op->cell_slab_off.as<int64_t>());
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaDeviceSynchronize());
-    op->have_coef = true;
-    op->family = family;
-    op->have_diag = false;
     return 0;
 }
 
@@ -1700,8 +1755,8 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
         }
     } else if (!rc) {
         // FP32 inner CG inside FP64 iterative refinement
-        int inner = o->inner_iter > 0 ? o->inner_iter : 30;
-        double itol = o->inner_tol > 0 ? o->inner_tol : 1e-4;
+        int inner = o->inner_iter > 0 ? o->inner_iter : 1000;
+        double itol = o->inner_tol > 0 ? o->inner_tol : 1e-5;
         float* z32 = nullptr;
         if (zdiag) {
             k_to_f32<<<nblk(n), 256, 0, st>>>(n, zdiag, S.z32.as<float>());

@@ -715,7 +715,183 @@ bool build_plan(int d, int64_t n, const int32_t* points, const uint8_t* active, 
     p.nodal_scratch = 0;
     for (int t = 0; t < nD; ++t)
         for (int j = 1; j < d; ++j) p.nodal_scratch += p.nodal_dom[t * (d + 1) + j];
+    p.inst_n_off = {0, n};
+    p.inst_t_off = {0, nD};
+    p.inst_c_off = {0, p.C};
+    p.slab_inst.assign(nD, 0);
     p.plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return true;
+}
+
+namespace {
+template <typename T>
+void append_shift(std::vector<T>& dst, const std::vector<T>& src, T shift, bool keep_negative) {
+    dst.reserve(dst.size() + src.size());
+    for (T v : src) dst.push_back((keep_negative && v < 0) ? v : v + shift);
+}
+
+// scratch elements of one phase-B item (slab, restriction outputs, convert stages)
+int64_t item_scratch(const Plan& p, const PhaseBItem& it) {
+    int64_t scr = p.slabs[it.t].n;
+    for (int32_t k = it.step_begin; k < it.step_end; ++k) scr += p.b_steps[k].n_dst;
+    if (it.t_conv >= 0)
+        for (int j = 1; j < p.d; ++j) scr += p.convert_dom[it.t_conv * (p.d + 1) + j];
+    return scr;
+}
+}  // namespace
+
+bool concat_plans(const std::vector<const Plan*>& parts, Plan& q) {
+    if (parts.empty()) { q.error = "no plans to concatenate"; return false; }
+    const int d = parts[0]->d;
+    for (const Plan* p : parts)
+        if (p->d != d) { q.error = "plans of different dimension"; return false; }
+    q = Plan();
+    q.d = d;
+    q.ncase = 1 << d;
+    q.maxdep.assign(d, 0);
+    q.sorted.assign(q.ncase, {});
+    q.inst_n_off.assign(1, 0);
+    q.inst_t_off.assign(1, 0);
+    q.inst_c_off.assign(1, 0);
+    int64_t cornerb = 0, prolb = 0, restrb = 0, nsb = 0, csb = 0;
+    std::vector<int64_t> pb, gmb, prolbv;
+    std::vector<int32_t> stepb;
+    for (size_t b = 0; b < parts.size(); ++b) {
+        const Plan& p = *parts[b];
+        const int64_t nb = q.n, Mb = q.M, Cb = q.C;
+        const int32_t tb = q.nD;
+        q.pts.insert(q.pts.end(), p.pts.begin(), p.pts.end());
+        q.act.insert(q.act.end(), p.act.begin(), p.act.end());
+        q.D.insert(q.D.end(), p.D.begin(), p.D.end());
+        append_shift<int32_t>(q.did, p.did, tb, false);
+        for (int j = 0; j < d; ++j) q.maxdep[j] = std::max(q.maxdep[j], p.maxdep[j]);
+        // exact-depth lists: offsets arrays have nD+1 entries
+        if (q.ex_off.empty()) { q.ex_off.push_back(0); q.exa_off.push_back(0); }
+        for (int t = 1; t <= p.nD; ++t) {
+            q.ex_off.push_back(p.ex_off[t] + (int64_t)q.ex.size());
+            q.exa_off.push_back(p.exa_off[t] + (int64_t)q.exa.size());
+        }
+        append_shift<int64_t>(q.ex, p.ex, nb, false);
+        append_shift<int64_t>(q.exa, p.exa, nb, false);
+        // slabs and cells
+        for (int t = 0; t < p.nD; ++t) {
+            Slab s = p.slabs[t];
+            s.off += Mb;
+            s.cell_off += Cb;
+            if (s.corner_off >= 0) s.corner_off += cornerb;
+            q.slabs.push_back(s);
+            q.slab_inst.push_back((int32_t)b);
+        }
+        append_shift<int64_t>(q.slab_pt, p.slab_pt, nb, false);
+        q.slab_key.insert(q.slab_key.end(), p.slab_key.begin(), p.slab_key.end());
+        q.cell_key.insert(q.cell_key.end(), p.cell_key.begin(), p.cell_key.end());
+        q.cell_corner.insert(q.cell_corner.end(), p.cell_corner.begin(), p.cell_corner.end());
+        cornerb += (int64_t)p.cell_key.size();
+        // stencil stage tables: stage_off has nD*d+1 entries, sources are local
+        for (int k = 0; k < p.nD * d; ++k) q.nodal.stage_off.push_back(p.nodal.stage_off[k] + nsb);
+        for (int k = 0; k < p.nD * d; ++k) q.convert.stage_off.push_back(p.convert.stage_off[k] + csb);
+        nsb += p.nodal.stage_off[p.nD * d];
+        csb += p.convert.stage_off[p.nD * d];
+        q.nodal.src.insert(q.nodal.src.end(), p.nodal.src.begin(), p.nodal.src.end());
+        q.nodal.code.insert(q.nodal.code.end(), p.nodal.code.begin(), p.nodal.code.end());
+        q.convert.src.insert(q.convert.src.end(), p.convert.src.begin(), p.convert.src.end());
+        q.convert.code.insert(q.convert.code.end(), p.convert.code.begin(), p.convert.code.end());
+        q.nodal_dom.insert(q.nodal_dom.end(), p.nodal_dom.begin(), p.nodal_dom.end());
+        q.convert_dom.insert(q.convert_dom.end(), p.convert_dom.begin(), p.convert_dom.end());
+        // prolongation / restriction tables (positions inside slabs are local)
+        append_shift<int64_t>(q.prol_tab, p.prol_tab, prolb, true);
+        q.prol.insert(q.prol.end(), p.prol.begin(), p.prol.end());
+        q.restr.insert(q.restr.end(), p.restr.begin(), p.restr.end());
+        for (int c = 0; c < q.ncase; ++c) append_shift<int32_t>(q.sorted[c], p.sorted[c], tb, false);
+        pb.push_back(q.p_total);
+        gmb.push_back(q.gm_total);
+        prolbv.push_back(prolb);
+        stepb.push_back((int32_t)q.b_steps.size());
+        for (PhaseBStep st : p.b_steps) {
+            st.t_dst += tb;
+            st.tab_off += restrb;
+            st.gm_off += q.gm_total;
+            q.b_steps.push_back(st);
+        }
+        prolb += (int64_t)p.prol.size();
+        restrb += (int64_t)p.restr.size();
+        q.p_total += p.p_total;
+        q.gm_total += p.gm_total;
+        q.n += p.n;
+        q.nD += p.nD;
+        q.M += p.M;
+        q.C += p.C;
+        q.max_slab = std::max(q.max_slab, p.max_slab);
+        q.nodal_scratch += p.nodal_scratch;
+        q.plan_seconds += p.plan_seconds;
+        q.inst_n_off.push_back(q.n);
+        q.inst_t_off.push_back(q.nD);
+        q.inst_c_off.push_back(q.C);
+    }
+    q.nodal.nsrc = 3;
+    q.convert.nsrc = 5;
+    q.nodal.stage_off.push_back(nsb);
+    q.convert.stage_off.push_back(csb);
+    // p_slab_off / gm_slab_off indexed (case, depth id) over the merged depth list
+    q.p_slab_off.assign((size_t)q.ncase * q.nD, -1);
+    q.gm_slab_off.assign((size_t)q.ncase * q.nD, -1);
+    for (size_t b = 0; b < parts.size(); ++b) {
+        const Plan& p = *parts[b];
+        for (int c = 0; c < q.ncase; ++c)
+            for (int t = 0; t < p.nD; ++t) {
+                int64_t po = p.p_slab_off[(size_t)c * p.nD + t], go = p.gm_slab_off[(size_t)c * p.nD + t];
+                size_t at = (size_t)c * q.nD + q.inst_t_off[b] + t;
+                q.p_slab_off[at] = po < 0 ? -1 : po + pb[b];
+                q.gm_slab_off[at] = go < 0 ? -1 : go + gmb[b];
+            }
+    }
+    // phase A levels merged by index
+    size_t la = 0;
+    for (const Plan* p : parts) la = std::max(la, p->a_level_off.size() - 1);
+    for (size_t L = 0; L < la; ++L) {
+        q.a_level_off.push_back((int32_t)q.a_items.size());
+        for (size_t b = 0; b < parts.size(); ++b) {
+            const Plan& p = *parts[b];
+            if (L + 1 >= p.a_level_off.size()) continue;
+            for (int32_t i = p.a_level_off[L]; i < p.a_level_off[L + 1]; ++i) {
+                PhaseAItem a = p.a_items[i];
+                a.t_src += q.inst_t_off[b];
+                a.t_dst += q.inst_t_off[b];
+                a.src_off += pb[b];
+                a.dst_off += pb[b];
+                a.tab_off += prolbv[b];
+                q.a_items.push_back(a);
+            }
+        }
+    }
+    q.a_level_off.push_back((int32_t)q.a_items.size());
+    // phase B levels merged by index; scratch arenas laid out side by side
+    size_t lb = 0;
+    for (const Plan* p : parts) lb = std::max(lb, p->b_level_off.size() - 1);
+    q.scratch_total = 0;
+    for (size_t L = 0; L < lb; ++L) {
+        q.b_level_off.push_back((int32_t)q.b_items.size());
+        int64_t arena = 0;
+        for (size_t b = 0; b < parts.size(); ++b) {
+            const Plan& p = *parts[b];
+            if (L + 1 >= p.b_level_off.size()) continue;
+            for (int32_t i = p.b_level_off[L]; i < p.b_level_off[L + 1]; ++i) {
+                PhaseBItem it = p.b_items[i];
+                int64_t need = item_scratch(p, it);
+                it.t += q.inst_t_off[b];
+                if (it.t_conv >= 0) it.t_conv += q.inst_t_off[b];
+                it.p_off += pb[b];
+                it.gm_off += gmb[b];
+                it.step_begin += stepb[b];
+                it.step_end += stepb[b];
+                it.scratch_off = arena;
+                arena += need;
+                q.b_items.push_back(it);
+            }
+        }
+        q.scratch_total = std::max(q.scratch_total, arena);
+    }
+    q.b_level_off.push_back((int32_t)q.b_items.size());
     return true;
 }
 

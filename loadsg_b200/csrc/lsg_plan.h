@@ -115,6 +115,11 @@ struct Plan {
     int64_t scratch_total = 0;         // max over levels of per-level scratch
     int64_t nodal_scratch = 0;
     int64_t max_slab = 0;              // max N_T
+    // instances of a concatenated plan (concat_plans); one instance otherwise
+    std::vector<int64_t> inst_n_off;   // point offsets, size instances+1
+    std::vector<int32_t> inst_t_off;   // depth-id offsets
+    std::vector<int64_t> inst_c_off;   // cell offsets
+    std::vector<int32_t> slab_inst;    // instance of every slab (depth id)
     // statistics
     double plan_seconds = 0.0;
     std::string error;
@@ -122,6 +127,14 @@ struct Plan {
 
 // Builds the plan; returns false and sets plan.error on invalid input.
 bool build_plan(int d, int64_t n, const int32_t* points, const uint8_t* active, Plan& plan);
+
+// Concatenates plans of the same dimension into one plan whose launches cover
+// every part: all offsets are shifted, and the level schedules of phases A and
+// B are merged by level index.  The parts are independent grids, so only each
+// part's own level order has to be kept; a merged level runs the level-L items
+// of all parts side by side.  The per-item arithmetic is unchanged, so a
+// part's result equals the result of its own plan bit for bit.
+bool concat_plans(const std::vector<const Plan*>& parts, Plan& out);
 
 // Helpers shared with the tests / C-ABI.
 int depth1(int32_t i);

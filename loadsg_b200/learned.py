@@ -88,10 +88,11 @@ class MLP:
         h = ctypes.c_void_p()
         _mcheck(_mlp_lib().lsg_mlp_create(F, _ptr(p), ctypes.byref(h)))
         self._h = h
+        self._destroy = _mlp_lib().lsg_mlp_destroy  # kept: module globals are gone at interpreter exit
 
     def __del__(self):
         if getattr(self, "_h", None):
-            _mlp_lib().lsg_mlp_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     def params(self):
