@@ -104,6 +104,33 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def host_cores():
+    """Cores this process may run on: the affinity mask, capped by a cgroup CPU
+    quota when one is set (os.cpu_count() reports the whole host, and OpenMP
+    with more threads than the quota allows slows to a crawl)."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    try:
+        quota, period = open("/sys/fs/cgroup/cpu.max").read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(int(quota) // int(period))))
+    except (OSError, ValueError):
+        pass
+    return max(1, n)
+
+
+def workload_points(name):
+    """Point count of a workload grid (host-side grid generator, no GPU)."""
+    import loadsg_b200 as lsg
+    if name == "d6_adaptive_corner":
+        return lsg.AdaptiveSparseGrid.adaptive(6, 7, 3, 0.6, "corner").n
+    if name.startswith("d6_regular_L"):
+        return lsg.AdaptiveSparseGrid.regular(6, int(name.split("L")[1])).n
+    return lsg.AdaptiveSparseGrid.regular(3, 7).n
+
+
 def cpu_reference_sample(args):
     """The reference's own CG (oracle/_ref, compiled from the LoAdSG sources) on
     the largest instance of the workload family it handles in seconds."""
@@ -112,8 +139,8 @@ def cpu_reference_sample(args):
     level = 3 if d == 6 else 5
     if not os.path.exists(exe):
         return {"value": None, "unit": "s", "cores": 0, "kind": "reference", "sample": f"{exe} missing"}
-    cores = os.cpu_count() or 1
-    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    cores = host_cores()
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_WAIT_POLICY="PASSIVE")
     rng = np.random.default_rng(0)
     with tempfile.TemporaryDirectory() as tmp:
         subprocess.run([exe, "grid", tmp, f"level={level}"], check=True, capture_output=True, env=env)
@@ -125,16 +152,80 @@ def cpu_reference_sample(args):
                ["coef=1", "cp=1,0.5,1,1,1"]
         # eps on r^T D^-1 r chosen as 1e-20 * f^T D^-1 f ~ 1e-10 relative residual
         t0 = time.perf_counter()
-        subprocess.run([exe, "cg", tmp, f"level={level}", f"f={tmp}/f.f64", "eps=1e-20"] + coef, check=True,
-                       capture_output=True, env=env)
+        try:
+            subprocess.run([exe, "cg", tmp, f"level={level}", f"f={tmp}/f.f64", "eps=1e-20"] + coef, check=True,
+                           capture_output=True, env=env, timeout=300)
+        except subprocess.TimeoutExpired:
+            return {"value": None, "unit": "s", "cores": cores, "kind": "reference",
+                    "sample": f"reference CG on d={d} level {level} did not finish within 300 s on {cores} threads"}
         wall = time.perf_counter() - t0
         meta = dict(l.split()[:2] for l in open(os.path.join(tmp, "meta_cg.txt")) if len(l.split()) >= 2)
     secs = float(meta.get("solve_seconds", wall))
-    return {"value": secs, "unit": "s", "cores": cores, "kind": "reference",
-            "sample": f"reference CG::solveHomogen (Jacobi) on d={d} regular level {level} (N={n}), "
-                      f"{meta.get('iterations')} iterations, rel.res {meta.get('relres')}; full workload infeasible "
-                      "for the reference (fixed hash capacities, O(N^2) grid completion)",
-            "per_dof_us": secs / n * 1e6}
+    # scaled to the workload: same iteration count, cost linear in the points
+    # (a lower bound: the reference's iteration count and per-point cost both
+    # grow with the grid)
+    n_work = workload_points(args.workload)
+    return {"value": secs * n_work / n, "unit": "s", "cores": cores, "kind": "reference",
+            "sample": f"reference CG::solveHomogen (Jacobi) on d={d} regular level {level} (N={n}): {secs:.2f} s, "
+                      f"{meta.get('iterations')} iterations, rel.res {meta.get('relres')}; value = that time x "
+                      f"{n_work}/{n} points (linear scaling, a lower bound); the full workload is infeasible for the "
+                      "reference (fixed hash capacities, O(N^2) grid completion)",
+            "sample_seconds": secs, "sample_points": n, "per_dof_us": secs / n * 1e6}
+
+
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:8.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
+def batch_leg(lsg, torch, dev, stream, count=48, seed=7):
+    """Many uneven grids solved in one batch against the same grids solved one
+    after another: d ~ U{4,5,6}, regular level ~ U{3..6} (129 to 40,193
+    points), a = 1 + 0.9 prod sin(pi m_i x_i) with m_i ~ U{1..3}, f ~ U[-1,1];
+    FP32+IR with Jacobi to relative residual 1e-10."""
+    rng = np.random.default_rng(seed)
+    grids, probs, fs = [], [], []
+    for _ in range(count):
+        d = int(rng.integers(4, 7))
+        level = int(rng.integers(3, 7))
+        g = lsg.AdaptiveSparseGrid.regular(d, level)
+        grids.append(g)
+        probs.append(lsg.MidpointDiffusion(lsg.COEF_SINPROD, [1.0, 0.9] + list(rng.integers(1, 4, d).astype(float))))
+        fs.append(rng.uniform(-1, 1, g.n) * g.active)
+    t0 = time.perf_counter()
+    b = lsg.Batch(grids, probs)
+    setup = time.perf_counter() - t0
+    log(f"batch: {count} grids, {b.size} points, created in {setup:.1f}s")
+    b.autotune(lsg.FP32, reps=2)
+    log("batch: autotuned")
+    f = torch.tensor(b.gather(fs), dtype=torch.float64, device=dev)
+    x = torch.zeros_like(f)
+    o = lsg.SolverOpts(1e-10, 1, 20000, 0, lsg.FP32, 1000, 1e-5, 1)
+    b.solve_device(f.data_ptr(), x.data_ptr(), o, stream)  # warm-up
+    x.zero_()
+    reps, tot = b.solve_device(f.data_ptr(), x.data_ptr(), o, stream)
+    log(f"batch: solved in {tot['seconds']:.3f}s ({tot['iterations']} batched iterations)")
+    # the same grids one at a time
+    seq = 0.0
+    seq_its = []
+    for g, p, fi in zip(grids, probs, fs):
+        m = lsg.MatrixVectorHomogen(g, p)
+        fd = torch.tensor(fi, dtype=torch.float64, device=dev)
+        xd = torch.zeros_like(fd)
+        lsg.CG.solve_device(m, fd.data_ptr(), xd.data_ptr(), o, stream)  # warm-up
+        xd.zero_()
+        r = lsg.CG.solve_device(m, fd.data_ptr(), xd.data_ptr(), o, stream)
+        seq += r["seconds"]
+        seq_its.append(r["iterations"])
+    log(f"batch: one at a time {seq:.3f}s")
+    return {"grids": count, "points": int(b.size), "description": batch_leg.__doc__.split(":", 1)[1].strip(),
+            "seconds": tot["seconds"], "batched_iterations": tot["iterations"],
+            "max_rel_residual": tot["rel_residual"], "all_converged": bool(tot["converged"]),
+            "one_at_a_time_seconds": seq, "speedup": seq / tot["seconds"] if tot["seconds"] > 0 else None,
+            "setup_seconds": setup, "kernel_launches": int(tot["kernel_launches"])}
 
 
 def main():
@@ -144,7 +235,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--workload", default="d6_adaptive_corner")
-    ap.add_argument("--precond", type=int, default=0)
+    ap.add_argument("--precond", type=int, default=2, help="0 Jacobi, 1 none, 2 learned diagonal")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -180,12 +272,37 @@ def main():
     m = lsg.MatrixVectorHomogen(g, prob)
     setup_s = time.perf_counter() - t0
     info = m.info()
+    log(f"operator: {g.n} points in {setup_s:.1f}s")
+    # launch parameters picked by the autotuner (setup, not timed)
+    tune_setting, tune_ms, tune_default_ms = m.autotune(lsg.FP32, reps=3)
+    log(f"autotune: {tune_default_ms:.2f} -> {tune_ms:.2f} ms per FP32 matvec")
+    # preconditioner setup: exact Jacobi diagonal vs the learned diagonal
+    precond = args.precond
+    weights = os.path.join(ROOT, "loadsg_b200", "weights", f"diag_mlp_d{g.d}.npz")
+    learned_ms = jacobi_ms = None
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m.diagonal(prob)
+    torch.cuda.synchronize()
+    jacobi_ms = (time.perf_counter() - t0) * 1e3
+    if precond == 2:
+        if os.path.exists(weights):
+            from loadsg_b200.learned import MLP
+            net = MLP.load(weights)
+            net.install(m)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            net.install(m)
+            torch.cuda.synchronize()
+            learned_ms = (time.perf_counter() - t0) * 1e3
+        else:
+            precond = 0
     dev = torch.device("cuda", local)
     f = torch.tensor(f_host, dtype=torch.float64, device=dev)
     x = torch.zeros(g.n, dtype=torch.float64, device=dev)
 
     def opts(precision, precond):
-        return lsg.SolverOpts(1e-10, 1, 20000, precond, precision, 40, 1e-3, 1)
+        return lsg.SolverOpts(1e-10, 1, 20000, precond, precision, 1000, 1e-5, 1)
 
     stream = torch.cuda.current_stream().cuda_stream
 
@@ -193,8 +310,10 @@ def main():
         x.zero_()
         return lsg.CG.solve_device(m, f.data_ptr(), x.data_ptr(), opts(precision, precond), stream)
 
+    log(f"preconditioner setup: jacobi {jacobi_ms} ms, learned {learned_ms} ms")
     for _ in range(args.warmup):
-        rep = solve(lsg.FP32, args.precond)
+        rep = solve(lsg.FP32, precond)
+        log(f"warm-up solve: {rep['seconds']:.2f}s, {rep['iterations']} iterations")
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -204,7 +323,7 @@ def main():
         torch.cuda.synchronize()
         ev0.record()
         for _ in range(args.steps):
-            reps.append(solve(lsg.FP32, args.precond))
+            reps.append(solve(lsg.FP32, precond))
         ev1.record()
         torch.cuda.synchronize()
     step_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
@@ -213,8 +332,13 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         step_s = float(t.item())
 
-    # plain FP64 CG on the same instance (the comparison the metric names)
+    # plain FP64 CG on the same instance (the comparison the metric names; the
+    # reference's CG is always Jacobi-preconditioned), and FP32+IR with Jacobi
+    log(f"timed: {step_s:.2f}s per solve")
     rep64 = solve(lsg.FP64, 0)
+    log(f"FP64 CG: {rep64['seconds']:.2f}s")
+    rep_jac = solve(lsg.FP32, 0) if precond != 0 else reps[-1]
+    log(f"FP32+IR Jacobi: {rep_jac['seconds']:.2f}s")
     # end to end through the C-ABI with host buffers
     xh = np.zeros(g.n)
     torch.cuda.synchronize()
@@ -222,8 +346,9 @@ def main():
     for _ in range(args.steps):
         xh[:] = 0.0
         lsg.CG.solveHomogen(1e-10, xh, f_host, m, prob, criterion=1, precision=lsg.FP32, max_iter=20000,
-                            precond=args.precond, inner_iter=40, inner_tol=1e-3)
+                            precond=precond, inner_iter=1000, inner_tol=1e-5)
     e2e_s = (time.perf_counter() - te) / args.steps
+    log(f"e2e: {e2e_s:.2f}s per solve")
 
     # matvec bandwidth and the phase-B roofline (CUDA events inside the library)
     x32 = torch.randn(g.n, dtype=torch.float32, device=dev)
@@ -241,6 +366,8 @@ def main():
         hbm, peak_src = 6650.0, "fallback"
     achieved = by32[3] / (ms32[3] * 1e-3) / 1e9
 
+    batch = None if args.no_batch else batch_leg(lsg, torch, dev, stream)
+
     if rank != 0:
         if dist:
             dist.barrier()
@@ -252,13 +379,17 @@ def main():
         "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 matvec / f64 refinement", "data": "synthetic",
         "config": {"workload": args.workload, "description": desc, "n_points": g.n, "n_active": g.getDOFS(),
-                   "tolerance": 1e-10, "precond": ["jacobi", "none", "learned"][args.precond],
+                   "tolerance": 1e-10, "precond": ["jacobi", "none", "learned"][precond],
                    "parallelism": f"replicas x{world}", "l2": "working set larger than L2 (126 MB)"},
         "iterations": reps[-1]["iterations"], "outer_iterations": reps[-1]["outer_iterations"],
         "rel_residual": reps[-1]["rel_residual"],
         "fp64_cg": {"seconds": rep64["seconds"], "iterations": rep64["iterations"],
                     "rel_residual": rep64["rel_residual"]},
         "speedup_vs_fp64_cg": rep64["seconds"] / step_s if step_s > 0 else None,
+        "fp32_ir_jacobi": {"seconds": rep_jac["seconds"], "iterations": rep_jac["iterations"],
+                           "rel_residual": rep_jac["rel_residual"]},
+        "preconditioner_setup_ms": {"jacobi_exact_diag": jacobi_ms, "learned": learned_ms},
+        "tuning": {"setting": tune_setting, "matvec_ms_fp32": tune_ms, "matvec_ms_fp32_default": tune_default_ms},
         "matvec": {"fp32_ms": ms32[4], "fp64_ms": ms64[4], "fp32_gbs": by32[4] / (ms32[4] * 1e-3) / 1e9,
                    "fp64_gbs": by64[4] / (ms64[4] * 1e-3) / 1e9, "phase_ms_fp32": list(ms32[:4]),
                    "cell_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9},
@@ -270,6 +401,8 @@ def main():
         "clocks": clk.summary(),
         "gpu_launches": int(sum(r["kernel_launches"] for r in reps)),
     }
+    if batch is not None:
+        line["batch"] = batch
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line))

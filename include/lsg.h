@@ -170,6 +170,26 @@ int lsg_operator_base_diag(lsg_operator *op, double *base, void *stream);
 /* D = base * softplus(mlp(features)) at active points, installed for precond = 2 */
 int lsg_operator_install_learned(lsg_operator *op, lsg_mlp *m, void *stream);
 
+/* ---- launch parameters of the matvec and the autotuner that picks them.
+ * The defaults suit large d=5/6 grids; lsg_operator_autotune times matvecs of
+ * this operator over a candidate set per parameter (coordinate descent, two
+ * passes, best of `reps` timings per setting) and keeps the fastest setting.
+ * No counterpart in the reference (OpenMP schedule only). */
+typedef struct {
+    int32_t cell_threads;    /* threads per cell-operator CTA: 64..256, multiple of 32 */
+    int32_t cell_segment;    /* dim-0 cells per work unit on complete slabs: 1..64 */
+    int32_t class_ratio;     /* slab-size ratio that starts a new cell-operator launch: 2..1024 */
+    int32_t level_threads;   /* threads per restriction-wavefront CTA: 32..128, multiple of 32 */
+    int32_t level_cap;       /* shared-memory elements per wavefront ping-pong buffer: 256..65536 */
+    int32_t prolong_threads; /* threads per prolongation CTA: 32..1024, multiple of 32 */
+} lsg_tuning;
+int lsg_operator_get_tuning(const lsg_operator *op, lsg_tuning *t);
+int lsg_operator_set_tuning(lsg_operator *op, const lsg_tuning *t);
+/* best (may be NULL): the setting kept; best_ms / default_ms (may be NULL):
+ * ms per matvec with it and with the setting the operator had on entry */
+int lsg_operator_autotune(lsg_operator *op, int32_t precision, int32_t reps, lsg_tuning *best, double *best_ms,
+                          double *default_ms);
+
 /* ---- batched operators and solves: many grids of uneven size (any mix of
  * dimensions), each with its own coefficient and right-hand side, applied and
  * solved together.  Grids of one dimension are concatenated into one
@@ -197,6 +217,8 @@ int lsg_batch_cg_solve_device(lsg_batch *b, const double *f, double *x, const ls
                               lsg_solve_report *reports, lsg_solve_report *total, void *stream);
 int lsg_batch_cg_solve(lsg_batch *b, const double *f, double *x, const lsg_solver_opts *opts,
                        lsg_solve_report *reports, lsg_solve_report *total);
+/* autotunes the operator of every dimension group of the batch */
+int lsg_batch_autotune(lsg_batch *b, int32_t precision, int32_t reps);
 
 /* ---- host-only planner (no GPU needed): the flattened integer tables.
  * lsg_plan_create builds the same tables lsg_operator_create uploads, so the

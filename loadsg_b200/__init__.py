@@ -75,6 +75,21 @@ class SolveReport(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    """Launch parameters of the matvec (lsg_tuning in include/lsg.h)."""
+    _fields_ = [
+        ("cell_threads", ctypes.c_int32),
+        ("cell_segment", ctypes.c_int32),
+        ("class_ratio", ctypes.c_int32),
+        ("level_threads", ctypes.c_int32),
+        ("level_cap", ctypes.c_int32),
+        ("prolong_threads", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def lib():
     """Loads liblsg.so (built in-tree by `python -m loadsg_b200.build`)."""
     global _LIB
@@ -109,6 +124,10 @@ def lib():
             "lsg_plan_export_stencil": (ctypes.c_int, [P, I64, P, P, P]),
             "lsg_grid_regular": (ctypes.c_int, [I32, I32, P, I64, P]),
             "lsg_grid_adaptive": (ctypes.c_int, [I32, I32, I32, D, I32, I32, P, P, I64, P]),
+            "lsg_operator_get_tuning": (ctypes.c_int, [P, P]),
+            "lsg_operator_set_tuning": (ctypes.c_int, [P, P]),
+            "lsg_operator_autotune": (ctypes.c_int, [P, I32, I32, P, P, P]),
+            "lsg_batch_autotune": (ctypes.c_int, [P, I32, I32]),
             "lsg_batch_create": (ctypes.c_int, [I32, P, P, P, P, P]),
             "lsg_batch_destroy": (None, [P]),
             "lsg_batch_size": (I64, [P]),
@@ -310,6 +329,27 @@ class MatrixVectorHomogen:
         _check(lib().lsg_matvec_device(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), precision,
                                        ctypes.c_void_p(stream)))
 
+    def tuning(self):
+        t = Tuning()
+        _check(lib().lsg_operator_get_tuning(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = Tuning()
+        _check(lib().lsg_operator_get_tuning(self._h, ctypes.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        _check(lib().lsg_operator_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self, precision=FP32, reps=3, cache=None):
+        """Picks the matvec launch parameters by timing (lsg_operator_autotune).
+        With cache (a JSON path, or True for $LSG_TUNING_CACHE or
+        ~/.cache/loadsg_b200/tuning.json) settings are reused for operators of
+        the same dimension, size class and precision.  Returns (setting,
+        best ms, ms with the previous setting); ms are None on a cache hit."""
+        from . import tuning as _tuning
+        return _tuning.autotune(self, precision, reps, cache)
+
     def profile(self, x_ptr, y_ptr, precision=FP32, iters=5):
         """Mean ms per matvec phase (nodal, P init, prolongation, restriction
         wavefronts with the cell operator, total) plus algorithmic bytes per
@@ -392,6 +432,9 @@ class Batch:
         if getattr(self, "_h", None):
             self._destroy(self._h)
             self._h = None
+
+    def autotune(self, precision=FP32, reps=3):
+        _check(lib().lsg_batch_autotune(self._h, precision, reps))
 
     def set_problem(self, i, problem):
         _check(lib().lsg_batch_set_coefficient(self._h, i, problem.family, _ptr(problem.params), problem.nparams))

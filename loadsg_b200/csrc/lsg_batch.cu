@@ -522,7 +522,8 @@ int batch_solve(lsg_batch* b, const double* f, double* x, const lsg_solver_opts*
             kb_to_f32<<<nb(n), kThreads, 0, st>>>(n, z, S.z32.as<float>());
             z32 = S.z32.as<float>();
         }
-        for (int outer = 0; outer < maxit; ++outer) {
+        // bounded like the single-grid refinement: at most 4 max_iter inner iterations
+        for (int outer = 0; outer < maxit && rounds < 4 * maxit; ++outer) {
             BT_TRY(cudaMemsetAsync(r, 0, n * 8, st));
             rc = batch_matvec<double>(b, x, r, st);
             if (rc) break;
@@ -702,6 +703,15 @@ int lsg_batch_matvec_device(lsg_batch* b, const void* x, void* y, int32_t precis
     if (precision == LSG_FP64) return batch_matvec<double>(b, (const double*)x, (double*)y, st);
     if (precision == LSG_FP32) return batch_matvec<float>(b, (const float*)x, (float*)y, st);
     return fail_msg(LSG_E_INVALID, "precision must be LSG_FP64 or LSG_FP32");
+}
+
+int lsg_batch_autotune(lsg_batch* b, int32_t precision, int32_t reps) {
+    if (!b) return fail_msg(LSG_E_INVALID, "null batch");
+    for (auto& g : b->groups) {
+        int rc = lsg_internal::autotune(g.op, precision, reps);
+        if (rc) return rc;
+    }
+    return 0;
 }
 
 int lsg_batch_cg_solve_device(lsg_batch* b, const double* f, double* x, const lsg_solver_opts* opts,

@@ -232,12 +232,13 @@ __device__ __forceinline__ void wht_face(V* v, int g) {
 // and the other dims short.  All lanes of a warp run the same number of
 // rounds and iterations (the group shuffles need them).
 template <int D, typename V>
-__device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, const V* __restrict__ ac, const V* lamg) {
+__device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, const V* __restrict__ ac, const V* lamg,
+                            int32_t segmax) {
     constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NH = CellCfg<D>::NH;
     const int g = threadIdx.x & (G - 1);
     const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
     const int32_t c0 = s.ext[0] + 1;  // cells along dim 0
-    const int32_t seg = c0 < 8 ? c0 : 8;
+    const int32_t seg = c0 < segmax ? c0 : segmax;
     const int32_t nseg = (c0 + seg - 1) / seg;
     const int64_t ncols = s.ncell / c0;
     const int64_t units = ncols * nseg;
@@ -352,7 +353,8 @@ __device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __rest
 template <int D, typename V>
 __global__ void __launch_bounds__(256, 2) k_cells(DevPlan P, const V* __restrict__ pc, V* __restrict__ zb,
                                                   const V* __restrict__ acell, const V* __restrict__ lam_all,
-                                                  const int32_t* __restrict__ order, int32_t ord0, int64_t cap) {
+                                                  const int32_t* __restrict__ order, int32_t ord0, int64_t cap,
+                                                  int32_t segmax) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NC = 1 << D;
     const lsg::PhaseBItem it = P.b_items[order[ord0 + blockIdx.x]];
@@ -371,14 +373,14 @@ __global__ void __launch_bounds__(256, 2) k_cells(DevPlan P, const V* __restrict
             z[e] = V(0);
         }
         __syncthreads();
-        if (s.dense) cells_dense<D, V>(s, u, z, ac, lamg);
+        if (s.dense) cells_dense<D, V>(s, u, z, ac, lamg, segmax);
         else cells_sparse<D, V>(P, s, u, z, ac, lamg);
         __syncthreads();
         for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) z_g[e] = z[e];
     } else {
         for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) z_g[e] = V(0);
         __syncthreads();
-        if (s.dense) cells_dense<D, V>(s, u_g, z_g, ac, lamg);
+        if (s.dense) cells_dense<D, V>(s, u_g, z_g, ac, lamg, segmax);
         else cells_sparse<D, V>(P, s, u_g, z_g, ac, lamg);
     }
 }
@@ -811,12 +813,42 @@ struct lsg_operator {
     bool have_learned = false;
     int64_t smem_cap64 = 0, smem_cap32 = 0;
     std::vector<int64_t> level_need;  // per phase-B level: largest vector of any item
+    lsg_tuning tune{256, 8, 4, 128, 12288, 256};  // launch parameters (lsg_operator_autotune)
     DBuf cell_order;                  // phase-B items ordered by slab size (k_cells)
     std::vector<int32_t> cell_class_off;  // size classes in cell_order
     std::vector<int64_t> cell_class_n;    // largest N_T per class
 };
 
 namespace {
+
+// k_cells items by slab size, largest first, in size classes: a new class
+// (launch) starts when slabs shrink by tune.class_ratio; shared memory per
+// launch = 2 N_T of the class's largest slab
+int build_cell_classes(lsg_operator* op) {
+    const lsg::Plan& p = op->plan;
+    std::vector<int32_t> ord(p.b_items.size());
+    for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int32_t)i;
+    std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) {
+        return p.slabs[p.b_items[a].t].n > p.slabs[p.b_items[b].t].n;
+    });
+    op->cell_class_off.clear();
+    op->cell_class_n.clear();
+    int64_t bound = -1;
+    for (size_t i = 0; i < ord.size(); ++i) {
+        int64_t n = p.slabs[p.b_items[ord[i]].t].n;
+        if (bound < 0 || n * op->tune.class_ratio < bound) {
+            op->cell_class_off.push_back((int32_t)i);
+            op->cell_class_n.push_back(n);
+            bound = n;
+        }
+    }
+    op->cell_class_off.push_back((int32_t)ord.size());
+    if (op->cell_order.p && op->cell_order.bytes == ord.size() * sizeof(int32_t)) {
+        CUDA_TRY(cudaMemcpy(op->cell_order.p, ord.data(), ord.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        return 0;
+    }
+    return op->cell_order.upload(ord, &op->dev_bytes) ? LSG_E_CUDA : 0;
+}
 
 int upload_plan(lsg_operator* op) {
     const lsg::Plan& p = op->plan;
@@ -938,29 +970,7 @@ int upload_plan(lsg_operator* op) {
         }
         op->level_need.push_back(mx);
     }
-    // k_cells items by slab size, largest first, in size classes (shared memory
-    // per launch = 2 N_T of the class's largest slab)
-    {
-        std::vector<int32_t> ord(p.b_items.size());
-        for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int32_t)i;
-        std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) {
-            return p.slabs[p.b_items[a].t].n > p.slabs[p.b_items[b].t].n;
-        });
-        op->cell_class_off.clear();
-        op->cell_class_n.clear();
-        int64_t bound = -1;
-        for (size_t i = 0; i < ord.size(); ++i) {
-            int64_t n = p.slabs[p.b_items[ord[i]].t].n;
-            if (bound < 0 || n * 4 < bound) {  // new class when slabs shrink 4x
-                op->cell_class_off.push_back((int32_t)i);
-                op->cell_class_n.push_back(n);
-                bound = n;
-            }
-        }
-        op->cell_class_off.push_back((int32_t)ord.size());
-        if (op->cell_order.upload(ord, tot)) return LSG_E_CUDA;
-    }
-    return 0;
+    return build_cell_classes(op);
 }
 
 template <typename V>
@@ -999,14 +1009,17 @@ int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* y,
         int64_t need = 2 * op->cell_class_n[c];
         int64_t alloc = need <= cap_elems ? need : 0;
         size_t smem = (size_t)((1 << D) + alloc) * sizeof(V);
-        k_cells<D, V><<<e - b, 256, smem, st>>>(op->dp, pc, zb, acell, lam, op->cell_order.as<int32_t>(), b, alloc);
+        k_cells<D, V><<<e - b, op->tune.cell_threads, smem, st>>>(op->dp, pc, zb, acell, lam,
+                                                                  op->cell_order.as<int32_t>(), b, alloc,
+                                                                  op->tune.cell_segment);
     }
-    const int64_t lvl_cap = 12288;  // elements per ping-pong buffer
+    // elements per ping-pong buffer (two buffers within the 220 KB opt-in)
+    const int64_t lvl_cap = std::min<int64_t>(op->tune.level_cap, (110 * 1024) / sizeof(V));
     for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
         int32_t b = p.b_level_off[L], e = p.b_level_off[L + 1];
         if (e <= b) continue;
         int64_t bufn = std::min<int64_t>(op->level_need[L], lvl_cap);
-        k_level<D, V><<<e - b, 128, 2 * bufn * sizeof(V), st>>>(op->dp, zb, gm, scratch, y, b, bufn);
+        k_level<D, V><<<e - b, op->tune.level_threads, 2 * bufn * sizeof(V), st>>>(op->dp, zb, gm, scratch, y, b, bufn);
     }
     CUDA_TRY(cudaGetLastError());
     return 0;
@@ -1033,7 +1046,7 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t
     if (ev) cudaEventRecord(ev[2], st);
     for (size_t L = 0; L + 1 < p.a_level_off.size(); ++L) {
         int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
-        if (e > b) k_prolong<V><<<e - b, 256, 0, st>>>(op->dp, w.pc.as<V>(), b);
+        if (e > b) k_prolong<V><<<e - b, op->tune.prolong_threads, 0, st>>>(op->dp, w.pc.as<V>(), b);
     }
     if (ev) cudaEventRecord(ev[3], st);
     rc = phaseB_launch<D, V>(op, w.pc.as<V>(), w.zb.as<V>(), w.gm.as<V>(), w.scratch.as<V>(), y, acell, lam, st);
@@ -1184,6 +1197,9 @@ int64_t matvec_launch_count(const lsg_operator* op) {
            (int64_t)(p.b_level_off.size() - 1);
 }
 int fail_msg(int code, const char* msg) { return fail(code, msg); }
+int autotune(lsg_operator* op, int32_t precision, int32_t reps) {
+    return lsg_operator_autotune(op, precision, reps, nullptr, nullptr, nullptr);
+}
 
 }  // namespace lsg_internal
 
@@ -1889,6 +1905,111 @@ static int lsg_internal_matvec32(lsg_operator* op, const float* x, float* y, cud
 }
 static const uint8_t* lsg_internal_active(lsg_operator* op) { return op->act.as<uint8_t>(); }
 
+// ============================================================================= launch parameters, autotuner
+namespace {
+
+__global__ void k_pattern(int64_t n, double* x64, float* x32) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = (double)((i * 2654435761ull) % 1000003ull) / 1000003.0 - 0.5;
+    if (x64) x64[i] = v;
+    if (x32) x32[i] = (float)v;
+}
+
+bool tuning_valid(const lsg_tuning& t) {
+    auto warps = [](int v, int lo, int hi) { return v >= lo && v <= hi && v % 32 == 0; };
+    return warps(t.cell_threads, 64, 256) && t.cell_segment >= 1 && t.cell_segment <= 64 && t.class_ratio >= 2 &&
+           t.class_ratio <= 1024 && warps(t.level_threads, 32, 128) && t.level_cap >= 256 && t.level_cap <= 65536 &&
+           warps(t.prolong_threads, 32, 1024);
+}
+
+}  // namespace
+
+extern "C" int lsg_operator_get_tuning(const lsg_operator* op, lsg_tuning* t) {
+    if (!op || !t) return fail(LSG_E_INVALID, "null argument");
+    *t = op->tune;
+    return 0;
+}
+
+extern "C" int lsg_operator_set_tuning(lsg_operator* op, const lsg_tuning* t) {
+    if (!op || !t) return fail(LSG_E_INVALID, "null argument");
+    if (!tuning_valid(*t)) return fail(LSG_E_INVALID, "launch parameters out of range");
+    op->tune = *t;
+    return build_cell_classes(op);
+}
+
+extern "C" int lsg_operator_autotune(lsg_operator* op, int32_t precision, int32_t reps, lsg_tuning* best,
+                                     double* best_ms, double* default_ms) {
+    if (!op) return fail(LSG_E_INVALID, "null operator");
+    if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
+    if (precision != LSG_FP64 && precision != LSG_FP32) return fail(LSG_E_INVALID, "bad precision");
+    if (reps < 1) reps = 3;
+    const bool f32 = precision == LSG_FP32;
+    int rc = f32 ? prepare<float>(op) : prepare<double>(op);
+    if (rc) return rc;
+    int64_t n = op->plan.n;
+    DBuf x, y;
+    size_t dummy = 0, vs = f32 ? 4 : 8;
+    if (x.alloc(n * vs, &dummy) || y.alloc(n * vs, &dummy)) return LSG_E_CUDA;
+    k_pattern<<<nblk(n), 256>>>(n, f32 ? nullptr : x.as<double>(), f32 ? x.as<float>() : nullptr);
+    CUDA_TRY(cudaMemset(y.p, 0, n * vs));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int err = 0;
+    auto run = [&]() {
+        return f32 ? matvec_dispatch<float>(op, x.as<float>(), y.as<float>(), 0)
+                   : matvec_dispatch<double>(op, x.as<double>(), y.as<double>(), 0);
+    };
+    auto time_cfg = [&](const lsg_tuning& t) -> double {
+        op->tune = t;
+        if (build_cell_classes(op) || run()) { err = 1; return 1e30; }
+        double bestt = 1e30;
+        for (int r = 0; r < reps; ++r) {
+            cudaEventRecord(e0, 0);
+            if (run()) { err = 1; return 1e30; }
+            cudaEventRecord(e1, 0);
+            if (cudaEventSynchronize(e1) != cudaSuccess) { err = 1; return 1e30; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            bestt = std::min(bestt, (double)ms);
+        }
+        return bestt;
+    };
+    const lsg_tuning start = op->tune;
+    lsg_tuning cur = start;
+    double cur_ms = time_cfg(cur), def_ms = cur_ms;
+    const std::vector<std::pair<int32_t lsg_tuning::*, std::vector<int32_t>>> space = {
+        {&lsg_tuning::cell_segment, {4, 8, 16}},      {&lsg_tuning::cell_threads, {128, 256}},
+        {&lsg_tuning::class_ratio, {2, 4, 16}},       {&lsg_tuning::level_threads, {64, 128}},
+        {&lsg_tuning::level_cap, {4096, 8192, 12288}}, {&lsg_tuning::prolong_threads, {128, 256, 512}}};
+    for (int pass = 0; pass < 2 && !err; ++pass) {
+        bool moved = false;
+        for (const auto& dim : space) {
+            for (int32_t v : dim.second) {
+                if (cur.*(dim.first) == v) continue;
+                lsg_tuning t = cur;
+                t.*(dim.first) = v;
+                double ms = time_cfg(t);
+                if (err) break;
+                if (ms < 0.99 * cur_ms) { cur = t; cur_ms = ms; moved = true; }
+            }
+            if (err) break;
+        }
+        if (!moved) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    op->tune = err ? start : cur;
+    rc = build_cell_classes(op);
+    if (err) return fail(LSG_E_CUDA, std::string("autotune: ") + (g_err.empty() ? "launch failed" : g_err));
+    if (rc) return rc;
+    if (best) *best = cur;
+    if (best_ms) *best_ms = cur_ms;
+    if (default_ms) *default_ms = def_ms;
+    return 0;
+}
+
 // ============================================================================= allocation-free matvec
 // Some callers cannot allocate device memory when they need a product: code
 // running while a CUDA graph is being captured (cudaMalloc is not permitted
@@ -1960,7 +2081,7 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
     if (nb > 0) k_pinit<V><<<nb, 256, 0, st>>>(op->dp, ml, pc, 0);
     for (size_t L = 0; L + 1 < p.a_level_off.size(); ++L) {
         int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
-        if (e > b) k_prolong<V><<<e - b, 256, 0, st>>>(op->dp, pc, b);
+        if (e > b) k_prolong<V><<<e - b, op->tune.prolong_threads, 0, st>>>(op->dp, pc, b);
     }
     rc = phaseB_launch<D, V>(op, pc, zb, gm, scratch, y, acell, lam, st);
     if (rc) return rc;

@@ -27,5 +27,6 @@ const lsg::Plan& plan(const lsg_operator* op);
 size_t device_bytes(const lsg_operator* op);
 int64_t matvec_launch_count(const lsg_operator* op);
 int fail_msg(int code, const char* msg);
+int autotune(lsg_operator* op, int32_t precision, int32_t reps);
 
 }  // namespace lsg_internal
