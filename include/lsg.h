@@ -170,6 +170,17 @@ int lsg_operator_base_diag(lsg_operator *op, double *base, void *stream);
 /* D = base * softplus(mlp(features)) at active points, installed for precond = 2 */
 int lsg_operator_install_learned(lsg_operator *op, lsg_mlp *m, void *stream);
 
+/* ---- prewavelet basis transforms (BasisTransformations/BasisTransformations.cpp).
+ * lsg_calc_nodal_by_prew: u = values at every grid point (hanging included) of
+ * the expansion sum_i prew_i psi_i over all points (calcNodalByPrew, :670-706).
+ * lsg_calc_prew_by_nodal: prew = its inverse from the values of u at the active
+ * points, 0 at hanging points (calcPrewByNodal, :486-545); u is not modified.
+ * Vectors of n doubles in storage order; the tables are built on first use. */
+int lsg_calc_nodal_by_prew(lsg_operator *op, const double *prew, double *u);
+int lsg_calc_prew_by_nodal(lsg_operator *op, double *prew, const double *u);
+int lsg_calc_nodal_by_prew_device(lsg_operator *op, const double *prew, double *u, void *stream);
+int lsg_calc_prew_by_nodal_device(lsg_operator *op, double *prew, const double *u, void *stream);
+
 /* ---- launch parameters of the matvec and the autotuner that picks them.
  * The defaults suit large d=5/6 grids; lsg_operator_autotune times matvecs of
  * this operator over a candidate set per parameter (coordinate descent, two

@@ -124,6 +124,10 @@ def lib():
             "lsg_plan_export_stencil": (ctypes.c_int, [P, I64, P, P, P]),
             "lsg_grid_regular": (ctypes.c_int, [I32, I32, P, I64, P]),
             "lsg_grid_adaptive": (ctypes.c_int, [I32, I32, I32, D, I32, I32, P, P, I64, P]),
+            "lsg_calc_nodal_by_prew": (ctypes.c_int, [P, P, P]),
+            "lsg_calc_prew_by_nodal": (ctypes.c_int, [P, P, P]),
+            "lsg_calc_nodal_by_prew_device": (ctypes.c_int, [P, P, P, P]),
+            "lsg_calc_prew_by_nodal_device": (ctypes.c_int, [P, P, P, P]),
             "lsg_operator_get_tuning": (ctypes.c_int, [P, P]),
             "lsg_operator_set_tuning": (ctypes.c_int, [P, P]),
             "lsg_operator_autotune": (ctypes.c_int, [P, I32, I32, P, P, P]),
@@ -396,6 +400,38 @@ class CG:
         _check(lib().lsg_cg_solve_device(matrix._h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(x_ptr),
                                          ctypes.byref(opts), ctypes.byref(rep), ctypes.c_void_p(stream)))
         return {k: getattr(rep, k) for k, _ in SolveReport._fields_}
+
+
+# --------------------------------------------------------------------------- basis transforms
+def calcNodalByPrew(prew, u, matrix):
+    """calcNodalByPrew(prew, u) (BasisTransformations/BasisTransformations.cpp:670-706):
+    u = values at every grid point of the prewavelet expansion prew (0 at
+    hanging points).  Host float64 arrays of length N; the grid comes from the
+    MatrixVectorHomogen (no coefficient needed)."""
+    prew = np.ascontiguousarray(prew, np.float64)
+    if u.dtype != np.float64 or not u.flags.c_contiguous:
+        raise ValueError("u must be a contiguous float64 array")
+    _check(lib().lsg_calc_nodal_by_prew(matrix._h, _ptr(prew), _ptr(u)))
+
+
+def calcPrewByNodal(prew, u, matrix):
+    """calcPrewByNodal(prew, u) (BasisTransformations.cpp:486-545): prew = the
+    prewavelet coefficients whose expansion takes the values u at the active
+    points (0 at hanging points); u is not modified."""
+    u = np.ascontiguousarray(u, np.float64)
+    if prew.dtype != np.float64 or not prew.flags.c_contiguous:
+        raise ValueError("prew must be a contiguous float64 array")
+    _check(lib().lsg_calc_prew_by_nodal(matrix._h, _ptr(prew), _ptr(u)))
+
+
+def calcNodalByPrew_device(prew_ptr, u_ptr, matrix, stream=0):
+    _check(lib().lsg_calc_nodal_by_prew_device(matrix._h, ctypes.c_void_p(prew_ptr), ctypes.c_void_p(u_ptr),
+                                               ctypes.c_void_p(stream)))
+
+
+def calcPrewByNodal_device(prew_ptr, u_ptr, matrix, stream=0):
+    _check(lib().lsg_calc_prew_by_nodal_device(matrix._h, ctypes.c_void_p(prew_ptr), ctypes.c_void_p(u_ptr),
+                                               ctypes.c_void_p(stream)))
 
 
 # --------------------------------------------------------------------------- batches

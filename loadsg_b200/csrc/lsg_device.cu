@@ -814,6 +814,7 @@ struct lsg_operator {
     int64_t smem_cap64 = 0, smem_cap32 = 0;
     std::vector<int64_t> level_need;  // per phase-B level: largest vector of any item
     lsg_tuning tune{256, 8, 4, 128, 12288, 256};  // launch parameters (lsg_operator_autotune)
+    std::shared_ptr<void> basis;      // basis-transform tables (lsg_basis.cu), built on first use
     DBuf cell_order;                  // phase-B items ordered by slab size (k_cells)
     std::vector<int32_t> cell_class_off;  // size classes in cell_order
     std::vector<int64_t> cell_class_n;    // largest N_T per class
@@ -1197,6 +1198,7 @@ int64_t matvec_launch_count(const lsg_operator* op) {
            (int64_t)(p.b_level_off.size() - 1);
 }
 int fail_msg(int code, const char* msg) { return fail(code, msg); }
+std::shared_ptr<void>& basis_slot(lsg_operator* op) { return op->basis; }
 int autotune(lsg_operator* op, int32_t precision, int32_t reps) {
     return lsg_operator_autotune(op, precision, reps, nullptr, nullptr, nullptr);
 }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 
 #include "lsg_plan.h"
 
@@ -28,5 +29,7 @@ size_t device_bytes(const lsg_operator* op);
 int64_t matvec_launch_count(const lsg_operator* op);
 int fail_msg(int code, const char* msg);
 int autotune(lsg_operator* op, int32_t precision, int32_t reps);
+// per-operator state of the basis transforms (lsg_basis.cu)
+std::shared_ptr<void>& basis_slot(lsg_operator* op);
 
 }  // namespace lsg_internal

@@ -895,4 +895,309 @@ bool concat_plans(const std::vector<const Plan*>& parts, Plan& q) {
     return true;
 }
 
+
+// ============================================================================= basis transforms
+namespace {
+
+inline int ctz64(int64_t v) { return __builtin_ctzll((unsigned long long)v); }
+
+// LR decomposition without pivoting of a band matrix of half-bandwidth 2
+// (sgoperation/matrix_operations.cc:34-60), same operation order; m holds the
+// bands m[5k+0..4] = M[k][k-2..k+2] on entry.
+void band_lr(int n, std::vector<double>& R, std::vector<double>& L) {
+    auto at = [n](int i, int j) { return (size_t)i * 5 + (size_t)(j - i + 2); };
+    L.assign((size_t)n * 5, 0.0);
+    for (int i = 0; i < n; ++i) L[at(i, i)] = 1.0;
+    for (int k = 0; k < n - 1; ++k)
+        for (int i = k + 1; i < std::min(k + 3, n); ++i) {
+            L[at(i, k)] = R[at(i, k)] / R[at(k, k)];
+            for (int j = k; j < std::min(k + 3, n); ++j) R[at(i, j)] = R[at(i, j)] - L[at(i, k)] * R[at(k, j)];
+        }
+}
+
+}  // namespace
+
+bool build_basis_plan(const Plan& p, BasisPlan& b, std::string& error) {
+    auto t0 = std::chrono::steady_clock::now();
+    const int d = p.d, nD = p.nD;
+    if (p.M >= ((int64_t)1 << 31) || p.n >= ((int64_t)1 << 29)) { error = "grid too large for the basis transforms"; return false; }
+    b = BasisPlan();
+    // ---- subgrid order: |T|_1 ascending, first appearance within equal norms
+    b.order.resize(nD);
+    for (int t = 0; t < nD; ++t) b.order[t] = t;
+    auto l1 = [&](int t) { int s = 0; for (int j = 0; j < d; ++j) s += p.D[t * d + j]; return s; };
+    std::stable_sort(b.order.begin(), b.order.end(), [&](int a, int c) { return l1(a) < l1(c); });
+    // ---- nodal transform over all points of each depth
+    b.ex_sorted.resize(p.ex.size());
+    std::vector<StageOut> nod(nD);
+#pragma omp parallel for schedule(dynamic)
+    for (int t = 0; t < nD; ++t) {
+        const Slab& sl = p.slabs[t];
+        Geometry g(d, sl.T);
+        std::vector<std::pair<uint64_t, int64_t>> kv;
+        for (int64_t e = p.ex_off[t]; e < p.ex_off[t + 1]; ++e) {
+            int64_t k = p.ex[e];
+            int64_t c[kMaxDim];
+            for (int j = 0; j < d; ++j) c[j] = coord_at(p.pts[k * d + j], sl.T[j]);
+            kv.emplace_back(g.key(c), k);
+        }
+        std::sort(kv.begin(), kv.end());
+        std::vector<uint64_t> keys(kv.size());
+        for (size_t e = 0; e < kv.size(); ++e) { keys[e] = kv[e].first; b.ex_sorted[p.ex_off[t] + e] = kv[e].second; }
+        std::vector<uint64_t> slab_keys(p.slab_key.begin() + sl.off, p.slab_key.begin() + sl.off + sl.n);
+        build_transform(g, keys, slab_keys, true, 3, nod[t]);
+    }
+    b.nodal.nsrc = 3;
+    b.nodal_dom.assign((size_t)nD * (d + 1), 0);
+    b.nodal.stage_off.assign((size_t)nD * d + 1, 0);
+    {
+        int64_t tot = 0;
+        for (int t = 0; t < nD; ++t) {
+            for (int j = 0; j <= d; ++j) b.nodal_dom[t * (d + 1) + j] = (int64_t)nod[t].dom[j].size();
+            for (int j = 0; j < d; ++j) { b.nodal.stage_off[t * d + j] = tot; tot += (int64_t)nod[t].code[j].size(); }
+        }
+        b.nodal.stage_off[nD * d] = tot;
+        b.nodal.src.resize(tot * 3);
+        b.nodal.code.resize(tot);
+        for (int t = 0; t < nD; ++t)
+            for (int j = 0; j < d; ++j) {
+                int64_t o = b.nodal.stage_off[t * d + j];
+                std::copy(nod[t].src[j].begin(), nod[t].src[j].end(), b.nodal.src.begin() + o * 3);
+                std::copy(nod[t].code[j].begin(), nod[t].code[j].end(), b.nodal.code.begin() + o);
+            }
+    }
+    nod.clear();
+    // ---- slab hierarchization neighbours
+    b.slab_nb.assign((size_t)p.M * d * 2, -1);
+    b.slab_dep.assign((size_t)p.M * d, 0);
+#pragma omp parallel for schedule(dynamic)
+    for (int t = 0; t < nD; ++t) {
+        const Slab& sl = p.slabs[t];
+        Geometry g(d, sl.T);
+        int64_t c[kMaxDim];
+        for (int64_t e = 0; e < sl.n; ++e) {
+            g.decode(p.slab_key[sl.off + e], c);
+            for (int j = 0; j < d; ++j) {
+                int own = sl.T[j] - ctz64(c[j]);
+                b.slab_dep[(size_t)(sl.off + e) * d + j] = (uint8_t)own;
+                int64_t step = (int64_t)1 << (sl.T[j] - own), cj = c[j];
+                int32_t* nb = &b.slab_nb[((size_t)(sl.off + e) * d + j) * 2];
+                if (cj - step > 0) {
+                    c[j] = cj - step;
+                    int64_t at = slab_pos(p, t, g, c);
+                    nb[0] = at < 0 ? -1 : (int32_t)(sl.off + at);
+                }
+                if (cj + step < g.cext[j]) {
+                    c[j] = cj + step;
+                    int64_t at = slab_pos(p, t, g, c);
+                    nb[1] = at < 0 ? -1 : (int32_t)(sl.off + at);
+                }
+                c[j] = cj;
+            }
+        }
+    }
+    // ---- point neighbours and per-(dim, depth) point lists
+    b.pt_nb.assign((size_t)p.n * d * 2, -1);
+    for (int j = 0; j < d; ++j) b.maxdep = std::max(b.maxdep, p.maxdep[j]);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < p.n; ++k) {
+        int t = p.did[k];
+        const Slab& sl = p.slabs[t];
+        Geometry g(d, sl.T);
+        int64_t c[kMaxDim];
+        for (int j = 0; j < d; ++j) c[j] = coord_at(p.pts[k * d + j], sl.T[j]);  // odd: own level
+        for (int j = 0; j < d; ++j) {
+            int64_t cj = c[j];
+            for (int side = 0; side < 2; ++side) {
+                int64_t q = side ? cj + 1 : cj - 1;
+                if (q <= 0 || q >= g.cext[j]) continue;
+                c[j] = q;
+                int64_t at = slab_pos(p, t, g, c);
+                if (at >= 0) b.pt_nb[((size_t)k * d + j) * 2 + side] = (int32_t)p.slab_pt[sl.off + at];
+            }
+            c[j] = cj;
+        }
+    }
+    {
+        int nl = d * (b.maxdep + 1);
+        b.lvl_off.assign(nl + 1, 0);
+        // active points only: vector assignments of the reference touch active entries
+        for (int64_t k = 0; k < p.n; ++k)
+            if (p.act[k])
+                for (int j = 0; j < d; ++j) b.lvl_off[j * (b.maxdep + 1) + p.D[p.did[k] * d + j] + 1]++;
+        for (int i = 0; i < nl; ++i) b.lvl_off[i + 1] += b.lvl_off[i];
+        b.lvl_pts.resize(b.lvl_off[nl]);
+        std::vector<int64_t> fill(b.lvl_off.begin(), b.lvl_off.end() - 1);
+        for (int64_t k = 0; k < p.n; ++k)
+            if (p.act[k])
+                for (int j = 0; j < d; ++j) b.lvl_pts[fill[j * (b.maxdep + 1) + p.D[p.did[k] * d + j]]++] = (int32_t)k;
+    }
+    // ---- calcPrewByNodal: components, bounding boxes and poles per depth, in
+    // the reference's processing order (subgrids from the finest backwards,
+    // BasisTransformations.cpp:486-545; SolvePrewavelet :468-484; components
+    // sgrid/komponente.cpp; GetPrewaveletCoefficients :100-172; the pole matrix
+    // sgoperation/matrix.cpp:76-150)
+    std::vector<int32_t> mark(p.n, -1);
+    for (int oi = nD - 1; oi >= 0; --oi) {
+        const int t = b.order[oi];
+        const Slab& sl = p.slabs[t];
+        const int32_t* T = sl.T;
+        Geometry g(d, T);
+        b.step_t.push_back(t);
+        b.step_group.push_back((int32_t)b.groups.size());
+        auto lookup = [&](const int64_t* c) -> int64_t {  // storage index of level-T coords, -1 if none
+            for (int j = 0; j < d; ++j)
+                if (c[j] <= 0 || c[j] >= g.cext[j]) return -1;
+            int64_t at = slab_pos(p, t, g, c);
+            return at < 0 ? -1 : p.slab_pt[sl.off + at];
+        };
+        auto usable = [&](const int64_t* c) { int64_t k = lookup(c); return k >= 0 && p.act[k]; };
+        for (int64_t e = p.ex_off[t]; e < p.ex_off[t + 1]; ++e) {
+            int64_t seed = p.ex[e];
+            if (!p.act[seed] || mark[seed] == t) continue;
+            // component: depth-T points connected through their 5^d stencils
+            int64_t mn[kMaxDim], mx[kMaxDim], c[kMaxDim], J[kMaxDim];
+            for (int j = 0; j < d; ++j) mn[j] = mx[j] = coord_at(p.pts[seed * d + j], T[j]);
+            std::vector<int64_t> stack{seed};
+            mark[seed] = t;
+            while (!stack.empty()) {
+                int64_t k = stack.back();
+                stack.pop_back();
+                for (int j = 0; j < d; ++j) {
+                    c[j] = coord_at(p.pts[k * d + j], T[j]);
+                    mn[j] = std::min(mn[j], c[j]);
+                    mx[j] = std::max(mx[j], c[j]);
+                }
+                // directions per dim: 0 centre, 1 left, 2 right, 3 left-left, 4 right-right
+                int dir[kMaxDim] = {0};
+                for (;;) {
+                    bool ok = true;
+                    for (int j = 0; j < d && ok; ++j) {
+                        switch (dir[j]) {
+                        case 0: J[j] = c[j]; break;
+                        case 1: ok = c[j] - 1 > 0; J[j] = c[j] - 1; break;
+                        case 2: ok = c[j] + 1 < g.cext[j]; J[j] = c[j] + 1; break;
+                        case 3: ok = c[j] - 1 > 0; J[j] = c[j] - 2; break;
+                        case 4: ok = c[j] + 1 < g.cext[j]; J[j] = c[j] + 2; break;
+                        }
+                    }
+                    if (ok) {
+                        int64_t q = lookup(J);
+                        if (q >= 0 && p.act[q] && mark[q] != t) {
+                            for (int j = 0; j < d; ++j) { mn[j] = std::min(mn[j], J[j]); mx[j] = std::max(mx[j], J[j]); }
+                            if (p.did[q] == t) { mark[q] = t; stack.push_back(q); }
+                        }
+                    }
+                    int j = 0;
+                    while (j < d && ++dir[j] == 5) { dir[j] = 0; ++j; }
+                    if (j == d) break;
+                }
+            }
+            // per dimension: pole length and matrix from the box's minimum corner
+            for (int dim = 0; dim < d; ++dim) {
+                const int64_t top = g.cext[dim];
+                int size = 1;
+                {
+                    int64_t w[kMaxDim];
+                    std::copy(mn, mn + d, w);
+                    while (w[dim] + 1 < top) {
+                        w[dim] += 1;
+                        if (!usable(w)) break;
+                        ++size;
+                    }
+                }
+                std::vector<double> R((size_t)size * 5, 0.0), L;
+                auto setM = [&](int i, int j, double v) {  // M[i][j]; entries outside the matrix are dropped
+                    if (i < 0 || i >= size || j < 0 || j >= size) return;
+                    R[(size_t)i * 5 + (size_t)(j - i + 2)] = v;
+                };
+                {
+                    int64_t w[kMaxDim];
+                    std::copy(mn, mn + d, w);
+                    int k = -1;
+                    const int depth = T[dim];
+                    while (w[dim] < top && usable(w)) {
+                        ++k;
+                        int64_t cp = w[dim];
+                        int pd = T[dim] - ctz64(cp);  // depth of the position in dim
+                        auto at = [&](int64_t off) { int64_t s2 = w[dim]; w[dim] = cp + off; bool u = w[dim] > 0 && w[dim] < top && usable(w); w[dim] = s2; return u; };
+                        if (pd == depth) {
+                            if (cp - 1 == 0) {
+                                setM(k, k, 0.9);
+                                if (pd == 1 && depth == 1) { setM(k, k, 1.0); break; }
+                                if (at(1)) setM(k + 1, k, -0.6);
+                                if (at(2)) setM(k + 2, k, 0.1);
+                            } else if (cp + 1 == top) {
+                                setM(k, k, 0.9);
+                                if (at(-1)) setM(k - 1, k, -0.6);
+                                if (at(-2)) setM(k - 2, k, 0.1);
+                            } else {
+                                setM(k, k, 1.0);
+                                if (at(-1)) setM(k - 1, k, -0.6);
+                                if (at(-2)) setM(k - 2, k, 0.1);
+                                if (at(1)) setM(k + 1, k, -0.6);
+                                if (at(2)) setM(k + 2, k, 0.1);
+                            }
+                        }
+                        if (pd < depth) {
+                            setM(k, k, 1.0);
+                            if (at(-1)) setM(k - 1, k, 0.5);
+                            if (at(1)) setM(k + 1, k, 0.5);
+                        }
+                        w[dim] += 1;
+                    }
+                }
+                PoleGroup pg{};
+                pg.t = t;
+                pg.dim = dim;
+                pg.size = size;
+                pg.lu_off = (int64_t)b.lu.size();
+                if (size >= 2) {
+                    band_lr(size, R, L);
+                    for (int k2 = 0; k2 < size; ++k2) {
+                        b.lu.push_back(k2 + 1 < size ? L[(size_t)(k2 + 1) * 5 + 1] : 0.0);
+                        b.lu.push_back(k2 + 2 < size ? L[(size_t)(k2 + 2) * 5 + 0] : 0.0);
+                        b.lu.push_back(R[(size_t)k2 * 5 + 2]);
+                        b.lu.push_back(k2 + 1 < size ? R[(size_t)k2 * 5 + 3] : 0.0);
+                        b.lu.push_back(k2 + 2 < size ? R[(size_t)k2 * 5 + 4] : 0.0);
+                    }
+                } else {
+                    b.lu.insert(b.lu.end(), {0.0, 0.0, R[2], 0.0, 0.0});
+                }
+                // poles: box positions with dim fixed at the minimum, dim 0 fastest
+                pg.pos_off = (int64_t)b.pole_pos.size();
+                int64_t w[kMaxDim];
+                std::copy(mn, mn + d, w);
+                int64_t np = 0;
+                for (;;) {
+                    int64_t q[kMaxDim];
+                    std::copy(w, w + d, q);
+                    for (int i = 0; i < size; ++i) {
+                        q[dim] = mn[dim] + i;
+                        int64_t k = lookup(q);
+                        bool isT = true;
+                        for (int j = 0; j < d; ++j) isT = isT && (q[j] & 1);
+                        b.pole_pos.push_back(k < 0 ? -1 : (int32_t)(4 * k + (p.act[k] ? 2 : 0) + (isT ? 1 : 0)));
+                    }
+                    ++np;
+                    int j = 0;
+                    for (; j < d; ++j) {
+                        if (j == dim) continue;
+                        if (w[j] == mx[j]) { w[j] = mn[j]; continue; }
+                        w[j] += 1;
+                        break;
+                    }
+                    if (j == d) break;
+                }
+                pg.npoles = np;
+                b.max_pole_elems = std::max(b.max_pole_elems, np * size);
+                b.groups.push_back(pg);
+            }
+        }
+    }
+    b.step_group.push_back((int32_t)b.groups.size());
+    b.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return true;
+}
+
 }  // namespace lsg

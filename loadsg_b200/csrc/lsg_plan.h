@@ -125,6 +125,45 @@ struct Plan {
     std::string error;
 };
 
+// Tables of the prewavelet basis transforms (BasisTransformations.cpp):
+// calcNodalByPrew evaluates a prewavelet expansion at every grid point,
+// calcPrewByNodal inverts it.  Built on first use of a transform.
+struct PoleGroup {        // one (depth, component, dimension) of calcPrewByNodal
+    int32_t t, dim, size;  // depth id, dimension, pole length
+    int32_t pad;
+    int64_t npoles;
+    int64_t pos_off;       // npoles * size entries: 4 * storage index + 2 * active + (depth == T), or -1
+    int64_t lu_off;        // 5 * size doubles: L[k+1][k], L[k+2][k], R[k][k], R[k][k+1], R[k][k+2]
+};
+
+struct BasisPlan {
+    std::vector<int32_t> order;       // depth ids coarse to fine (ListOfDepthOrderedSubgrids)
+    // prewavelet -> level-T nodal values over every point of depth T (hanging included)
+    StageSet nodal;
+    std::vector<int64_t> nodal_dom;   // nD*(d+1)
+    std::vector<int64_t> ex_sorted;   // per depth, its points sorted by level-T key (offsets: Plan::ex_off)
+    // hierarchization inside slab T: per slab entry and dim, the slab entries at
+    // the entry's own level left/right in that dim (global slab positions, -1 none)
+    std::vector<int32_t> slab_nb;     // M*d*2
+    std::vector<uint8_t> slab_dep;    // M*d: depth of the entry's point per dim
+    // full-grid (de)hierarchization: per point and dim, storage indices of the
+    // left/right neighbours at the point's own level (-1: boundary or absent)
+    std::vector<int32_t> pt_nb;       // n*d*2
+    int maxdep = 0;
+    std::vector<int64_t> lvl_off;     // (dim * (maxdep+1) + depth) -> range in lvl_pts (active points)
+    std::vector<int32_t> lvl_pts;
+    // calcPrewByNodal: pole groups in processing order, grouped per depth
+    std::vector<PoleGroup> groups;
+    std::vector<int32_t> step_t;      // depth id of each step (reverse subgrid order)
+    std::vector<int32_t> step_group;  // groups of step s: [step_group[s], step_group[s+1])
+    std::vector<int32_t> pole_pos;
+    std::vector<double> lu;
+    int64_t max_pole_elems = 0;       // largest npoles*size of a group
+    double seconds = 0.0;
+};
+
+bool build_basis_plan(const Plan& p, BasisPlan& b, std::string& error);
+
 // Builds the plan; returns false and sets plan.error on invalid input.
 bool build_plan(int d, int64_t n, const int32_t* points, const uint8_t* active, Plan& plan);
 

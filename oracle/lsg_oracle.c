@@ -657,3 +657,83 @@ int lsgo_cg(lsgo_grid *g, int family, const double *params, const double *f, dou
     free(z); free(r); free(gg); free(dv); free(h);
     return 0;
 }
+
+/* ------------------------------------------------------------ basis transforms
+ * BasisTransformations/BasisTransformations.cpp.  Subgrids are visited in the
+ * order of ListOfDepthOrderedSubgrids (sgrid/ListOfDepthOrderedGrids.cc:76-150):
+ * |T|_1 ascending, first appearance within equal norms; hierarchization runs
+ * the list backwards, dehierarchization forwards. */
+static int *subgrid_order(const lsgo_grid *g) {
+    int *o = (int *)malloc(sizeof(int) * (size_t)g->nD);
+    int n = 0, maxl1 = 0;
+    for (int t = 0; t < g->nD; ++t) {
+        int l1 = 0;
+        for (int k = 0; k < g->d; ++k) l1 += g->D[t * g->d + k];
+        if (l1 > maxl1) maxl1 = l1;
+    }
+    for (int l = 0; l <= maxl1; ++l)
+        for (int t = 0; t < g->nD; ++t) {
+            int l1 = 0;
+            for (int k = 0; k < g->d; ++k) l1 += g->D[t * g->d + k];
+            if (l1 == l) o[n++] = t;
+        }
+    return o;
+}
+
+/* v = v -+ 0.5 (Links(v) + Rechts(v)) on the points of every subgrid T' (<= lim
+ * when lim is given): CalcHierarchicalBasis (:13-38, :390-409, sign -1) and
+ * CalcNodalBasis (:174-198, sign +1) */
+static void hier_sweep(const lsgo_grid *g, const int *order, double *v, const int32_t *lim, int sign) {
+    int d = g->d;
+    for (int dd = 0; dd < d; ++dd) {
+        for (int q = 0; q < g->nD; ++q) {
+            int t = order[sign < 0 ? g->nD - 1 - q : q];
+            const int32_t *T = g->D + t * d;
+            if (T[dd] == 0 || (lim && !depth_le(T, lim, d))) continue;
+            for (int64_t e = g->ex_off[t]; e < g->ex_off[t + 1]; ++e) {
+                int64_t k = g->ex[e];
+                if (!g->act[k]) continue;  /* expression assignments touch active entries */
+                int64_t l = nbr(g, k, dd, 0), r = nbr(g, k, dd, 1);
+                double s = 0.5 * ((l >= 0 ? v[l] : 0.0) + (r >= 0 ? v[r] : 0.0));
+                v[k] = sign < 0 ? v[k] - s : v[k] + s;
+            }
+        }
+    }
+}
+
+int lsgo_nodal_by_prew(lsgo_grid *g, const double *prew, double *u) {
+    /* calcNodalByPrew (:670-706) with CalcHierbyPrew (:321-353) */
+    int d = g->d;
+    int *order = subgrid_order(g);
+    double *hier = (double *)calloc((size_t)g->n, sizeof(double));
+    double *hnew = (double *)malloc(sizeof(double) * (size_t)g->n);
+    if (!order || !hier || !hnew) { free(order); free(hier); free(hnew); return -1; }
+    stencil_t s;
+    int32_t J[MAXD];
+    for (int q = g->nD - 1; q >= 0; --q) {
+        int t = order[q];
+        const int32_t *T = g->D + t * d;
+        memset(hnew, 0, sizeof(double) * (size_t)g->n);
+        for (int64_t e = g->ex_off[t]; e < g->ex_off[t + 1]; ++e) {  /* every point of depth T */
+            int64_t k = g->ex[e];
+            double coeff = prew[k], w;
+            int pos[MAXD] = {0}, more;
+            stencil_build(g, k, &s);
+            do {
+                more = stencil_next(g, &s, pos, J, &w);
+                int64_t j = lsgo_lookup(g, J);
+                if (j >= 0) hnew[j] = hnew[j] + coeff * w;
+            } while (more);
+        }
+        hier_sweep(g, order, hnew, T, -1);
+        for (int64_t k = 0; k < g->n; ++k)
+            if (depth_le(g->dep + k * d, T, d)) hier[k] = hier[k] + hnew[k];
+    }
+    for (int64_t k = 0; k < g->n; ++k) u[k] = g->act[k] ? hier[k] : 0.0;  /* u = 0.0; u = hier */
+    hier_sweep(g, order, u, NULL, +1);
+    free(order);
+    free(hier);
+    free(hnew);
+    return 0;
+}
+

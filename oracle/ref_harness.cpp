@@ -13,7 +13,9 @@
 //     consumed by LocalStiffnessMatricesMemoryDistribution and
 //     MatrixVectorHomogen::multiplication (MatrixVectorHomogen.h:659-759);
 //   * the Jacobi diagonal (Preconditioning, applications/cg_method.h:81-754)
-//     and CG::solveHomogen (cg_method.h:759-886).
+//     and CG::solveHomogen (cg_method.h:759-886);
+//   * the basis transforms calcNodalByPrew / calcPrewByNodal
+//     (BasisTransformations/BasisTransformations.cpp:486-545,670-706).
 // Outputs are raw little-endian arrays in an output directory plus meta.txt;
 // tests/golden/make_golden.py packs them into .npz fixtures.
 #include "sparseEXPDE.h"
@@ -327,6 +329,18 @@ int main(int argc, char **argv) {
         dump("x.f64", x);
         g_meta << "iterations " << it << "\nrelres " << sqrt(rr / ff) << "\nsolve_seconds " << secs
                << "\nprecond_seconds " << tp << "\n";
+    } else if (cmd == "prew2nodal" || cmd == "nodal2prew") {
+        // prew2nodal: u = calcNodalByPrew(x); nodal2prew: p = calcPrewByNodal(x)
+        std::vector<double> x = read_f64(opt("x", ""), N);
+        VectorSparseG in(grid), out(grid);
+        set_vec(in, x);
+        auto t0 = std::chrono::steady_clock::now();
+        if (cmd == "prew2nodal") calcNodalByPrew(in, out);
+        else calcPrewByNodal(out, in);
+        double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        dump("y.f64", get_vec(out, N));
+        dump("x_after.f64", get_vec(in, N));
+        g_meta << "seconds " << secs << "\n";
     } else {
         fprintf(stderr, "unknown command %s\n", cmd.c_str());
         return 2;

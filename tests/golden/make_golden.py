@@ -8,6 +8,10 @@ it, and packs the arrays into tests/golden/<name>.npz.  The fixtures are small
 reference.
 
     python tests/golden/make_golden.py [--refsrc /path/to/library/source] [--only NAME]
+    python tests/golden/make_golden.py --cmds prew2nodal,nodal2prew   # add commands to existing fixtures
+
+prew2nodal / nodal2prew run calcNodalByPrew / calcPrewByNodal on the fixture's
+x (BasisTransformations/BasisTransformations.cpp:486-545,670-706).
 """
 import argparse
 import os
@@ -94,7 +98,7 @@ def make_case(name, d, gridargs, coef, cmds, refsrc):
         out["f"] = f
         for c in cmds:
             extra = []
-            if c in ("matvec", "poisson"):
+            if c in ("matvec", "poisson", "prew2nodal", "nodal2prew"):
                 extra = [f"x={tmp}/x_in.f64"]
             if c == "cg":
                 extra = [f"f={tmp}/f_in.f64", "eps=1e-20"]
@@ -114,15 +118,37 @@ def make_case(name, d, gridargs, coef, cmds, refsrc):
     print(f"{name}: N={n} -> {os.path.getsize(path)} bytes")
 
 
+def add_commands(name, d, gridargs, coef, cmds, refsrc):
+    """Runs further commands on an existing fixture's grid and x and stores their outputs."""
+    path = os.path.join(HERE, f"{name}.npz")
+    z = dict(np.load(path))
+    run(["make", "-s", "-C", ORACLE, "ref", f"D={d}", f"REFSRC={refsrc}", "-j8"])
+    exe = os.path.join(ORACLE, "_ref", f"d{d}", "ref_harness")
+    fam, params = coef
+    args = gridargs.split() + [f"coef={fam}", "cp=" + ",".join(repr(float(p)) for p in params)]
+    with tempfile.TemporaryDirectory() as tmp:
+        z["x"].tofile(os.path.join(tmp, "x_in.f64"))
+        for c in cmds:
+            run([exe, c, tmp] + args + [f"x={tmp}/x_in.f64"])
+            meta, arrs = read_meta(os.path.join(tmp, f"meta_{c}.txt"))
+            z.update(load_arrays(tmp, [a for a in arrs if a.startswith("y.")], c + "_"))
+    np.savez_compressed(path, **z)
+    print(f"{name}: added {cmds}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--refsrc", default="/root/reference/library/source")
     ap.add_argument("--only", default=None)
+    ap.add_argument("--cmds", default=None, help="comma list: add these commands to existing fixtures")
     a = ap.parse_args()
     for case in CASES:
         if a.only and case[0] != a.only:
             continue
-        make_case(*case, refsrc=a.refsrc)
+        if a.cmds:
+            add_commands(case[0], case[1], case[2], case[3], a.cmds.split(","), refsrc=a.refsrc)
+        else:
+            make_case(*case, refsrc=a.refsrc)
 
 
 if __name__ == "__main__":
