@@ -203,7 +203,7 @@ def batch_leg(lsg, torch, dev, stream, count=48, seed=7):
     log("batch: autotuned")
     f = torch.tensor(b.gather(fs), dtype=torch.float64, device=dev)
     x = torch.zeros_like(f)
-    o = lsg.SolverOpts(1e-10, 1, 20000, 0, lsg.FP32, 1000, 1e-5, 1)
+    o = lsg.SolverOpts(1e-10, 1, 3000, 0, lsg.FP32, 1000, 1e-5, 1)
     b.solve_device(f.data_ptr(), x.data_ptr(), o, stream)  # warm-up
     x.zero_()
     reps, tot = b.solve_device(f.data_ptr(), x.data_ptr(), o, stream)
@@ -228,6 +228,50 @@ def batch_leg(lsg, torch, dev, stream, count=48, seed=7):
             "setup_seconds": setup, "kernel_launches": int(tot["kernel_launches"])}
 
 
+def d8_sweep(lsg, torch, solve_up_to=40000):
+    """FP32/FP64 matvec time, algorithmic GB/s and cell-operator GFLOP/s on d=8
+    grids refined toward the hyperplane x_1 = 1/2 (regular level L, 2 rounds
+    adding the sons of points with |x_1 - 1/2| < 0.3 * 2^(1-r), completed),
+    a = 1 + 0.5 sin(2 pi x_1) cos(2 pi x_2); on the smaller grids also the
+    FP32+IR and FP64 solves to relative residual 1e-10."""
+    try:
+        hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        hbm = 6650.0
+    for level in (2, 3, 4):
+        t0 = time.perf_counter()
+        g = lsg.AdaptiveSparseGrid.adaptive(8, level, 2, 0.3, "plane")
+        prob = lsg.MidpointDiffusion(lsg.COEF_SIN2PI, [1.0, 0.5])
+        m = lsg.MatrixVectorHomogen(g, prob)
+        setup = time.perf_counter() - t0
+        info = m.info()
+        x32 = torch.randn(g.n, dtype=torch.float32, device="cuda")
+        y32 = torch.zeros_like(x32)
+        x64, y64 = x32.double(), torch.zeros(g.n, dtype=torch.float64, device="cuda")
+        m.profile(x32.data_ptr(), y32.data_ptr(), lsg.FP32, 1)
+        ms32, by32, flops = m.profile(x32.data_ptr(), y32.data_ptr(), lsg.FP32, 3)
+        ms64, by64, _ = m.profile(x64.data_ptr(), y64.data_ptr(), lsg.FP64, 2)
+        line = {"sweep": "d8_plane", "level": level, "refine": 2, "n_points": g.n, "n_active": g.getDOFS(),
+                "case_cells": int(info["case_cells"]), "device_bytes": int(info["device_bytes"]),
+                "setup_seconds": setup, "fp32_ms": ms32[4], "fp64_ms": ms64[4],
+                "fp32_gbs": by32[4] / (ms32[4] * 1e-3) / 1e9, "fp64_gbs": by64[4] / (ms64[4] * 1e-3) / 1e9,
+                "fp32_hbm_frac": by32[4] / (ms32[4] * 1e-3) / 1e9 / hbm,
+                "cell_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9}
+        if g.n <= solve_up_to:
+            rng = np.random.default_rng(0)
+            f = torch.tensor(rng.uniform(-1, 1, g.n) * g.active, device="cuda")
+            x = torch.zeros_like(f)
+            st = torch.cuda.current_stream().cuda_stream
+            for name, prec in (("fp32_ir", lsg.FP32), ("fp64", lsg.FP64)):
+                x.zero_()
+                r = lsg.CG.solve_device(m, f.data_ptr(), x.data_ptr(),
+                                        lsg.SolverOpts(1e-10, 1, 20000, 0, prec, 1000, 1e-5, 1), st)
+                line[f"{name}_solve"] = {"seconds": r["seconds"], "iterations": r["iterations"],
+                                         "rel_residual": r["rel_residual"]}
+        print(json.dumps(line), flush=True)
+        del m
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -237,6 +281,8 @@ def main():
     ap.add_argument("--workload", default="d6_adaptive_corner")
     ap.add_argument("--precond", type=int, default=2, help="0 Jacobi, 1 none, 2 learned diagonal")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--sweep", action="store_true",
+                    help="matvec sweep over d=8 grids refined toward x_1 = 1/2 (one JSON line per grid) instead")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -260,6 +306,10 @@ def main():
     import loadsg_b200 as lsg
 
     torch.cuda.set_device(local)
+    if args.sweep:
+        if rank == 0:
+            d8_sweep(lsg, torch)
+        return
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -302,7 +352,7 @@ def main():
     x = torch.zeros(g.n, dtype=torch.float64, device=dev)
 
     def opts(precision, precond):
-        return lsg.SolverOpts(1e-10, 1, 20000, precond, precision, 1000, 1e-5, 1)
+        return lsg.SolverOpts(1e-10, 1, 3000, precond, precision, 1000, 1e-5, 1)
 
     stream = torch.cuda.current_stream().cuda_stream
 
@@ -324,6 +374,7 @@ def main():
         ev0.record()
         for _ in range(args.steps):
             reps.append(solve(lsg.FP32, precond))
+            log(f"timed solve: {reps[-1]['iterations']} iterations, {reps[-1]['outer_iterations']} refinement steps")
         ev1.record()
         torch.cuda.synchronize()
     step_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
@@ -345,8 +396,9 @@ def main():
     te = time.perf_counter()
     for _ in range(args.steps):
         xh[:] = 0.0
-        lsg.CG.solveHomogen(1e-10, xh, f_host, m, prob, criterion=1, precision=lsg.FP32, max_iter=20000,
-                            precond=precond, inner_iter=1000, inner_tol=1e-5)
+        rep_e2e = lsg.CG.solveHomogen(1e-10, xh, f_host, m, prob, criterion=1, precision=lsg.FP32, max_iter=3000,
+                                      precond=precond, inner_iter=1000, inner_tol=1e-5)
+        log(f"e2e solve: {rep_e2e['iterations']} iterations, {rep_e2e['outer_iterations']} refinement steps")
     e2e_s = (time.perf_counter() - te) / args.steps
     log(f"e2e: {e2e_s:.2f}s per solve")
 

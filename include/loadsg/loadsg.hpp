@@ -130,6 +130,11 @@ public:
         check(lsg_matvec(op_, prew.getDatatableVector(), Ax.getDatatableVector()));
     }
     lsg_operator* handle() { return op_; }
+    // picks the matvec launch parameters by timing (lsg_operator_autotune); needs a problem set
+    void autotune(const MidpointDiffusion& problem, int32_t precision = LSG_FP32, int reps = 3) {
+        setProblem(problem);
+        check(lsg_operator_autotune(op_, precision, reps, nullptr, nullptr, nullptr));
+    }
 
 private:
     lsg_operator* op_ = nullptr;
@@ -160,5 +165,17 @@ struct CG {
         return true;
     }
 };
+
+// calcNodalByPrew(prew, u) / calcPrewByNodal(prew, u)
+// (BasisTransformations/BasisTransformations.h:119-125): the grid's flattened
+// tables live in the operator, so the operator is passed as well.
+template <int D>
+inline void calcNodalByPrew(const VectorSparseG<D>& prew, VectorSparseG<D>& u, MatrixVectorHomogen<D>& matrix) {
+    check(lsg_calc_nodal_by_prew(matrix.handle(), prew.getDatatableVector(), u.getDatatableVector()));
+}
+template <int D>
+inline void calcPrewByNodal(VectorSparseG<D>& prew, const VectorSparseG<D>& u, MatrixVectorHomogen<D>& matrix) {
+    check(lsg_calc_prew_by_nodal(matrix.handle(), prew.getDatatableVector(), u.getDatatableVector()));
+}
 
 }  // namespace lsg

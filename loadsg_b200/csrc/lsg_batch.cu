@@ -76,8 +76,8 @@ __device__ __forceinline__ double bsum(double v, double* red) {
 
 // Per-grid scalars, structure of arrays of `count` entries each.
 struct Scal {
-    double *delta, *dg, *tau, *dnew, *beta, *rr, *stop, *scale;
-    int32_t *conv, *its, *bad;
+    double *delta, *dg, *tau, *dnew, *beta, *rr, *stop, *scale, *best;
+    int32_t *conv, *its, *bad, *best_it;
     int32_t* pending;
 };
 
@@ -155,8 +155,10 @@ __global__ void kb_update_rxh(const Chunk* __restrict__ ch, const double* __rest
 }
 
 // per grid: delta_new, rr from the chunk partials; convergence test; iteration count
+// stall > 0 (inner FP32 solves of the refinement): a grid whose residual has
+// not dropped below 0.9 x its best for `stall` iterations stops iterating
 __global__ void kb_check(const int32_t* __restrict__ cb, const int32_t* __restrict__ ce, const double* __restrict__ part,
-                         Scal s, int crit, double eps, int count_its) {
+                         Scal s, int crit, double eps, int count_its, int stall) {
     __shared__ double red[32];
     int i = blockIdx.x;
     double a1 = 0.0, a2 = 0.0;
@@ -176,6 +178,11 @@ __global__ void kb_check(const int32_t* __restrict__ cb, const int32_t* __restri
     if (!isfinite(a1) || !isfinite(a2)) { s.bad[i] = 1; done = true; }
     else if (crit == 0) done = a1 < eps * eps || a1 <= eps;  // cg_method.h:852,871
     else done = a2 <= s.stop[i];
+    if (!count_its) { s.best[i] = a2; s.best_it[i] = s.its[i]; }
+    else if (stall > 0 && !done) {
+        if (a2 < 0.81 * s.best[i]) { s.best[i] = a2; s.best_it[i] = s.its[i]; }
+        else if (s.its[i] - s.best_it[i] >= stall) done = true;
+    }
     if (done) s.conv[i] = 1;
     else atomicAdd(s.pending, 1);
 }
@@ -311,6 +318,7 @@ struct BSolver {
     lsg_batch* B;
     int count;
     int64_t n;
+    int stall = 0;  // stall window of the current loop (0: off)
     Buf r, g, d, h, z, part, sc, flags, ff, rr64;
     Buf r32, g32, d32, h32, e32, z32;
     Buf outer_conv, outer_its;
@@ -324,8 +332,8 @@ struct BSolver {
         rc |= d.alloc(n * 8);
         rc |= h.alloc(n * 8);
         rc |= part.alloc((size_t)B->nchunks * 2 * 8);
-        rc |= sc.alloc((size_t)count * 8 * 8);
-        rc |= flags.alloc(((size_t)count * 3 + 1) * 4);
+        rc |= sc.alloc((size_t)count * 9 * 8);
+        rc |= flags.alloc(((size_t)count * 4 + 1) * 4);
         rc |= ff.alloc((size_t)count * 8);
         rc |= rr64.alloc((size_t)count * 8);
         rc |= outer_conv.alloc((size_t)count * 4);
@@ -348,11 +356,13 @@ struct BSolver {
         S.rr = s + 5 * count;
         S.stop = s + 6 * count;
         S.scale = s + 7 * count;
+        S.best = s + 8 * count;
         int32_t* f = flags.as<int32_t>();
         S.conv = f;
         S.its = f + count;
         S.bad = f + 2 * count;
-        S.pending = f + 3 * count;
+        S.best_it = f + 3 * count;
+        S.pending = f + 4 * count;
         for (Buf* bf : {&r, &g, &d, &h, &sc, &flags, &outer_conv, &outer_its, &r32, &g32, &d32, &h32, &e32})
             if (bf->p) BT_TRY(cudaMemset(bf->p, 0, bf->bytes));
         return 0;
@@ -379,7 +389,7 @@ struct BSolver {
         BT_TRY(cudaMemsetAsync(dv, 0, n * sizeof(V), st));
         kb_dot2<V><<<B->nchunks, kThreads, 0, st>>>(ch(), rv, hv, part.as<double>());
         BT_TRY(cudaMemsetAsync(S.pending, 0, 4, st));
-        kb_check<<<count, kThreads, 0, st>>>(cb(), ce(), part.as<double>(), S, crit, eps, 0);
+        kb_check<<<count, kThreads, 0, st>>>(cb(), ce(), part.as<double>(), S, crit, eps, 0, 0);
         kb_set_delta<<<nb(count), kThreads, 0, st>>>(count, S);
         BT_TRY(cudaGetLastError());
         return 0;
@@ -395,7 +405,7 @@ struct BSolver {
         kb_tau<<<nb(count), kThreads, 0, st>>>(count, S);
         kb_update_rxh<V><<<B->nchunks, kThreads, 0, st>>>(ch(), S.tau, rv, x, gv, dv, hv, zv, act(), part.as<double>());
         BT_TRY(cudaMemsetAsync(S.pending, 0, 4, st));
-        kb_check<<<count, kThreads, 0, st>>>(cb(), ce(), part.as<double>(), S, crit, eps, 1);
+        kb_check<<<count, kThreads, 0, st>>>(cb(), ce(), part.as<double>(), S, crit, eps, 1, stall);
         BT_TRY(cudaMemcpyAsync(pend_h, S.pending, 4, cudaMemcpyDeviceToHost, st));
         BT_TRY(cudaGetLastError());
         return 0;
@@ -543,8 +553,10 @@ int batch_solve(lsg_batch* b, const double* f, double* x, const lsg_solver_opts*
             rc = S.start<float>(S.r32.as<float>(), S.d32.as<float>(), S.h32.as<float>(), z32, 1, itol, st);
             if (rc) break;
             int ran = 0;
+            S.stall = 100;
             rc = S.loop<float>(S.e32.as<float>(), S.r32.as<float>(), S.g32.as<float>(), S.d32.as<float>(),
                                S.h32.as<float>(), z32, 1, itol, inner, graph, st, &ran, &launches);
+            S.stall = 0;
             if (rc) break;
             rounds += ran;
             kb_axpy_f32<<<b->nchunks, kThreads, 0, st>>>(S.ch(), S.S.scale, S.e32.as<float>(), x);

@@ -1632,7 +1632,7 @@ int cg_body(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, bool want_rr, c
 // h, d, s[0], s[3] the start state.  Returns iterations in *its.
 template <typename V>
 int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int crit, double rr_stop, int maxit,
-            bool use_graph, cudaStream_t st, int* its, double* last_rr, int64_t* launches) {
+            bool use_graph, cudaStream_t st, int* its, double* last_rr, int64_t* launches, int stall_window = 0) {
     cudaGraphExec_t exec = nullptr;
     bool want_rr = crit == 1;
     int it = 0;
@@ -1652,6 +1652,12 @@ int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int
     CUDA_TRY(cudaMemcpyAsync(S.pin.h, S.s.as<double>(), 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     if ((crit == 0 && !(S.pin.h[0] > eps)) || (crit == 1 && S.pin.h[5] <= rr_stop)) maxit = 0;
+    // stall_window > 0 (inner FP32 solves of the refinement): stop once the
+    // recursive residual has not dropped below 0.9 x its best value for that
+    // many iterations -- FP32 cannot reduce it further, the outer FP64
+    // residual takes over
+    double best = S.pin.h[5];
+    int best_it = 0;
     for (int i = 1; i <= maxit; ++i) {
         if (use_graph) {
             cudaError_t e = cudaGraphLaunch(exec, st);
@@ -1670,6 +1676,10 @@ int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int
         // (cg_method.h:852,871) -- so it ends as soon as delta' <= eps as well
         if (crit == 0 && (dn < eps * eps || dn <= eps)) break;
         if (crit == 1 && S.pin.h[5] <= rr_stop) break;
+        if (stall_window > 0) {
+            if (S.pin.h[5] < 0.81 * best) { best = S.pin.h[5]; best_it = i; }
+            else if (i - best_it >= stall_window) break;
+        }
     }
     if (exec) cudaGraphExecDestroy(exec);
     *its = it;
@@ -1783,7 +1793,8 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
         double* r = S.r.as<double>();
         int total = 0, outer = 0;
         double rr_prev = -1.0;
-        for (outer = 0; outer < maxit && total < maxit * 4; ++outer) {
+        int slow_steps = 0;
+        for (outer = 0; outer < maxit && total < maxit; ++outer) {
             CUDA_TRY(cudaMemsetAsync(r, 0, n * 8, st));
             rc = lsg_internal_matvec64(op, x, r, st);
             if (rc) break;
@@ -1799,6 +1810,12 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
                 if (rc) break;
                 k_to_f32<<<nblk(n), 256, 0, st>>>(n, op->diag.as<double>(), S.z32.as<float>());
                 z32 = S.z32.as<float>();
+            }
+            // refinement that stopped making progress (with the exact diagonal): give up
+            if (rr_prev > 0 && rr > 0.25 * rr_prev) {
+                if (++slow_steps >= 3) { rc = fail(LSG_E_NOCONV, "iterative refinement stagnated"); break; }
+            } else {
+                slow_steps = 0;
             }
             rr_prev = rr;
             double nr = std::sqrt(rr);
@@ -1821,7 +1838,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             int its = 0;
             double lrr = 0.0;
             rc = cg_loop<float>(S, e32, r32, S.g32.as<float>(), d32, h32, z32, 0.0, 1, itol * itol, inner,
-                                o->use_graph != 0, st, &its, &lrr, &R.kernel_launches);
+                                o->use_graph != 0, st, &its, &lrr, &R.kernel_launches, 100);
             R.kernel_launches += matvec_launches(op->plan) + 12;
             if (rc) break;
             total += its;

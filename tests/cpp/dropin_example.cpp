@@ -22,7 +22,13 @@ int main() {
         rr += r * r;
         ff += f.getValue(k) * f.getValue(k);
     }
-    std::printf("N=%lld iterations=%d relres=%.3e\n", (long long)grid.getMaximalOccupiedSecondTable(), it,
-                std::sqrt(rr / ff));
-    return std::sqrt(rr / ff) < 1e-8 ? 0 : 1;
+    // solution read out as nodal values and back (calcNodalByPrew / calcPrewByNodal)
+    lsg::VectorSparseG<3> u(grid), back(grid);
+    lsg::calcNodalByPrew<3>(x, u, m);
+    lsg::calcPrewByNodal<3>(back, u, m);
+    double dmax = 0;
+    for (int64_t k = 0; k < x.size(); ++k) dmax = std::fmax(dmax, std::fabs(back.getValue(k) - x.getValue(k)));
+    std::printf("N=%lld iterations=%d relres=%.3e transform round trip %.3e\n",
+                (long long)grid.getMaximalOccupiedSecondTable(), it, std::sqrt(rr / ff), dmax);
+    return (std::sqrt(rr / ff) < 1e-8 && dmax < 1e-10) ? 0 : 1;
 }
