@@ -27,6 +27,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -231,17 +232,68 @@ __device__ __forceinline__ void wht_face(V* v, int g) {
 // Segments (instead of whole columns) keep all lanes busy when dim 0 is long
 // and the other dims short.  All lanes of a warp run the same number of
 // rounds and iterations (the group shuffles need them).
+// FP32 face transform on packed pairs (Blackwell f32x2 add/FMA): value 2q+e of
+// the face is component e of v[q]; local dim 1 (bit 0) pairs the two
+// components, local dims 2..DL-1 pair whole float2s, dims DL..D-1 go across
+// lanes.  Bitwise the same as wht_face<D, float> (p - q is fma(q, -1, p)).
+template <int D>
+__device__ __forceinline__ void wht_face_f2(float2* v, int g) {
+    constexpr int DL = CellCfg<D>::DL, NP = CellCfg<D>::NH / 2;
+    const float2 neg1 = make_float2(-1.f, -1.f);
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+        float a = v[q].x, b = v[q].y;
+        v[q] = make_float2(a + b, a - b);
+    }
+#pragma unroll
+    for (int k = 1; k < DL - 1; ++k)
+#pragma unroll
+        for (int q = 0; q < NP; ++q)
+            if (!(q & (1 << (k - 1)))) {
+                float2 p = v[q], w = v[q | (1 << (k - 1))];
+                v[q] = __fadd2_rn(p, w);
+                v[q | (1 << (k - 1))] = __ffma2_rn(w, neg1, p);
+            }
+#pragma unroll
+    for (int k = DL; k < D; ++k) {
+        int m = 1 << (k - DL);
+        float sg = (g & m) ? -1.f : 1.f;
+        float2 sgn = make_float2(sg, sg);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            float2 p;
+            p.x = __shfl_xor_sync(0xffffffffu, v[q].x, m);
+            p.y = __shfl_xor_sync(0xffffffffu, v[q].y, m);
+            v[q] = __ffma2_rn(sgn, v[q], p);
+        }
+    }
+}
+
+// z += sum over the slab's cells of a_c H diag(lam) H u_c on a dense slab.
+// Work unit = a segment of `seg` consecutive cells of one dim-0 column (seg and
+// the column length 2^T_0 are powers of two, so every segment is full and the
+// unit decode is shifts and masks).  The Hadamard transform factorises as
+// H = H_0 (x) H_rest; the H_rest transform of a face is shared by the two cells
+// on either side of it, so per cell only the new (right) face is transformed
+// forward, and the left-face outputs of this cell and the right-face outputs
+// of the previous one are summed before one inverse H_rest.  A segment
+// transforms its first left face itself and scatters its last right face;
+// faces on the boundary drop out.  Segments (instead of whole columns) keep
+// all lanes busy when dim 0 is long and the other dims short.  All lanes of a
+// warp run the same number of rounds and iterations (the group shuffles need
+// them); a lane group without a unit works on zeros.
 template <int D, typename V>
 __device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, const V* __restrict__ ac, const V* lamg,
                             int32_t segmax) {
     constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NH = CellCfg<D>::NH;
+    constexpr bool PACK = std::is_same<V, float>::value && NH >= 4;
     const int g = threadIdx.x & (G - 1);
     const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
-    const int32_t c0 = s.ext[0] + 1;  // cells along dim 0
-    const int32_t seg = c0 < segmax ? c0 : segmax;
-    const int32_t nseg = (c0 + seg - 1) / seg;
-    const int64_t ncols = s.ncell / c0;
-    const int64_t units = ncols * nseg;
+    const int lc0 = s.T[0];
+    const int32_t c0 = 1 << lc0;  // cells along dim 0
+    const int lseg = min(lc0, 31 - __clz(segmax));
+    const int32_t seg = 1 << lseg;
+    const int64_t units = s.ncell >> lseg;
     const int64_t rounds = (units + ngroups - 1) / ngroups;
     V lp[NH], lm[NH];  // eigenvalues for s_0 = + (bit 0 clear) and s_0 = - (bit 0 set)
 #pragma unroll
@@ -249,16 +301,15 @@ __device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, con
     for (int64_t r = 0; r < rounds; ++r) {
         int64_t unit = r * ngroups + group;
         bool live = unit < units;
-        int64_t col = live ? unit / nseg : 0;
-        int32_t m0s = live ? (int32_t)(unit % nseg) * seg : 0;
-        int32_t m0e = min(m0s + seg, c0);
+        int64_t cell0 = live ? unit << lseg : 0;  // linear index of the segment's first cell
+        int32_t m0s = (int32_t)(cell0 & (c0 - 1));
+        int64_t col = cell0 >> lc0;
         int32_t m[D];
-        int64_t rem = col;
+        int sh = 0;
 #pragma unroll
         for (int k = 1; k < D; ++k) {
-            int32_t ck = s.ext[k] + 1;
-            m[k] = (int32_t)(rem % ck);
-            rem /= ck;
+            m[k] = (int32_t)((col >> sh) & ((1 << s.T[k]) - 1));
+            sh += s.T[k];
         }
         int32_t off[NH];
         bool ok[NH];
@@ -273,47 +324,142 @@ __device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, con
                 good = good && c >= 1 && c <= s.ext[k];
                 o += (c - 1) * s.stride[k];
             }
-            off[j] = o;
+            off[j] = o + m0s;  // slab position of face corner j at dim-0 coordinate m0s + 1
             ok[j] = good;
         }
-        V lh[NH], cr[NH];  // transformed left face, carried right-face output
+        const V* acol = ac + cell0;
+        if constexpr (PACK) {
+            constexpr int NP = NH / 2;
+            float2 lp2[NP], lm2[NP];
 #pragma unroll
-        for (int j = 0; j < NH; ++j) {
-            lh[j] = (ok[j] && m0s >= 1) ? u[off[j] + m0s - 1] : V(0);
-            cr[j] = V(0);
-        }
-        wht_face<D, V>(lh, g);
-        const V* acol = ac + col * c0;
-        for (int32_t i = 0; i < seg; ++i) {
-            int32_t m0 = m0s + i;
-            bool cv = live && m0 < m0e;
-            V rh[NH];
-            bool rin = cv && m0 + 1 <= s.ext[0];
+            for (int q = 0; q < NP; ++q) {
+                lp2[q] = make_float2((float)lp[2 * q], (float)lp[2 * q + 1]);
+                lm2[q] = make_float2((float)lm[2 * q], (float)lm[2 * q + 1]);
+            }
+            float2 lh[NP], cr[NP];
 #pragma unroll
-            for (int j = 0; j < NH; ++j) rh[j] = (ok[j] && rin) ? u[off[j] + m0] : V(0);
-            wht_face<D, V>(rh, g);
-            V a = cv ? acol[m0] : V(0);
-            V outl[NH];
+            for (int q = 0; q < NP; ++q) {
+                lh[q].x = (ok[2 * q] && m0s >= 1) ? u[off[2 * q] - 1] : 0.f;
+                lh[q].y = (ok[2 * q + 1] && m0s >= 1) ? u[off[2 * q + 1] - 1] : 0.f;
+                cr[q] = make_float2(0.f, 0.f);
+            }
+            wht_face_f2<D>(lh, g);
+            const float2 neg1 = make_float2(-1.f, -1.f);
+#pragma unroll 2
+            for (int32_t i = 0; i < seg; ++i) {
+                const int32_t m0 = m0s + i;
+                const bool rin = m0 + 1 < c0;
+                float2 rh[NP];
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    rh[q].x = (ok[2 * q] && rin) ? u[off[2 * q] + i] : 0.f;
+                    rh[q].y = (ok[2 * q + 1] && rin) ? u[off[2 * q + 1] + i] : 0.f;
+                }
+                wht_face_f2<D>(rh, g);
+                float a = live ? (float)acol[i] : 0.f;
+                float2 a2 = make_float2(a, a);
+                float2 outl[NP];
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    float2 sp = __fmul2_rn(__fadd2_rn(lh[q], rh[q]), __fmul2_rn(a2, lp2[q]));
+                    float2 sm = __fmul2_rn(__ffma2_rn(rh[q], neg1, lh[q]), __fmul2_rn(a2, lm2[q]));
+                    outl[q] = __fadd2_rn(__fadd2_rn(sp, sm), cr[q]);
+                    lh[q] = rh[q];
+                    cr[q] = __ffma2_rn(sm, neg1, sp);
+                }
+                wht_face_f2<D>(outl, g);
+                if (m0 >= 1) {
+#pragma unroll
+                    for (int q = 0; q < NP; ++q) {
+                        if (ok[2 * q]) atomicAdd((float*)&z[off[2 * q] + i - 1], outl[q].x);
+                        if (ok[2 * q + 1]) atomicAdd((float*)&z[off[2 * q + 1] + i - 1], outl[q].y);
+                    }
+                }
+            }
+            // right face of the segment's last cell, unless it lies on the boundary
+            wht_face_f2<D>(cr, g);
+            if (m0s + seg < c0) {
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    if (ok[2 * q]) atomicAdd((float*)&z[off[2 * q] + seg - 1], cr[q].x);
+                    if (ok[2 * q + 1]) atomicAdd((float*)&z[off[2 * q + 1] + seg - 1], cr[q].y);
+                }
+            }
+        } else {
+            V lh[NH], cr[NH];  // transformed left face, carried right-face output
 #pragma unroll
             for (int j = 0; j < NH; ++j) {
-                V sp = (lh[j] + rh[j]) * (a * lp[j]);
-                V sm = (lh[j] - rh[j]) * (a * lm[j]);
-                outl[j] = sp + sm + cr[j];
-                if (cv) {
+                lh[j] = (ok[j] && m0s >= 1) ? u[off[j] - 1] : V(0);
+                cr[j] = V(0);
+            }
+            wht_face<D, V>(lh, g);
+            for (int32_t i = 0; i < seg; ++i) {
+                const int32_t m0 = m0s + i;
+                const bool rin = m0 + 1 < c0;
+                V rh[NH];
+#pragma unroll
+                for (int j = 0; j < NH; ++j) rh[j] = (ok[j] && rin) ? u[off[j] + i] : V(0);
+                wht_face<D, V>(rh, g);
+                V a = live ? acol[i] : V(0);
+                V outl[NH];
+#pragma unroll
+                for (int j = 0; j < NH; ++j) {
+                    V sp = (lh[j] + rh[j]) * (a * lp[j]);
+                    V sm = (lh[j] - rh[j]) * (a * lm[j]);
+                    outl[j] = sp + sm + cr[j];
                     lh[j] = rh[j];
                     cr[j] = sp - sm;
                 }
+                wht_face<D, V>(outl, g);
+                if (m0 >= 1) {
+#pragma unroll
+                    for (int j = 0; j < NH; ++j)
+                        if (ok[j]) atomicAdd(&z[off[j] + i - 1], outl[j]);
+                }
             }
-            wht_face<D, V>(outl, g);
+            wht_face<D, V>(cr, g);
+            if (m0s + seg < c0) {
 #pragma unroll
-            for (int j = 0; j < NH; ++j)
-                if (cv && ok[j] && m0 >= 1) atomicAdd(&z[off[j] + m0 - 1], outl[j]);
+                for (int j = 0; j < NH; ++j)
+                    if (ok[j]) atomicAdd(&z[off[j] + seg - 1], cr[j]);
+            }
         }
-        // right face of the segment's last cell, unless it lies on the boundary
-        wht_face<D, V>(cr, g);
+    }
+}
+
+// FP32 full-cell transform on packed pairs: value 2q+e of the lane's NL
+// corners is component e of v[q]; bit 0 inside pairs, bits 1..DL-1 across
+// pairs, dims DL..D-1 across lanes.  Bitwise the same as wht_group<D, float>.
+template <int D>
+__device__ __forceinline__ void wht_group_f2(float2* v, int g) {
+    constexpr int DL = CellCfg<D>::DL, NP = CellCfg<D>::NL / 2;
+    const float2 neg1 = make_float2(-1.f, -1.f);
 #pragma unroll
-        for (int j = 0; j < NH; ++j)
-            if (ok[j] && m0e < c0) atomicAdd(&z[off[j] + m0e - 1], cr[j]);
+    for (int q = 0; q < NP; ++q) {
+        float a = v[q].x, b = v[q].y;
+        v[q] = make_float2(a + b, a - b);
+    }
+#pragma unroll
+    for (int k = 1; k < DL; ++k)
+#pragma unroll
+        for (int q = 0; q < NP; ++q)
+            if (!(q & (1 << (k - 1)))) {
+                float2 p = v[q], w = v[q | (1 << (k - 1))];
+                v[q] = __fadd2_rn(p, w);
+                v[q | (1 << (k - 1))] = __ffma2_rn(w, neg1, p);
+            }
+#pragma unroll
+    for (int k = DL; k < D; ++k) {
+        int m = 1 << (k - DL);
+        float sg = (g & m) ? -1.f : 1.f;
+        float2 sgn = make_float2(sg, sg);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            float2 p;
+            p.x = __shfl_xor_sync(0xffffffffu, v[q].x, m);
+            p.y = __shfl_xor_sync(0xffffffffu, v[q].y, m);
+            v[q] = __ffma2_rn(sgn, v[q], p);
+        }
     }
 }
 
@@ -321,6 +467,7 @@ template <int D, typename V>
 __device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __restrict__ u, V* z,
                              const V* __restrict__ ac, const V* lamg) {
     constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NL = CellCfg<D>::NL;
+    constexpr bool PACK = std::is_same<V, float>::value && NL >= 4;
     const int g = threadIdx.x & (G - 1);
     const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
     const int64_t rounds = (s.ncell + ngroups - 1) / ngroups;
@@ -329,20 +476,40 @@ __device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __rest
         bool live = ci < s.ncell;
         const int32_t* cp = P.cell_corner + ((s.corner_off + (live ? ci : 0)) << D) + (g << DL);
         int32_t pos[NL];
-        V v[NL];
 #pragma unroll
-        for (int b = 0; b < NL; ++b) {
-            pos[b] = live ? cp[b] : -1;
-            v[b] = pos[b] >= 0 ? u[pos[b]] : V(0);
-        }
-        wht_group<D, V>(v, g);
+        for (int b = 0; b < NL; ++b) pos[b] = live ? cp[b] : -1;
         V a = live ? ac[ci] : V(0);
+        if constexpr (PACK) {
+            constexpr int NP = NL / 2;
+            float2 v[NP];
 #pragma unroll
-        for (int b = 0; b < NL; ++b) v[b] *= a * lamg[b];
-        wht_group<D, V>(v, g);
+            for (int q = 0; q < NP; ++q) {
+                v[q].x = pos[2 * q] >= 0 ? u[pos[2 * q]] : 0.f;
+                v[q].y = pos[2 * q + 1] >= 0 ? u[pos[2 * q + 1]] : 0.f;
+            }
+            wht_group_f2<D>(v, g);
+            float2 a2 = make_float2((float)a, (float)a);
 #pragma unroll
-        for (int b = 0; b < NL; ++b)
-            if (pos[b] >= 0) atomicAdd(&z[pos[b]], v[b]);
+            for (int q = 0; q < NP; ++q)
+                v[q] = __fmul2_rn(v[q], __fmul2_rn(a2, make_float2((float)lamg[2 * q], (float)lamg[2 * q + 1])));
+            wht_group_f2<D>(v, g);
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                if (pos[2 * q] >= 0) atomicAdd((float*)&z[pos[2 * q]], v[q].x);
+                if (pos[2 * q + 1] >= 0) atomicAdd((float*)&z[pos[2 * q + 1]], v[q].y);
+            }
+        } else {
+            V v[NL];
+#pragma unroll
+            for (int b = 0; b < NL; ++b) v[b] = pos[b] >= 0 ? u[pos[b]] : V(0);
+            wht_group<D, V>(v, g);
+#pragma unroll
+            for (int b = 0; b < NL; ++b) v[b] *= a * lamg[b];
+            wht_group<D, V>(v, g);
+#pragma unroll
+            for (int b = 0; b < NL; ++b)
+                if (pos[b] >= 0) atomicAdd(&z[pos[b]], v[b]);
+        }
     }
 }
 
@@ -1937,7 +2104,8 @@ __global__ void k_pattern(int64_t n, double* x64, float* x32) {
 
 bool tuning_valid(const lsg_tuning& t) {
     auto warps = [](int v, int lo, int hi) { return v >= lo && v <= hi && v % 32 == 0; };
-    return warps(t.cell_threads, 64, 256) && t.cell_segment >= 1 && t.cell_segment <= 64 && t.class_ratio >= 2 &&
+    return warps(t.cell_threads, 64, 256) && t.cell_segment >= 1 && t.cell_segment <= 64 &&
+           (t.cell_segment & (t.cell_segment - 1)) == 0 && t.class_ratio >= 2 &&
            t.class_ratio <= 1024 && warps(t.level_threads, 32, 128) && t.level_cap >= 256 && t.level_cap <= 65536 &&
            warps(t.prolong_threads, 32, 1024);
 }
