@@ -163,9 +163,15 @@ __global__ void k_prolong(DevPlan P, V* __restrict__ pc, int32_t item0) {
 // lane g of the group holds the NL = 2^DL corners whose high bits (dims
 // DL..D-1) equal g.  The Walsh-Hadamard butterflies of dims < DL are
 // register-local, those of dims >= DL use warp shuffles inside the group.
-template <int D>
+// lane-group layout: FP32 keeps 2^3 corners per lane (smaller register
+// footprint, three CTAs per SM), FP64 2^4 (measured on d = 6 grids)
+#ifndef LSG_F32_LOCAL_DIMS
+#define LSG_F32_LOCAL_DIMS 3
+#endif
+template <int D, typename V>
 struct CellCfg {
-    static constexpr int DL = D <= 4 ? D : 4;
+    static constexpr int KDL = std::is_same<V, float>::value ? LSG_F32_LOCAL_DIMS : 4;
+    static constexpr int DL = D <= KDL ? D : KDL;
     static constexpr int G = 1 << (D - DL);
     static constexpr int NL = 1 << DL;
     static constexpr int NH = NL / 2;  // corners per dim-0 face held by one lane
@@ -173,7 +179,7 @@ struct CellCfg {
 
 template <int D, typename V>
 __device__ __forceinline__ void wht_group(V* v, int g) {
-    constexpr int DL = CellCfg<D>::DL, NL = CellCfg<D>::NL;
+    constexpr int DL = CellCfg<D, V>::DL, NL = CellCfg<D, V>::NL;
 #pragma unroll
     for (int k = 0; k < DL; ++k)
 #pragma unroll
@@ -199,7 +205,7 @@ __device__ __forceinline__ void wht_group(V* v, int g) {
 // local dims 1..DL-1 (bit k-1 of the local index), dims DL..D-1 across lanes.
 template <int D, typename V>
 __device__ __forceinline__ void wht_face(V* v, int g) {
-    constexpr int DL = CellCfg<D>::DL, NH = CellCfg<D>::NH;
+    constexpr int DL = CellCfg<D, V>::DL, NH = CellCfg<D, V>::NH;
 #pragma unroll
     for (int k = 0; k < DL - 1; ++k)
 #pragma unroll
@@ -238,7 +244,7 @@ __device__ __forceinline__ void wht_face(V* v, int g) {
 // lanes.  Bitwise the same as wht_face<D, float> (p - q is fma(q, -1, p)).
 template <int D>
 __device__ __forceinline__ void wht_face_f2(float2* v, int g) {
-    constexpr int DL = CellCfg<D>::DL, NP = CellCfg<D>::NH / 2;
+    constexpr int DL = CellCfg<D, float>::DL, NP = CellCfg<D, float>::NH / 2;
     const float2 neg1 = make_float2(-1.f, -1.f);
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
@@ -285,7 +291,7 @@ __device__ __forceinline__ void wht_face_f2(float2* v, int g) {
 template <int D, typename V>
 __device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, const V* __restrict__ ac, const V* lamg,
                             int32_t segmax) {
-    constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NH = CellCfg<D>::NH;
+    constexpr int DL = CellCfg<D, V>::DL, G = CellCfg<D, V>::G, NH = CellCfg<D, V>::NH;
     constexpr bool PACK = std::is_same<V, float>::value && NH >= 4;
     const int g = threadIdx.x & (G - 1);
     const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
@@ -432,7 +438,7 @@ __device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, con
 // pairs, dims DL..D-1 across lanes.  Bitwise the same as wht_group<D, float>.
 template <int D>
 __device__ __forceinline__ void wht_group_f2(float2* v, int g) {
-    constexpr int DL = CellCfg<D>::DL, NP = CellCfg<D>::NL / 2;
+    constexpr int DL = CellCfg<D, float>::DL, NP = CellCfg<D, float>::NL / 2;
     const float2 neg1 = make_float2(-1.f, -1.f);
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
@@ -466,7 +472,7 @@ __device__ __forceinline__ void wht_group_f2(float2* v, int g) {
 template <int D, typename V>
 __device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __restrict__ u, V* z,
                              const V* __restrict__ ac, const V* lamg) {
-    constexpr int DL = CellCfg<D>::DL, G = CellCfg<D>::G, NL = CellCfg<D>::NL;
+    constexpr int DL = CellCfg<D, V>::DL, G = CellCfg<D, V>::G, NL = CellCfg<D, V>::NL;
     constexpr bool PACK = std::is_same<V, float>::value && NL >= 4;
     const int g = threadIdx.x & (G - 1);
     const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
@@ -518,7 +524,7 @@ __device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __rest
 // class): the cell operator does not depend on the gM chain, so it needs no
 // wavefront ordering.  u and z live in shared memory when 2 N_T fits.
 template <int D, typename V>
-__global__ void __launch_bounds__(256, 2) k_cells(DevPlan P, const V* __restrict__ pc, V* __restrict__ zb,
+__global__ void __launch_bounds__(256, std::is_same<V, float>::value ? 3 : 2) k_cells(DevPlan P, const V* __restrict__ pc, V* __restrict__ zb,
                                                   const V* __restrict__ acell, const V* __restrict__ lam_all,
                                                   const int32_t* __restrict__ order, int32_t ord0, int64_t cap,
                                                   int32_t segmax) {
@@ -528,7 +534,7 @@ __global__ void __launch_bounds__(256, 2) k_cells(DevPlan P, const V* __restrict
     const DevSlab& s = P.slabs[it.t];
     V* lam = reinterpret_cast<V*>(smem_raw);
     for (int b = threadIdx.x; b < NC; b += blockDim.x) lam[b] = lam_all[(int64_t)it.t * NC + b];
-    const V* lamg = lam + ((threadIdx.x & (CellCfg<D>::G - 1)) << CellCfg<D>::DL);
+    const V* lamg = lam + ((threadIdx.x & (CellCfg<D, V>::G - 1)) << CellCfg<D, V>::DL);
     const V* u_g = pc + it.p_off;
     V* z_g = zb + it.p_off;
     const V* ac = acell + s.cell_off;
