@@ -188,16 +188,17 @@ def train(out=DEFAULT_WEIGHTS, d=5, level=4, refine=2, n_train=64, n_val=8, epoc
     import torch
     F = n_features(d)
     t0 = time.time()
+    levels = list(level) if isinstance(level, (list, tuple)) else [level]
     feats, targets = [], []
     for s in range(n_train):
-        _, _, m = make_instance(d, level, refine, s, family)
+        _, _, m = make_instance(d, levels[s % len(levels)], refine, s, family)
         X, y = instance_data(m)
         feats.append(X)
         targets.append(y)
     X = torch.cat(feats)
     Y = torch.cat(targets)
     log(f"training rows {X.shape[0]} from {n_train} instances ({time.time() - t0:.1f}s)")
-    val = [make_instance(d, level, refine, 10000 + s, family) for s in range(n_val)]
+    val = [make_instance(d, levels[-1], refine, 10000 + s, family) for s in range(n_val)]  # deepest grids
     net = MLP(F, seed=seed)
     gen = torch.Generator(device="cuda").manual_seed(seed)
     best = (None, float("inf"), None)
@@ -255,17 +256,20 @@ def main():
     ap.add_argument("cmd", choices=["train", "report"])
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--d", type=int, default=5)
-    ap.add_argument("--level", type=int, default=4)
+    ap.add_argument("--level", default="4", help="level, or comma list cycled over the training instances")
     ap.add_argument("--refine", type=int, default=2)
     ap.add_argument("--family", default="lognormal")
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--n-train", type=int, default=64)
+    ap.add_argument("--n-val", type=int, default=8)
     ap.add_argument("--seeds", default="10000,10001,10002,10003")
     a = ap.parse_args()
     if a.cmd == "train":
-        train(out=a.out, d=a.d, level=a.level, refine=a.refine, epochs=a.epochs, n_train=a.n_train, family=a.family)
+        levels = [int(v) for v in a.level.split(",")]
+        train(out=a.out, d=a.d, level=levels, refine=a.refine, epochs=a.epochs, n_train=a.n_train, n_val=a.n_val,
+              family=a.family)
     else:
-        report(a.out, a.d, a.level, a.refine, a.family, [int(x) for x in a.seeds.split(",")])
+        report(a.out, a.d, int(a.level.split(",")[-1]), a.refine, a.family, [int(x) for x in a.seeds.split(",")])
 
 
 if __name__ == "__main__":
