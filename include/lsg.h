@@ -190,7 +190,7 @@ typedef struct {
     int32_t cell_threads;    /* threads per cell-operator CTA: 64..256, multiple of 32 */
     int32_t cell_segment;    /* dim-0 cells per work unit on complete slabs: a power of two, 1..64 */
     int32_t class_ratio;     /* slab-size ratio that starts a new cell-operator launch: 2..1024 */
-    int32_t level_threads;   /* threads per restriction-wavefront CTA: 32..128, multiple of 32 */
+    int32_t level_threads;   /* threads per restriction-wavefront CTA: 32..512, multiple of 32 */
     int32_t level_cap;       /* shared-memory elements per wavefront ping-pong buffer: 256..65536 */
     int32_t prolong_threads; /* threads per prolongation CTA: 32..1024, multiple of 32 */
 } lsg_tuning;

@@ -563,7 +563,7 @@ __global__ void __launch_bounds__(256, std::is_same<V, float>::value ? 3 : 2) k_
 // the restriction steps with the gM swap-add, and ConvertToPrewavelet2 into y.
 // Buffers ping-pong in shared memory when the item's largest vector fits.
 template <int D, typename V>
-__global__ void __launch_bounds__(128) k_level(DevPlan P, const V* __restrict__ zb, V* __restrict__ gm,
+__global__ void __launch_bounds__(512) k_level(DevPlan P, const V* __restrict__ zb, V* __restrict__ gm,
                                                V* __restrict__ scratch, V* __restrict__ y, int32_t item0,
                                                int64_t buf_elems) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -986,7 +986,7 @@ struct lsg_operator {
     bool have_learned = false;
     int64_t smem_cap64 = 0, smem_cap32 = 0;
     std::vector<int64_t> level_need;  // per phase-B level: largest vector of any item
-    lsg_tuning tune{256, 8, 4, 128, 12288, 256};  // launch parameters (lsg_operator_autotune)
+    lsg_tuning tune{256, 8, 4, 512, 12288, 256};  // launch parameters (lsg_operator_autotune)
     std::shared_ptr<void> basis;      // basis-transform tables (lsg_basis.cu), built on first use
     DBuf cell_order;                  // phase-B items ordered by slab size (k_cells)
     std::vector<int32_t> cell_class_off;  // size classes in cell_order
@@ -2112,7 +2112,7 @@ bool tuning_valid(const lsg_tuning& t) {
     auto warps = [](int v, int lo, int hi) { return v >= lo && v <= hi && v % 32 == 0; };
     return warps(t.cell_threads, 64, 256) && t.cell_segment >= 1 && t.cell_segment <= 64 &&
            (t.cell_segment & (t.cell_segment - 1)) == 0 && t.class_ratio >= 2 &&
-           t.class_ratio <= 1024 && warps(t.level_threads, 32, 128) && t.level_cap >= 256 && t.level_cap <= 65536 &&
+           t.class_ratio <= 1024 && warps(t.level_threads, 32, 512) && t.level_cap >= 256 && t.level_cap <= 65536 &&
            warps(t.prolong_threads, 32, 1024);
 }
 
@@ -2174,7 +2174,7 @@ extern "C" int lsg_operator_autotune(lsg_operator* op, int32_t precision, int32_
     double cur_ms = time_cfg(cur), def_ms = cur_ms;
     const std::vector<std::pair<int32_t lsg_tuning::*, std::vector<int32_t>>> space = {
         {&lsg_tuning::cell_segment, {4, 8, 16}},      {&lsg_tuning::cell_threads, {128, 256}},
-        {&lsg_tuning::class_ratio, {2, 4, 16}},       {&lsg_tuning::level_threads, {64, 128}},
+        {&lsg_tuning::class_ratio, {2, 4, 16}},       {&lsg_tuning::level_threads, {64, 128, 256, 512}},
         {&lsg_tuning::level_cap, {4096, 8192, 12288}}, {&lsg_tuning::prolong_threads, {128, 256, 512}}};
     for (int pass = 0; pass < 2 && !err; ++pass) {
         bool moved = false;

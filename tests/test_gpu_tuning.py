@@ -19,6 +19,7 @@ SETTINGS = [
     dict(cell_segment=64, class_ratio=1024),
     dict(level_threads=32, level_cap=256),     # most wavefront items spill to global scratch
     dict(level_threads=64, level_cap=65536),
+    dict(level_threads=512),
     dict(prolong_threads=32),
     dict(prolong_threads=1024, cell_threads=64),
 ]
@@ -53,7 +54,7 @@ def test_every_setting_matches_reference(cases, setting):
 def test_invalid_settings_are_rejected(cases):
     _, _, m = make(cases[0])
     for bad in (dict(cell_threads=512), dict(cell_threads=100), dict(cell_segment=0), dict(class_ratio=1),
-                dict(level_threads=256), dict(level_cap=16), dict(prolong_threads=2048)):
+                dict(level_threads=1024), dict(level_cap=16), dict(prolong_threads=2048)):
         with pytest.raises(lsg.LsgError):
             m.set_tuning(**bad)
 
