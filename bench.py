@@ -417,6 +417,10 @@ def main():
     except Exception:
         hbm, peak_src = 6650.0, "fallback"
     achieved = by32[3] / (ms32[3] * 1e-3) / 1e9
+    # DRAM bytes of one phase B on this workload, from the ncu capture summarised in
+    # profiles/phaseB_dram_d6_adaptive_corner.md (dram__bytes_read.sum + dram__bytes_write.sum
+    # over the 21 phase-B launches of one FP32 matvec)
+    traffic = 2.23e9 if args.workload == "d6_adaptive_corner" else None
 
     batch = None if args.no_batch else batch_leg(lsg, torch, dev, stream)
 
@@ -444,10 +448,12 @@ def main():
         "tuning": {"setting": tune_setting, "matvec_ms_fp32": tune_ms, "matvec_ms_fp32_default": tune_default_ms},
         "matvec": {"fp32_ms": ms32[4], "fp64_ms": ms64[4], "fp32_gbs": by32[4] / (ms32[4] * 1e-3) / 1e9,
                    "fp64_gbs": by64[4] / (ms64[4] * 1e-3) / 1e9, "phase_ms_fp32": list(ms32[:4]),
-                   "cell_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9},
+                   "cell_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9,
+                   # nominal FP32 rate: 148 SMs x 128 lanes x 2 flops x 1.965 GHz = 74.4 TFLOP/s
+                   "cell_fp32_frac_of_nominal": flops / (ms32[3] * 1e-3) / 74.4e12},
         "roofline": {"bound": "hbm", "kernel": "phase B: k_cells (cell operator) + k_level (restriction wavefronts)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": peak_src, "traffic": None},
+                     "peak_source": peak_src, "traffic": traffic, "traffic_unit": "bytes per phase B (ncu)"},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16 * g.n, "d2h_bytes_per_step": 8 * g.n},
         "setup_seconds": setup_s, "plan_seconds": info["plan_seconds"], "device_bytes": info["device_bytes"],
         "clocks": clk.summary(),
