@@ -173,6 +173,16 @@ def cpu_reference_sample(args):
             "sample_seconds": secs, "sample_points": n, "per_dof_us": secs / n * 1e6}
 
 
+def max_over_ranks(x, dist, device):
+    """The slowest rank's value (replicas: the job takes as long as its slowest GPU)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 _T0 = time.perf_counter()
 
 
@@ -377,11 +387,7 @@ def main():
             log(f"timed solve: {reps[-1]['iterations']} iterations, {reps[-1]['outer_iterations']} refinement steps")
         ev1.record()
         torch.cuda.synchronize()
-    step_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
-    if dist:
-        t = torch.tensor([step_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_s = float(t.item())
+    step_s = max_over_ranks(ev0.elapsed_time(ev1) / 1e3 / args.steps, dist, dev)
 
     # plain FP64 CG on the same instance (the comparison the metric names; the
     # reference's CG is always Jacobi-preconditioned), and FP32+IR with Jacobi

@@ -1,0 +1,58 @@
+"""Host-side logic of bench.py for N > 1 GPUs, on CPU: replicas only (one
+independent instance per rank, no collective on the data path), timing is the
+maximum over ranks, and the reference arm runs on rank 0 alone.  Ranks are
+processes on a gloo process group over 127.0.0.1."""
+import os
+import socket
+import subprocess
+import sys
+
+import numpy as np
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        out[rank] = bench.max_over_ranks(1.5 + rank, dist, "cpu")
+    finally:
+        dist.destroy_process_group()
+
+
+def test_time_is_max_over_ranks():
+    world = 2
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
+        assert dict(out) == {0: 2.5, 1: 2.5}
+
+
+def test_single_process_value_passes_through():
+    assert bench.max_over_ranks(3.25, None, "cpu") == 3.25
+
+
+def test_each_rank_solves_its_own_instance():
+    g0, fam0, p0, f0, _ = bench.workload("d3_regular_L7", 0)
+    g1, fam1, p1, f1, _ = bench.workload("d3_regular_L7", 1)
+    assert g0.n == g1.n and fam0 == fam1  # same size per GPU: weak scaling
+    assert not np.array_equal(f0, f1)     # independent right-hand sides
+    assert not np.any(f0[g0.active == 0])
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
+                       capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == ""
