@@ -291,6 +291,8 @@ def main():
     ap.add_argument("--workload", default="d6_adaptive_corner")
     ap.add_argument("--precond", type=int, default=2, help="0 Jacobi, 1 none, 2 learned diagonal")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-grids", type=int, default=48, help="grids in the batch leg")
+    ap.add_argument("--batch-only", action="store_true", help="run only the batch leg (one JSON line)")
     ap.add_argument("--sweep", action="store_true",
                     help="matvec sweep over d=8 grids refined toward x_1 = 1/2 (one JSON line per grid) instead")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -319,6 +321,12 @@ def main():
     if args.sweep:
         if rank == 0:
             d8_sweep(lsg, torch)
+        return
+    if args.batch_only:
+        dev = torch.device("cuda", local)
+        b = batch_leg(lsg, torch, dev, torch.cuda.current_stream().cuda_stream, count=args.batch_grids)
+        if rank == 0:
+            print(json.dumps({"batch": b}))
         return
     dist = None
     if world > 1:
@@ -428,7 +436,7 @@ def main():
     # over the 21 phase-B launches of one FP32 matvec)
     traffic = 2.23e9 if args.workload == "d6_adaptive_corner" else None
 
-    batch = None if args.no_batch else batch_leg(lsg, torch, dev, stream)
+    batch = None if args.no_batch else batch_leg(lsg, torch, dev, stream, count=args.batch_grids)
 
     if rank != 0:
         if dist:
