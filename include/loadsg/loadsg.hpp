@@ -105,6 +105,7 @@ private:
 struct MidpointDiffusion {
     int32_t family;
     std::vector<double> params;
+    int32_t form = LSG_FORM_STIFFNESS;  // LSG_FORM_MASS: a(x) u v (HelmHoltz for a = 1)
 };
 
 template <int D>
@@ -118,8 +119,10 @@ public:
     MatrixVectorHomogen& operator=(const MatrixVectorHomogen&) = delete;
 
     void setProblem(const MidpointDiffusion& p) {
-        if (have_ && p.family == fam_ && p.params == par_) return;
+        if (have_ && p.family == fam_ && p.params == par_ && p.form == form_) return;
         check(lsg_operator_set_coefficient(op_, p.family, p.params.data(), (int32_t)p.params.size()));
+        check(lsg_operator_set_form(op_, p.form));
+        form_ = p.form;
         fam_ = p.family;
         par_ = p.params;
         have_ = true;
@@ -139,7 +142,7 @@ public:
 private:
     lsg_operator* op_ = nullptr;
     bool have_ = false;
-    int32_t fam_ = -1;
+    int32_t fam_ = -1, form_ = LSG_FORM_STIFFNESS;
     std::vector<double> par_;
 };
 

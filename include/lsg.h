@@ -39,6 +39,13 @@ extern "C" {
 #define LSG_COEF_LOGNORMAL 3
 #define LSG_COEF_SIN2PI 4
 
+/* Bilinear form of the local matrices (lsg_operator_set_form): the plugin's
+ * a(x_c) times the exact Q1 stiffness (StencilTemplate::integration of a
+ * diffusion plugin, stencils/Stencil.h:740) or times the exact Q1 mass
+ * (HelmHoltz::integration, stencils/Stencil.h:900-919, for a = 1). */
+#define LSG_FORM_STIFFNESS 0
+#define LSG_FORM_MASS 1
+
 typedef struct lsg_operator lsg_operator;
 
 typedef struct {
@@ -169,6 +176,12 @@ int lsg_operator_features(lsg_operator *op, float *feat, void *stream);
 int lsg_operator_base_diag(lsg_operator *op, double *base, void *stream);
 /* D = base * softplus(mlp(features)) at active points, installed for precond = 2 */
 int lsg_operator_install_learned(lsg_operator *op, lsg_mlp *m, void *stream);
+
+/* Selects the bilinear form of the matvec and the diagonal: LSG_FORM_STIFFNESS
+ * (default; -div(a grad u)) or LSG_FORM_MASS (a u, the reference's HelmHoltz
+ * operator for a = 1: right-hand sides <f, psi_i> from nodal values of f and
+ * L2 norms u^T M u).  The CG solvers take either form. */
+int lsg_operator_set_form(lsg_operator *op, int32_t form);
 
 /* ---- prewavelet basis transforms (BasisTransformations/BasisTransformations.cpp).
  * lsg_calc_nodal_by_prew: u = values at every grid point (hanging included) of

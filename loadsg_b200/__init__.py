@@ -124,6 +124,7 @@ def lib():
             "lsg_plan_export_stencil": (ctypes.c_int, [P, I64, P, P, P]),
             "lsg_grid_regular": (ctypes.c_int, [I32, I32, P, I64, P]),
             "lsg_grid_adaptive": (ctypes.c_int, [I32, I32, I32, D, I32, I32, P, P, I64, P]),
+            "lsg_operator_set_form": (ctypes.c_int, [P, I32]),
             "lsg_calc_nodal_by_prew": (ctypes.c_int, [P, P, P]),
             "lsg_calc_prew_by_nodal": (ctypes.c_int, [P, P, P]),
             "lsg_calc_nodal_by_prew_device": (ctypes.c_int, [P, P, P, P]),
@@ -212,10 +213,15 @@ class AdaptiveSparseGrid:
         return (2 * (idx - (1 << t)) + 1) / (2.0 ** t)
 
 
+FORM_STIFFNESS, FORM_MASS = 0, 1
+
+
 class MidpointDiffusion:
     """-div(a grad u) with a sampled at cell midpoints: the local stiffness
     entry of a cell is a(x_c) times the exact Q1 entry (the value a
     StencilTemplate::integration plugin returns, stencils/Stencil.h:740)."""
+
+    form = FORM_STIFFNESS
 
     def __init__(self, family, params):
         self.family = int(family)
@@ -223,6 +229,15 @@ class MidpointDiffusion:
         p = np.asarray(params, np.float64).ravel()
         self.params[: len(p)] = p
         self.nparams = len(p)
+
+
+class MidpointMass(MidpointDiffusion):
+    """a(x) u v with a sampled at cell midpoints: a(x_c) times the exact Q1 mass
+    entry.  For a = 1 this is the reference's HelmHoltz operator
+    (stencils/Stencil.h:873-919): right-hand sides <f, psi_i> from nodal values
+    of f, and L2 norms u^T M u of prewavelet expansions."""
+
+    form = FORM_MASS
 
 
 class Plan:
@@ -312,6 +327,7 @@ class MatrixVectorHomogen:
     def set_problem(self, problem):
         if problem is not self._problem:
             _check(lib().lsg_operator_set_coefficient(self._h, problem.family, _ptr(problem.params), problem.nparams))
+            _check(lib().lsg_operator_set_form(self._h, problem.form))
             self._problem = problem
 
     def info(self):

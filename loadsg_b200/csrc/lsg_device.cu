@@ -674,7 +674,7 @@ __global__ void k_cell_coef(DevPlan P, int64_t c_lo, int64_t c_hi, int t_lo, int
 // cells inside the grid that touch the support of psi_i of
 // a_c * sum_k qK_k prod_{j!=k} qM_j (v is a tensor product on every such cell).
 template <int D>
-__global__ void k_diag(DevPlan P, const double* __restrict__ acell, double* __restrict__ diag) {
+__global__ void k_diag(DevPlan P, const double* __restrict__ acell, double* __restrict__ diag, int form) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= P.n) return;
     if (!P.act[k]) { diag[k] = 0.0; return; }
@@ -735,11 +735,16 @@ __global__ void k_diag(DevPlan P, const double* __restrict__ acell, double* __re
                 qM[j] = h[j] * (a * a + a * b + b * b) / 3.0;
             }
             double sum = 0.0;
-            for (int i = 0; i < D; ++i) {
-                double prod = qK[i];
-                for (int j = 0; j < D; ++j)
-                    if (j != i) prod *= qM[j];
-                sum += prod;
+            if (form == 1) {  // mass: prod_j qM_j
+                sum = 1.0;
+                for (int j = 0; j < D; ++j) sum *= qM[j];
+            } else {
+                for (int i = 0; i < D; ++i) {
+                    double prod = qK[i];
+                    for (int j = 0; j < D; ++j)
+                        if (j != i) prod *= qM[j];
+                    sum += prod;
+                }
             }
             acc += acell[s.cell_off + ci] * sum;
         }
@@ -968,7 +973,9 @@ struct lsg_operator {
     // tables
     DBuf slabs, did, act, exa_off, exa, cell_key, cell_corner, nodal_stage, nodal_src, nodal_code, nodal_dom, nodal_scr,
         conv_stage, conv_src, conv_code, conv_dom, prol, restr, a_items, b_items, b_steps, pts, cell_slab_off;
-    DBuf lam64, lam32;
+    DBuf lam64, lam32;   // Hadamard-basis eigenvalues of the Q1 stiffness (form 0)
+    DBuf mu64, mu32;     // ... of the Q1 mass (form 1)
+    int32_t form = 0;
     // coefficient (one family and parameter set per part of a concatenated plan)
     bool have_coef = false;
     int32_t family = 0;
@@ -1083,8 +1090,8 @@ int upload_plan(lsg_operator* op) {
     if (rc) return LSG_E_CUDA;
     // Hadamard-basis eigenvalues of the Q1 element per depth, 1/2^d folded in
     int nc = 1 << d;
-    std::vector<double> lam(p.nD * (size_t)nc);
-    std::vector<float> lamf(lam.size());
+    std::vector<double> lam(p.nD * (size_t)nc), mu_t(lam.size());
+    std::vector<float> lamf(lam.size()), muf_t(lam.size());
     for (int t = 0; t < p.nD; ++t) {
         double h[lsg::kMaxDim];
         for (int k = 0; k < d; ++k) h[k] = std::ldexp(1.0, -p.slabs[t].T[k]);
@@ -1099,10 +1106,16 @@ int upload_plan(lsg_operator* op) {
             }
             lam[(size_t)t * nc + sgn] = l / nc;
             lamf[(size_t)t * nc + sgn] = (float)(l / nc);
+            double mu = 1.0;  // mass: M1 = (h/6)[[2,1],[1,2]] has eigenvalues h/2 (+) and h/6 (-)
+            for (int j = 0; j < d; ++j) mu *= ((sgn >> j) & 1) ? h[j] / 6.0 : h[j] / 2.0;
+            mu_t[(size_t)t * nc + sgn] = mu / nc;
+            muf_t[(size_t)t * nc + sgn] = (float)(mu / nc);
         }
     }
     rc |= op->lam64.upload(lam, tot);
     rc |= op->lam32.upload(lamf, tot);
+    rc |= op->mu64.upload(mu_t, tot);
+    rc |= op->mu32.upload(muf_t, tot);
     if (rc) return LSG_E_CUDA;
     DevPlan& P = op->dp;
     P.d = d;
@@ -1209,7 +1222,8 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t
     rc = set_phaseB_smem<D, V>();
     if (rc) return rc;
     const V* acell = std::is_same<V, double>::value ? (const V*)op->acell64.p : (const V*)op->acell32.p;
-    const V* lam = std::is_same<V, double>::value ? (const V*)op->lam64.p : (const V*)op->lam32.p;
+    const V* lam = std::is_same<V, double>::value ? (const V*)(op->form ? op->mu64.p : op->lam64.p)
+                                                  : (const V*)(op->form ? op->mu32.p : op->lam32.p);
     int64_t na = p.exa_off[p.nD];
     if (ev) cudaEventRecord(ev[0], st);
     if (na > 0) k_zero_active<V><<<nblk(na), 256, 0, st>>>(op->dp.exa, na, y);
@@ -1279,14 +1293,14 @@ int compute_diag(lsg_operator* op, cudaStream_t st) {
     const double* a = op->acell64.as<double>();
     double* dg = op->diag.as<double>();
     switch (op->plan.d) {
-    case 1: k_diag<1><<<g, 128, 0, st>>>(op->dp, a, dg); break;
-    case 2: k_diag<2><<<g, 128, 0, st>>>(op->dp, a, dg); break;
-    case 3: k_diag<3><<<g, 128, 0, st>>>(op->dp, a, dg); break;
-    case 4: k_diag<4><<<g, 128, 0, st>>>(op->dp, a, dg); break;
-    case 5: k_diag<5><<<g, 128, 0, st>>>(op->dp, a, dg); break;
-    case 6: k_diag<6><<<g, 128, 0, st>>>(op->dp, a, dg); break;
-    case 7: k_diag<7><<<g, 128, 0, st>>>(op->dp, a, dg); break;
-    case 8: k_diag<8><<<g, 128, 0, st>>>(op->dp, a, dg); break;
+    case 1: k_diag<1><<<g, 128, 0, st>>>(op->dp, a, dg, op->form); break;
+    case 2: k_diag<2><<<g, 128, 0, st>>>(op->dp, a, dg, op->form); break;
+    case 3: k_diag<3><<<g, 128, 0, st>>>(op->dp, a, dg, op->form); break;
+    case 4: k_diag<4><<<g, 128, 0, st>>>(op->dp, a, dg, op->form); break;
+    case 5: k_diag<5><<<g, 128, 0, st>>>(op->dp, a, dg, op->form); break;
+    case 6: k_diag<6><<<g, 128, 0, st>>>(op->dp, a, dg, op->form); break;
+    case 7: k_diag<7><<<g, 128, 0, st>>>(op->dp, a, dg, op->form); break;
+    case 8: k_diag<8><<<g, 128, 0, st>>>(op->dp, a, dg, op->form); break;
     }
     CUDA_TRY(cudaGetLastError());
     op->have_diag = true;
@@ -2118,6 +2132,14 @@ bool tuning_valid(const lsg_tuning& t) {
 
 }  // namespace
 
+extern "C" int lsg_operator_set_form(lsg_operator* op, int32_t form) {
+    if (!op) return fail(LSG_E_INVALID, "null operator");
+    if (form != LSG_FORM_STIFFNESS && form != LSG_FORM_MASS) return fail(LSG_E_INVALID, "unknown operator form");
+    if (form != op->form) op->have_diag = false;
+    op->form = form;
+    return 0;
+}
+
 extern "C" int lsg_operator_get_tuning(const lsg_operator* op, lsg_tuning* t) {
     if (!op || !t) return fail(LSG_E_INVALID, "null argument");
     *t = op->tune;
@@ -2262,7 +2284,8 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
     int rc = set_phaseB_smem<D, V>();
     if (rc) return rc;
     const V* acell = std::is_same<V, double>::value ? (const V*)op->acell64.p : (const V*)op->acell32.p;
-    const V* lam = std::is_same<V, double>::value ? (const V*)op->lam64.p : (const V*)op->lam32.p;
+    const V* lam = std::is_same<V, double>::value ? (const V*)(op->form ? op->mu64.p : op->lam64.p)
+                                                  : (const V*)(op->form ? op->mu32.p : op->lam32.p);
     // Every region is written before it is read within one call (nodal slabs by
     // k_nodal, P by k_pinit, gM only where an earlier item of the same call
     // wrote it, item scratch by its own item), so nothing needs clearing;

@@ -41,6 +41,7 @@ def lib():
         L.lsgo_diag.argtypes = [P, ctypes.c_int, P, P]
         L.lsgo_cg.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_double, ctypes.c_int, P]
         L.lsgo_nodal_by_prew.argtypes = [P, P, P]
+        L.lsgo_set_form.argtypes = [P, ctypes.c_int]
         _LIB = L
     return _LIB
 
@@ -92,7 +93,9 @@ class OracleGrid:
         p[: len(params)] = params
         return p
 
-    def matvec(self, family, params, x, y=None):
+    def matvec(self, family, params, x, y=None, form=0):
+        """form 0: diffusion (stiffness), 1: mass (the reference's HelmHoltz local matrix)."""
+        lib().lsgo_set_form(self._h, form)
         x = np.ascontiguousarray(x, np.float64)
         y = np.zeros(self.n) if y is None else np.array(y, np.float64)
         p = self._params(params)
@@ -100,7 +103,8 @@ class OracleGrid:
             raise MemoryError("oracle matvec failed")
         return y
 
-    def diag(self, family, params):
+    def diag(self, family, params, form=0):
+        lib().lsgo_set_form(self._h, form)
         out = np.zeros(self.n)
         p = self._params(params)
         lib().lsgo_diag(self._h, family, _ptr(p), _ptr(out))
@@ -131,6 +135,7 @@ class OracleGrid:
         return p
 
     def cg(self, family, params, f, eps, maxit=500, x0=None):
+        lib().lsgo_set_form(self._h, 0)
         f = np.ascontiguousarray(f, np.float64)
         x = np.zeros(self.n) if x0 is None else np.array(x0, np.float64)
         p = self._params(params)

@@ -74,4 +74,18 @@ static inline double lsg_q1_stiffness(int d, const double *h, unsigned p, unsign
     return sum;
 }
 
+/* Exact Q1 mass entry (coefficient 1): prod_j (same side ? h_j/3 : h_j/6), the
+ * value HelmHoltz::integration returns (stencils/Stencil.h:900-919 with
+ * integral_RR = h^3/3, integral_LR = h^3/6, times exponent^2 = 1/h^2). */
+static inline double lsg_q1_mass(int d, const double *h, unsigned p, unsigned q) {
+    double prod = 1.0;
+    for (int j = 0; j < d; ++j) prod *= (((p >> j) & 1u) == ((q >> j) & 1u)) ? h[j] / 3.0 : h[j] / 6.0;
+    return prod;
+}
+
+/* form 0: stiffness (diffusion), 1: mass */
+static inline double lsg_q1_entry(int form, int d, const double *h, unsigned p, unsigned q) {
+    return form == 1 ? lsg_q1_mass(d, h, p, q) : lsg_q1_stiffness(d, h, p, q);
+}
+
 #endif

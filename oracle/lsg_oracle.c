@@ -29,6 +29,7 @@ struct lsgo_grid {
     int32_t *D;     /* nD*d */
     int32_t *did;   /* per point: position of its depth in the depth list */
     int32_t maxdep[MAXD];
+    int form;        /* 0 stiffness (diffusion), 1 mass: the local matrix of the plugin */
     int64_t *ex_off; /* points of exact depth, storage order */
     int64_t *ex;
     struct celllist **cells; /* per depth, built on first use */
@@ -335,7 +336,7 @@ static void cells_apply(lsgo_grid *g, int t, int family, const double *params, c
             for (unsigned q = p; q < (1u << d); ++q) {
                 int64_t kq = corner[q];
                 if (kq < 0) continue;
-                double val = a * lsg_q1_stiffness(d, cl->h, p, q);
+                double val = a * lsg_q1_entry(g->form, d, cl->h, p, q);
                 if (p == q) z[kq] += val * u[kp];
                 else {
                     z[kq] += val * u[kp];
@@ -606,7 +607,7 @@ int lsgo_diag(lsgo_grid *g, int family, const double *params, double *diag) {
                     for (unsigned q = 0; q < (1u << d); ++q) {
                         int64_t kq = corner[q];
                         if (kq < 0 || v[kq] == 0.0) continue;
-                        acc += v[kp] * a * lsg_q1_stiffness(d, cl->h, p, q) * v[kq];
+                        acc += v[kp] * a * lsg_q1_entry(g->form, d, cl->h, p, q) * v[kq];
                     }
                 }
             }
@@ -737,3 +738,4 @@ int lsgo_nodal_by_prew(lsgo_grid *g, const double *prew, double *u) {
     return 0;
 }
 
+void lsgo_set_form(lsgo_grid *g, int form) { g->form = form; }

@@ -42,6 +42,10 @@ int lsgo_diag(lsgo_grid *g, int family, const double *params, double *diag);
 int lsgo_cg(lsgo_grid *g, int family, const double *params, const double *f, double *x, double eps,
             int maxit, int *iterations);
 
+/* Local matrix of the plugin used by lsgo_matvec / lsgo_diag / lsgo_cg:
+ * 0 = a(x_c) * Q1 stiffness (default), 1 = a(x_c) * Q1 mass (HelmHoltz). */
+void lsgo_set_form(lsgo_grid *g, int form);
+
 /* calcNodalByPrew (BasisTransformations/BasisTransformations.cpp:670-706):
  * u = values at every point of the expansion sum_i prew_i psi_i (all points). */
 int lsgo_nodal_by_prew(lsgo_grid *g, const double *prew, double *u);

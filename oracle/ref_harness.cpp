@@ -76,6 +76,7 @@ class MidpointDiffusion : public StencilTemplate {
 public:
     int family;
     std::vector<double> p;
+    int form = 0;  // 0: a(x_c) * Q1 stiffness, 1: a(x_c) * Q1 mass
     MidpointDiffusion(AdaptiveSparseGrid &g, int fam, std::vector<double> par)
         : StencilTemplate(g), family(fam), p(par) { p.resize(LSG_COEF_MAXPARAM, 0.0); }
     double integration(CellDimension &cell, CellIndexDirection &dp, CellIndexDirection &dq) override {
@@ -88,7 +89,7 @@ public:
             if (dp.getDirection(d) == Right) mp |= 1u << d;
             if (dq.getDirection(d) == Right) mq |= 1u << d;
         }
-        return lsg_coef_eval(family, p.data(), D, xc) * lsg_q1_stiffness(D, h, mp, mq);
+        return lsg_coef_eval(family, p.data(), D, xc) * lsg_q1_entry(form, D, h, mp, mq);
     }
 };
 
@@ -275,6 +276,24 @@ int main(int argc, char **argv) {
         dump_grid(grid);
     } else if (cmd == "tables") {
         dump_tables(grid);
+    } else if (cmd == "mass" || cmd == "helmholtz") {
+        // mass: the midpoint plugin with the Q1 mass matrix; helmholtz: the
+        // reference's own HelmHoltz stencil (Stencil.h:873-919, coefficient 1)
+        std::vector<double> x = read_f64(opt("x", ""), N);
+        MultiLevelAdaptiveSparseGrid mgrid(&grid);
+        MatrixVectorHomogen m(grid, mgrid, true, false);
+        VectorSparseG xv(grid), yv(grid);
+        set_vec(xv, x);
+        if (cmd == "helmholtz") {
+            HelmHoltz helm(grid);
+            m.multiplication(xv, yv, helm);
+        } else {
+            MidpointDiffusion plug = make_plugin(grid);
+            plug.form = 1;
+            LocalStiffnessMatricesMemoryDistribution lsm(grid, plug, 1);
+            m.multiplication(xv, yv, lsm);
+        }
+        dump("y.f64", get_vec(yv, N));
     } else if (cmd == "matvec" || cmd == "poisson") {
         std::vector<double> x = read_f64(opt("x", ""), N);
         MultiLevelAdaptiveSparseGrid mgrid(&grid);
@@ -298,8 +317,9 @@ int main(int argc, char **argv) {
         }
         dump("y.f64", get_vec(yv, N));
         g_meta << "matvec_seconds " << secs << "\n";
-    } else if (cmd == "diag") {
+    } else if (cmd == "diag" || cmd == "massdiag") {
         MidpointDiffusion plug = make_plugin(grid);
+        if (cmd == "massdiag") plug.form = 1;
         LocalStiffnessMatricesMemoryDistribution lsm(grid, plug, 1);
         VectorSparseG z(grid);
         Preconditioning<LocalStiffnessMatricesMemoryDistribution> P(z, lsm);

@@ -11,7 +11,9 @@ reference.
     python tests/golden/make_golden.py --cmds prew2nodal,nodal2prew   # add commands to existing fixtures
 
 prew2nodal / nodal2prew run calcNodalByPrew / calcPrewByNodal on the fixture's
-x (BasisTransformations/BasisTransformations.cpp:486-545,670-706).
+x (BasisTransformations/BasisTransformations.cpp:486-545,670-706); mass /
+massdiag use the midpoint plugin with the Q1 mass matrix, helmholtz the
+reference's own HelmHoltz stencil (stencils/Stencil.h:873-919).
 """
 import argparse
 import os
@@ -99,7 +101,7 @@ def make_case(name, d, gridargs, coef, cmds, refsrc):
         out["f"] = f
         for c in cmds:
             extra = []
-            if c in ("matvec", "poisson", "prew2nodal", "nodal2prew"):
+            if c in ("matvec", "poisson", "prew2nodal", "nodal2prew", "mass", "helmholtz"):
                 extra = [f"x={tmp}/x_in.f64"]
             if c == "cg":
                 extra = [f"f={tmp}/f_in.f64", "eps=1e-20"]
@@ -135,7 +137,7 @@ def add_commands(name, d, gridargs, coef, cmds, refsrc):
         for c in cmds:
             run([exe, c, tmp] + args + [f"x={tmp}/x_in.f64"])
             meta, arrs = read_meta(os.path.join(tmp, f"meta_{c}.txt"))
-            z.update(load_arrays(tmp, [a for a in arrs if a.startswith("y.")], c + "_"))
+            z.update(load_arrays(tmp, [a for a in arrs if a.startswith("y.") or a.startswith("diag.")], c + "_"))
     np.savez_compressed(path, **z)
     print(f"{name}: added {cmds}")
 

@@ -139,3 +139,65 @@ def test_solve_to_relative_residual(precision, tol):
     o = oracle.OracleGrid(g.points, g.active)
     r = f - o.matvec(lsg.COEF_SINPROD, [1.0, 0.5, 1, 1, 1], x)
     assert np.linalg.norm(r) / np.linalg.norm(f) <= tol * 1.05
+
+
+def test_mass_matches_reference(golden):
+    """Mass form (lsg_operator_set_form(LSG_FORM_MASS)): the midpoint plugin with
+    the Q1 mass matrix, and for a = 1 the reference's HelmHoltz stencil."""
+    if "mass_y" not in golden:
+        pytest.skip("no mass vector")
+    import torch
+    g = lsg.AdaptiveSparseGrid(golden["points"], golden["active"])
+    prob = lsg.MidpointMass(int(golden["coef_family"]), golden["coef_params"])
+    m = lsg.MatrixVectorHomogen(g, prob)
+    y = np.zeros(g.n)
+    m.multiplication(golden["x"], y, prob)
+    assert rel(y, golden["mass_y"]) < 1e-12
+    x32 = torch.tensor(golden["x"], dtype=torch.float32, device="cuda")
+    y32 = torch.zeros_like(x32)
+    m.multiplication_device(x32.data_ptr(), y32.data_ptr(), lsg.FP32)
+    torch.cuda.synchronize()
+    assert rel(y32.double().cpu().numpy(), golden["mass_y"]) < 2e-5
+    one = lsg.MidpointMass(lsg.COEF_CONST, [1.0])
+    y1 = np.zeros(g.n)
+    m.multiplication(golden["x"], y1, one)
+    assert rel(y1, golden["helmholtz_y"]) < 1e-12
+
+
+def test_mass_diag_matches_reference(golden):
+    if "massdiag_diag" not in golden:
+        pytest.skip("no mass diagonal")
+    g = lsg.AdaptiveSparseGrid(golden["points"], golden["active"])
+    prob = lsg.MidpointMass(int(golden["coef_family"]), golden["coef_params"])
+    m = lsg.MatrixVectorHomogen(g, prob)
+    assert rel(m.diagonal(prob), golden["massdiag_diag"]) < 1e-12
+
+
+def test_forms_switch_on_one_operator(golden):
+    """Switching the form back and forth recomputes the diagonal and reuses the tables."""
+    if "mass_y" not in golden or "diag_diag" not in golden:
+        pytest.skip("needs both forms")
+    g = lsg.AdaptiveSparseGrid(golden["points"], golden["active"])
+    fam, par = int(golden["coef_family"]), golden["coef_params"]
+    stiff, mass = lsg.MidpointDiffusion(fam, par), lsg.MidpointMass(fam, par)
+    m = lsg.MatrixVectorHomogen(g, stiff)
+    for prob, key in ((stiff, "matvec_y"), (mass, "mass_y"), (stiff, "matvec_y")):
+        y = np.zeros(g.n)
+        m.multiplication(golden["x"], y, prob)
+        assert rel(y, golden[key]) < 1e-12
+    assert rel(m.diagonal(stiff), golden["diag_diag"]) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [lsg.FP64, lsg.FP32])
+def test_mass_solve_l2_projection(precision):
+    """CG on the prewavelet mass matrix (an L2 projection) to relative residual 1e-10."""
+    g = lsg.AdaptiveSparseGrid.adaptive(3, 4, 2, 0.6, "corner")
+    prob = lsg.MidpointMass(lsg.COEF_SINPROD, [1.0, 0.5, 1.0, 1.0, 1.0])
+    m = lsg.MatrixVectorHomogen(g, prob)
+    f = np.random.default_rng(3).uniform(-1, 1, g.n) * g.active
+    x = np.zeros(g.n)
+    rep = lsg.CG.solveHomogen(1e-10, x, f, m, prob, criterion=1, precision=precision)
+    assert rep["converged"] == 1 and rep["rel_residual"] <= 1e-10
+    og = oracle.OracleGrid(g.points, g.active)
+    r = f - og.matvec(prob.family, prob.params[:prob.nparams], x, form=1) * g.active
+    assert np.linalg.norm(r) <= 2e-10 * np.linalg.norm(f)

@@ -59,3 +59,23 @@ def test_cg_matches_reference(golden):
     # recursive residual, so the last iteration or two depend on rounding
     assert abs(it - int(golden["cg_meta_iterations"])) <= 2
     assert rel(x, golden["cg_x"]) < 1e-9
+
+
+def test_mass_matches_reference(golden):
+    """The midpoint plugin with the Q1 mass matrix (LocalStiffnessMatrices path
+    of the reference) and, for a = 1, the reference's own HelmHoltz stencil."""
+    if "mass_y" not in golden:
+        return
+    g = oracle.OracleGrid(golden["points"], golden["active"])
+    y = g.matvec(int(golden["coef_family"]), golden["coef_params"], golden["x"], form=1)
+    assert rel(y, golden["mass_y"]) < 1e-13
+    y1 = g.matvec(0, [1.0], golden["x"], form=1)
+    assert rel(y1, golden["helmholtz_y"]) < 1e-13
+
+
+def test_mass_diag_matches_reference(golden):
+    if "massdiag_diag" not in golden:
+        return
+    g = oracle.OracleGrid(golden["points"], golden["active"])
+    dg = g.diag(int(golden["coef_family"]), golden["coef_params"], form=1)
+    assert rel(dg, golden["massdiag_diag"]) < 1e-13
