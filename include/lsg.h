@@ -193,6 +193,13 @@ int lsg_calc_nodal_by_prew(lsg_operator *op, const double *prew, double *u);
 int lsg_calc_prew_by_nodal(lsg_operator *op, double *prew, const double *u);
 int lsg_calc_nodal_by_prew_device(lsg_operator *op, const double *prew, double *u, void *stream);
 int lsg_calc_prew_by_nodal_device(lsg_operator *op, double *prew, const double *u, void *stream);
+/* H1 seminorm and L2 norm of the function with nodal values u (n doubles,
+ * host): H1::getValue / L2::getValue (applications/H1_Norm.cpp): prewavelet
+ * coefficients v = calcPrewByNodal(u), value = sqrt(sum over active points of
+ * v_i (A v)_i) with A the coefficient-1 stiffness (Poisson) or mass
+ * (HelmHoltz) operator; the operator's own coefficient and form stay set. */
+int lsg_h1_norm(lsg_operator *op, const double *u, double *value);
+int lsg_l2_norm(lsg_operator *op, const double *u, double *value);
 
 /* ---- launch parameters of the matvec and the autotuner that picks them.
  * The defaults suit large d=5/6 grids; lsg_operator_autotune times matvecs of

@@ -125,6 +125,8 @@ def lib():
             "lsg_grid_regular": (ctypes.c_int, [I32, I32, P, I64, P]),
             "lsg_grid_adaptive": (ctypes.c_int, [I32, I32, I32, D, I32, I32, P, P, I64, P]),
             "lsg_operator_set_form": (ctypes.c_int, [P, I32]),
+            "lsg_h1_norm": (ctypes.c_int, [P, P, P]),
+            "lsg_l2_norm": (ctypes.c_int, [P, P, P]),
             "lsg_calc_nodal_by_prew": (ctypes.c_int, [P, P, P]),
             "lsg_calc_prew_by_nodal": (ctypes.c_int, [P, P, P]),
             "lsg_calc_nodal_by_prew_device": (ctypes.c_int, [P, P, P, P]),
@@ -448,6 +450,32 @@ def calcNodalByPrew_device(prew_ptr, u_ptr, matrix, stream=0):
 def calcPrewByNodal_device(prew_ptr, u_ptr, matrix, stream=0):
     _check(lib().lsg_calc_prew_by_nodal_device(matrix._h, ctypes.c_void_p(prew_ptr), ctypes.c_void_p(u_ptr),
                                                ctypes.c_void_p(stream)))
+
+
+class H1:
+    """H1::getValue (applications/H1_Norm.cpp): the H1 seminorm of the function
+    with nodal values u.  The reference takes (grid, mgrid); here the
+    MatrixVectorHomogen of the grid (any coefficient: the norm uses a = 1)."""
+
+    def __init__(self, matrix):
+        self.matrix = matrix
+
+    def getValue(self, u):
+        u = np.ascontiguousarray(u, np.float64)
+        out = np.zeros(1)
+        _check(lib().lsg_h1_norm(self.matrix._h, _ptr(u), _ptr(out)))
+        return float(out[0])
+
+
+class L2(H1):
+    """L2::getValue (applications/H1_Norm.cpp): the L2 norm of the function with
+    nodal values u (mass form, the reference's HelmHoltz with a = 1)."""
+
+    def getValue(self, u):
+        u = np.ascontiguousarray(u, np.float64)
+        out = np.zeros(1)
+        _check(lib().lsg_l2_norm(self.matrix._h, _ptr(u), _ptr(out)))
+        return float(out[0])
 
 
 # --------------------------------------------------------------------------- batches

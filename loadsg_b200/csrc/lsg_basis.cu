@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <memory>
 #include <string>
 #include <vector>
@@ -325,6 +326,56 @@ int prew_by_nodal(lsg_operator* op, double* prew, const double* u, cudaStream_t 
     return 0;
 }
 
+// partial sums of a[i] b[i] over active points, one per CTA (summed on the host in order)
+__global__ void k_dot_active(int64_t n, const uint8_t* __restrict__ act, const double* __restrict__ a,
+                             const double* __restrict__ b, double* __restrict__ part) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (act[i]) acc += a[i] * b[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) part[blockIdx.x] = acc;
+    }
+}
+
+// H1::getValue / L2::getValue (applications/H1_Norm.cpp): v = calcPrewByNodal(u),
+// sqrt(sum over active points of v (A v)) with A the coefficient-1 stiffness
+// (Poisson) or mass (HelmHoltz) operator
+int norm_value(lsg_operator* op, const double* u_host, int form, double* value) {
+    if (!op || !u_host || !value) return fail_msg(LSG_E_INVALID, "null argument");
+    BasisState* Sp = nullptr;
+    int rc = ensure_basis(op, &Sp);
+    if (rc) return rc;
+    const int64_t n = Sp->n;
+    constexpr int kParts = 592;
+    double *u = nullptr, *v = nullptr, *Av = nullptr, *part = nullptr;
+    BS_TRY(cudaMalloc(&u, n * 8 * 3 + kParts * 8));
+    v = u + n;
+    Av = v + n;
+    part = Av + n;
+    std::vector<double> hp(kParts);
+    if (cudaMemcpy(u, u_host, n * 8, cudaMemcpyHostToDevice) != cudaSuccess) rc = fail_msg(LSG_E_CUDA, "cudaMemcpy");
+    if (!rc) rc = prew_by_nodal(op, v, u, 0);
+    if (!rc && cudaMemset(Av, 0, n * 8) != cudaSuccess) rc = fail_msg(LSG_E_CUDA, "cudaMemset");
+    if (!rc) rc = lsg_internal::matvec64_unit(op, form, v, Av, 0);
+    if (!rc) {
+        k_dot_active<<<kParts, 256>>>(n, Sp->act.as<uint8_t>(), v, Av, part);
+        if (cudaMemcpy(hp.data(), part, kParts * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = fail_msg(LSG_E_CUDA, "cudaMemcpy");
+    }
+    cudaFree(u);
+    if (rc) return rc;
+    double sum = 0.0;
+    for (double x : hp) sum += x;
+    *value = std::sqrt(sum);
+    return 0;
+}
+
 int host_call(lsg_operator* op, const double* in, double* out, bool to_nodal) {
     if (!op || !in || !out) return fail_msg(LSG_E_INVALID, "null argument");
     const int64_t n = lsg_internal::plan(op).n;
@@ -356,5 +407,9 @@ int lsg_calc_prew_by_nodal_device(lsg_operator* op, double* prew, const double* 
 int lsg_calc_nodal_by_prew(lsg_operator* op, const double* prew, double* u) { return host_call(op, prew, u, true); }
 
 int lsg_calc_prew_by_nodal(lsg_operator* op, double* prew, const double* u) { return host_call(op, u, prew, false); }
+
+int lsg_h1_norm(lsg_operator* op, const double* u, double* value) { return norm_value(op, u, 0, value); }
+
+int lsg_l2_norm(lsg_operator* op, const double* u, double* value) { return norm_value(op, u, 1, value); }
 
 }  // extern "C"

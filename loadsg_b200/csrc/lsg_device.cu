@@ -975,6 +975,7 @@ struct lsg_operator {
         conv_stage, conv_src, conv_code, conv_dom, prol, restr, a_items, b_items, b_steps, pts, cell_slab_off;
     DBuf lam64, lam32;   // Hadamard-basis eigenvalues of the Q1 stiffness (form 0)
     DBuf mu64, mu32;     // ... of the Q1 mass (form 1)
+    DBuf one64, one32;   // unit coefficient per cell (constant-coefficient norms)
     int32_t form = 0;
     // coefficient (one family and parameter set per part of a concatenated plan)
     bool have_coef = false;
@@ -1315,6 +1316,11 @@ static int lsg_internal_matvec32(lsg_operator* op, const float* x, float* y, cud
 static const uint8_t* lsg_internal_active(lsg_operator* op);
 
 // ============================================================================= C-ABI
+__global__ void k_fill_one(int64_t n, double* a64, float* a32) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) { a64[i] = 1.0; a32[i] = 1.0f; }
+}
+
 namespace lsg_internal {
 
 int create_from_plan(lsg::Plan&& plan, lsg_operator** out) {
@@ -1385,6 +1391,28 @@ int64_t matvec_launch_count(const lsg_operator* op) {
            (int64_t)(p.b_level_off.size() - 1);
 }
 int fail_msg(int code, const char* msg) { return fail(code, msg); }
+
+// y = A x with coefficient 1 in the given form (Poisson / HelmHoltz of the
+// norms), leaving the operator's own coefficient and form in place
+int matvec64_unit(lsg_operator* op, int form, const double* x, double* y, cudaStream_t st) {
+    const int64_t C = std::max<int64_t>(op->plan.C, 1);
+    if (!op->one64.p) {
+        if (op->one64.alloc(C * sizeof(double), &op->dev_bytes) || op->one32.alloc(C * sizeof(float), &op->dev_bytes))
+            return LSG_E_CUDA;
+        k_fill_one<<<nblk(C), 256, 0, st>>>(C, op->one64.as<double>(), op->one32.as<float>());
+    }
+    int rc = prepare<double>(op);
+    if (rc) return rc;
+    std::swap(op->acell64.p, op->one64.p);
+    std::swap(op->acell32.p, op->one32.p);
+    const int32_t f0 = op->form;
+    op->form = form;
+    rc = matvec_dispatch<double>(op, x, y, st);
+    op->form = f0;
+    std::swap(op->acell64.p, op->one64.p);
+    std::swap(op->acell32.p, op->one32.p);
+    return rc;
+}
 std::shared_ptr<void>& basis_slot(lsg_operator* op) { return op->basis; }
 int autotune(lsg_operator* op, int32_t precision, int32_t reps) {
     return lsg_operator_autotune(op, precision, reps, nullptr, nullptr, nullptr);

@@ -29,6 +29,8 @@ size_t device_bytes(const lsg_operator* op);
 int64_t matvec_launch_count(const lsg_operator* op);
 int fail_msg(int code, const char* msg);
 int autotune(lsg_operator* op, int32_t precision, int32_t reps);
+// y = A x with coefficient 1 in form 0 (stiffness) or 1 (mass), FP64
+int matvec64_unit(lsg_operator* op, int form, const double* x, double* y, cudaStream_t st);
 // per-operator state of the basis transforms (lsg_basis.cu)
 std::shared_ptr<void>& basis_slot(lsg_operator* op);
 

@@ -134,6 +134,15 @@ class OracleGrid:
         p[act] = np.linalg.solve(A[act], np.asarray(u, np.float64)[act])
         return p
 
+    def norm(self, u, h1=True):
+        """H1::getValue / L2::getValue (applications/H1_Norm.cpp): v = the exact
+        inverse of calcNodalByPrew applied to u, sqrt(v . A v) over active points
+        with the coefficient-1 stiffness (H1) or mass (L2) matrix; small grids."""
+        v = self.prew_by_nodal(u)
+        Av = self.matvec(0, [1.0], v, form=0 if h1 else 1)
+        act = np.asarray(self.active) > 0
+        return float(np.sqrt(np.sum(v[act] * Av[act])))
+
     def cg(self, family, params, f, eps, maxit=500, x0=None):
         lib().lsgo_set_form(self._h, 0)
         f = np.ascontiguousarray(f, np.float64)

@@ -276,6 +276,23 @@ int main(int argc, char **argv) {
         dump_grid(grid);
     } else if (cmd == "tables") {
         dump_tables(grid);
+    } else if (cmd == "h1norm" || cmd == "l2norm") {
+        // H1::getValue / L2::getValue (applications/H1_Norm.cpp) of the nodal values x
+        std::vector<double> x = read_f64(opt("x", ""), N);
+        MultiLevelAdaptiveSparseGrid mgrid(&grid);
+        VectorSparseG uv(grid);
+        set_vec(uv, x);
+        double val;
+        if (cmd == "h1norm") {
+            H1 norm(grid, mgrid);
+            val = norm.getValue(uv);
+        } else {
+            L2 norm(grid, mgrid);
+            val = norm.getValue(uv);
+        }
+        char buf[64];
+        snprintf(buf, sizeof buf, "%.17g", val);
+        g_meta << "value " << buf << "\n";
     } else if (cmd == "mass" || cmd == "helmholtz") {
         // mass: the midpoint plugin with the Q1 mass matrix; helmholtz: the
         // reference's own HelmHoltz stencil (Stencil.h:873-919, coefficient 1)

@@ -13,7 +13,8 @@ reference.
 prew2nodal / nodal2prew run calcNodalByPrew / calcPrewByNodal on the fixture's
 x (BasisTransformations/BasisTransformations.cpp:486-545,670-706); mass /
 massdiag use the midpoint plugin with the Q1 mass matrix, helmholtz the
-reference's own HelmHoltz stencil (stencils/Stencil.h:873-919).
+reference's own HelmHoltz stencil (stencils/Stencil.h:873-919); h1norm /
+l2norm are H1::getValue / L2::getValue (applications/H1_Norm.cpp) of x.
 """
 import argparse
 import os
@@ -101,7 +102,7 @@ def make_case(name, d, gridargs, coef, cmds, refsrc):
         out["f"] = f
         for c in cmds:
             extra = []
-            if c in ("matvec", "poisson", "prew2nodal", "nodal2prew", "mass", "helmholtz"):
+            if c in ("matvec", "poisson", "prew2nodal", "nodal2prew", "mass", "helmholtz", "h1norm", "l2norm"):
                 extra = [f"x={tmp}/x_in.f64"]
             if c == "cg":
                 extra = [f"f={tmp}/f_in.f64", "eps=1e-20"]
@@ -138,6 +139,12 @@ def add_commands(name, d, gridargs, coef, cmds, refsrc):
             run([exe, c, tmp] + args + [f"x={tmp}/x_in.f64"])
             meta, arrs = read_meta(os.path.join(tmp, f"meta_{c}.txt"))
             z.update(load_arrays(tmp, [a for a in arrs if a.startswith("y.") or a.startswith("diag.")], c + "_"))
+            for k, v in meta.items():
+                if k != "ok":
+                    try:
+                        z[f"{c}_meta_{k}"] = np.float64(float(v))
+                    except ValueError:
+                        pass
     np.savez_compressed(path, **z)
     print(f"{name}: added {cmds}")
 

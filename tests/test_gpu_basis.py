@@ -73,3 +73,18 @@ def test_device_entry_points_match_host():
     lsg.calcPrewByNodal_device(qd.data_ptr(), ud.data_ptr(), m)
     torch.cuda.synchronize()
     assert rel(qd.cpu().numpy(), q_h) < 1e-13
+
+
+def test_norms_match_reference(golden):
+    """lsg_h1_norm / lsg_l2_norm (H1::getValue, L2::getValue of applications/H1_Norm.cpp)."""
+    if "h1norm_meta_value" not in golden:
+        pytest.skip("no norms")
+    g = lsg.AdaptiveSparseGrid(golden["points"], golden["active"])
+    m = lsg.MatrixVectorHomogen(g, lsg.MidpointDiffusion(int(golden["coef_family"]), golden["coef_params"]))
+    for cls, key in ((lsg.H1, "h1norm_meta_value"), (lsg.L2, "l2norm_meta_value")):
+        ref = float(golden[key])
+        assert abs(cls(m).getValue(golden["x"]) - ref) <= 1e-12 * ref
+    # the operator's own coefficient and form are left in place
+    y = np.zeros(g.n)
+    m.multiplication(golden["x"], y, m._problem)
+    assert rel(y, golden["matvec_y"]) < 1e-12

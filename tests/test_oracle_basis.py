@@ -20,3 +20,13 @@ def test_prew_by_nodal_is_the_exact_inverse(golden):
     ref = golden["nodal2prew_y"]
     assert np.abs(p - ref).max() <= 1e-13 * np.abs(ref).max()
     assert not np.any(ref[golden["active"] == 0])
+
+
+def test_norms_match_reference(golden):
+    """H1::getValue / L2::getValue of the fixture's x read as nodal values."""
+    if "h1norm_meta_value" not in golden:
+        return
+    g = oracle.OracleGrid(golden["points"], golden["active"])
+    for key, h1 in (("h1norm_meta_value", True), ("l2norm_meta_value", False)):
+        ref = float(golden[key])
+        assert abs(g.norm(golden["x"], h1) - ref) <= 1e-12 * ref
