@@ -8,6 +8,11 @@
  *
  * Each entry point names the reference interface it replaces (paths relative
  * to LoAdSG's library/source/).
+ *
+ * An operator (or batch) keeps work buffers, its coefficient and its form in
+ * its own state, so calls on one operator must come from one host thread at
+ * a time (like the reference's MatrixVectorHomogen); different operators are
+ * independent.
  */
 #ifndef LSG_H
 #define LSG_H

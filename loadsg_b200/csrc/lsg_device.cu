@@ -976,6 +976,7 @@ struct lsg_operator {
     DBuf lam64, lam32;   // Hadamard-basis eigenvalues of the Q1 stiffness (form 0)
     DBuf mu64, mu32;     // ... of the Q1 mass (form 1)
     DBuf one64, one32;   // unit coefficient per cell (constant-coefficient norms)
+    bool unit_coef = false;  // matvec with coefficient 1 (set only inside matvec64_unit)
     int32_t form = 0;
     // coefficient (one family and parameter set per part of a concatenated plan)
     bool have_coef = false;
@@ -1161,6 +1162,13 @@ int upload_plan(lsg_operator* op) {
     return build_cell_classes(op);
 }
 
+// per-cell coefficient the cell operator multiplies by
+template <typename V>
+const V* cell_coef(const lsg_operator* op) {
+    if (std::is_same<V, double>::value) return (const V*)(op->unit_coef ? op->one64.p : op->acell64.p);
+    return (const V*)(op->unit_coef ? op->one32.p : op->acell32.p);
+}
+
 template <typename V>
 int ensure_work(lsg_operator* op, lsg_operator::Work& w) {
     if (w.ml.p) return 0;
@@ -1222,7 +1230,7 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t
     if (rc) return rc;
     rc = set_phaseB_smem<D, V>();
     if (rc) return rc;
-    const V* acell = std::is_same<V, double>::value ? (const V*)op->acell64.p : (const V*)op->acell32.p;
+    const V* acell = cell_coef<V>(op);
     const V* lam = std::is_same<V, double>::value ? (const V*)(op->form ? op->mu64.p : op->lam64.p)
                                                   : (const V*)(op->form ? op->mu32.p : op->lam32.p);
     int64_t na = p.exa_off[p.nD];
@@ -1403,14 +1411,12 @@ int matvec64_unit(lsg_operator* op, int form, const double* x, double* y, cudaSt
     }
     int rc = prepare<double>(op);
     if (rc) return rc;
-    std::swap(op->acell64.p, op->one64.p);
-    std::swap(op->acell32.p, op->one32.p);
     const int32_t f0 = op->form;
     op->form = form;
+    op->unit_coef = true;
     rc = matvec_dispatch<double>(op, x, y, st);
+    op->unit_coef = false;
     op->form = f0;
-    std::swap(op->acell64.p, op->one64.p);
-    std::swap(op->acell32.p, op->one32.p);
     return rc;
 }
 std::shared_ptr<void>& basis_slot(lsg_operator* op) { return op->basis; }
@@ -2311,7 +2317,7 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
     V* nscratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm + b_sc);
     int rc = set_phaseB_smem<D, V>();
     if (rc) return rc;
-    const V* acell = std::is_same<V, double>::value ? (const V*)op->acell64.p : (const V*)op->acell32.p;
+    const V* acell = cell_coef<V>(op);
     const V* lam = std::is_same<V, double>::value ? (const V*)(op->form ? op->mu64.p : op->lam64.p)
                                                   : (const V*)(op->form ? op->mu32.p : op->lam32.p);
     // Every region is written before it is read within one call (nodal slabs by
