@@ -757,13 +757,15 @@ __global__ void k_diag(DevPlan P, const double* __restrict__ acell, double* __re
 
 
 // ----------------------------------------------------------------------------- learned diagonal
-// Features of point k for the diagonal MLP (F = 5d + 2): depths t_j / 8,
-// coordinates x_j, next-to-boundary flags, log a(x), sum_j t_j / (8 d), and the
-// log-coefficient differences log a(x +- h_j e_j) - log a(x), h_j = 2^-t_j.
-__global__ void k_features(DevPlan P, int family, const double* __restrict__ params, float* __restrict__ feat) {
+// Features of point k for the diagonal MLP (F = 7d + 2): depths t_j / 8,
+// coordinates x_j, next-to-boundary flags, log a(x), sum_j t_j / (8 d), the
+// log-coefficient differences log a(x +- h_j e_j) - log a(x), h_j = 2^-t_j, and
+// whether the same-depth points two level steps left / right exist (nbmask).
+__global__ void k_features(DevPlan P, int family, const double* __restrict__ params, const uint16_t* __restrict__ nbmask,
+                           float* __restrict__ feat) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= P.n) return;
-    int d = P.d, F = 5 * d + 2;
+    int d = P.d, F = 7 * d + 2;
     float* f = feat + k * F;
     double x[lsg::kMaxDim], h[lsg::kMaxDim];
     int tsum = 0;
@@ -790,6 +792,8 @@ __global__ void k_features(DevPlan P, int family, const double* __restrict__ par
         f[3 * d + 3 + 2 * j] = (float)(log(fmax(lsg_coef_eval_dev(family, params, d, x), 1e-300)) - la);
         x[j] = xs;
     }
+    const uint16_t m = nbmask[k];
+    for (int j = 0; j < 2 * d; ++j) f[5 * d + 2 + j] = ((m >> j) & 1) ? 1.f : 0.f;
 }
 
 // Cheap diagonal a(x_k) * psi_k^T K_ref psi_k for a constant coefficient on a
@@ -984,6 +988,7 @@ struct lsg_operator {
     std::vector<uint8_t> part_coef;
     DBuf acell64, acell32, params;
     DBuf feat, mlp_out, base;  // learned-diagonal work buffers
+    DBuf nbmask;               // same-depth neighbour flags (features)
     // work buffers per precision
     struct Work {
         DBuf ml, pc, zb, gm, scratch, nscratch;
@@ -2379,7 +2384,12 @@ extern "C" int lsg_mlp_forward(lsg_mlp* m, const float* X, int64_t rows, float* 
 extern "C" int lsg_operator_features(lsg_operator* op, float* feat, void* stream) {
     if (!op || !feat) return fail(LSG_E_INVALID, "null argument");
     if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
-    k_features<<<nblk(op->plan.n, 128), 128, 0, (cudaStream_t)stream>>>(op->dp, op->family, op->params.as<double>(), feat);
+    if (!op->nbmask.p) {  // same-depth neighbour flags, built on first use
+        std::vector<uint16_t> m = lsg::same_depth_neighbor_mask(op->plan);
+        if (op->nbmask.upload(m, &op->dev_bytes)) return LSG_E_CUDA;
+    }
+    k_features<<<nblk(op->plan.n, 128), 128, 0, (cudaStream_t)stream>>>(op->dp, op->family, op->params.as<double>(),
+                                                                        op->nbmask.as<uint16_t>(), feat);
     CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -2396,7 +2406,7 @@ extern "C" int lsg_operator_install_learned(lsg_operator* op, lsg_mlp* m, void* 
     if (!op || !m) return fail(LSG_E_INVALID, "null argument");
     if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
     int64_t n = op->plan.n;
-    int F = 5 * op->plan.d + 2;
+    int F = 7 * op->plan.d + 2;
     size_t* tot = &op->dev_bytes;
     int rc = 0;
     if (!op->feat.p) rc |= op->feat.alloc((size_t)n * F * sizeof(float), tot);

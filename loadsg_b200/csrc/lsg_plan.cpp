@@ -917,6 +917,28 @@ void band_lr(int n, std::vector<double>& R, std::vector<double>& L) {
 
 }  // namespace
 
+std::vector<uint16_t> same_depth_neighbor_mask(const Plan& p) {
+    const int d = p.d;
+    std::vector<uint16_t> mask(p.n, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < p.n; ++k) {
+        const int t = p.did[k];
+        const Slab& sl = p.slabs[t];
+        Geometry g(d, sl.T);
+        int64_t c[kMaxDim];
+        for (int j = 0; j < d; ++j) c[j] = coord_at(p.pts[k * d + j], sl.T[j]);
+        uint16_t m = 0;
+        for (int j = 0; j < d; ++j) {
+            const int64_t cj = c[j];
+            if (cj - 2 >= 1) { c[j] = cj - 2; if (slab_pos(p, t, g, c) >= 0) m |= (uint16_t)(1u << (2 * j)); }
+            if (cj + 2 < g.cext[j]) { c[j] = cj + 2; if (slab_pos(p, t, g, c) >= 0) m |= (uint16_t)(1u << (2 * j + 1)); }
+            c[j] = cj;
+        }
+        mask[k] = m;
+    }
+    return mask;
+}
+
 bool build_basis_plan(const Plan& p, BasisPlan& b, std::string& error) {
     auto t0 = std::chrono::steady_clock::now();
     const int d = p.d, nD = p.nD;

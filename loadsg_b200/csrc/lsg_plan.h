@@ -164,6 +164,11 @@ struct BasisPlan {
 
 bool build_basis_plan(const Plan& p, BasisPlan& b, std::string& error);
 
+// Per point, bit 2j / 2j+1: the point of the same depth two level-T steps to the
+// left / right in dim j exists (a feature of the learned diagonal: where it is
+// missing, part of the prewavelet's support has no cells).
+std::vector<uint16_t> same_depth_neighbor_mask(const Plan& p);
+
 // Builds the plan; returns false and sets plan.error on invalid input.
 bool build_plan(int d, int64_t n, const int32_t* points, const uint8_t* active, Plan& plan);
 

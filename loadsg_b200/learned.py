@@ -1,7 +1,8 @@
 """Learned diagonal preconditioner: data, training and use.
 
 A point's features (depth multi-index, coordinates, next-to-boundary flags,
-local log-coefficient samples; computed on the GPU) go through a 3x64 MLP
+local log-coefficient samples, whether its same-depth neighbours exist;
+computed on the GPU) go through a 3x64 MLP
 whose softplus output scales a cheap constant-coefficient diagonal:
 D = base * softplus(mlp(features)).  The network is trained on the GPU
 (loadsg_b200/csrc/lsg_mlp.cu: forward, backward and Adam kernels) to match the
@@ -29,7 +30,7 @@ H = 64
 
 
 def n_features(d):
-    return 5 * d + 2
+    return 7 * d + 2
 
 
 def n_params(F):
