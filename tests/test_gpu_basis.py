@@ -21,6 +21,8 @@ def mat(g):
 
 
 def test_nodal_by_prew_matches_reference(golden):
+    if "prew2nodal_y" not in golden:
+        pytest.skip("no transform vectors")
     g = lsg.AdaptiveSparseGrid(golden["points"], golden["active"])
     u = np.zeros(g.n)
     lsg.calcNodalByPrew(golden["x"], u, mat(g))
@@ -28,6 +30,8 @@ def test_nodal_by_prew_matches_reference(golden):
 
 
 def test_prew_by_nodal_matches_reference(golden):
+    if "nodal2prew_y" not in golden:
+        pytest.skip("no transform vectors")
     g = lsg.AdaptiveSparseGrid(golden["points"], golden["active"])
     p = np.zeros(g.n)
     x = golden["x"].copy()
