@@ -225,11 +225,6 @@ __global__ void kb_dot2(const Chunk* __restrict__ ch, const V* __restrict__ r, c
     }
 }
 
-__global__ void kb_fill(int count, double* __restrict__ v, double val) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) v[i] = val;
-}
-
 // stop thresholds: eps^2 * ff for the relative-residual criterion
 __global__ void kb_stop(int count, Scal s, const double* __restrict__ ff, double eps2) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -237,15 +232,23 @@ __global__ void kb_stop(int count, Scal s, const double* __restrict__ ff, double
 }
 
 // IR: outer convergence on the FP64 residual, per-grid scale 1/||r|| (0 when done)
+// the inner stop for grids still refining: reduce by itol, or only by 0.1 x the
+// factor still missing to the target when that is looser (the last step of a
+// refinement needs little)
 __global__ void kb_outer(int count, Scal s, const double* __restrict__ rr64, const double* __restrict__ ff, double eps2,
-                         int32_t* __restrict__ outer_conv, int32_t* __restrict__ outer_its) {
+                         double itol, int32_t* __restrict__ outer_conv, int32_t* __restrict__ outer_its) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     double rr = rr64[i];
     bool done = outer_conv[i] || rr <= eps2 * ff[i] || !isfinite(rr);
     if (!isfinite(rr)) s.bad[i] = 1;
     if (done) { outer_conv[i] = 1; s.scale[i] = 0.0; }
-    else { s.scale[i] = 1.0 / sqrt(rr); outer_its[i] += 1; }
+    else {
+        s.scale[i] = 1.0 / sqrt(rr);
+        outer_its[i] += 1;
+        double t = fmax(itol, fmin(0.5, 0.1 * sqrt(eps2 * ff[i] / rr)));
+        s.stop[i] = t * t;
+    }
     s.conv[i] = done ? 1 : 0;  // inner CG runs only on grids still refining
     if (!done) atomicAdd(s.pending, 1);
 }
@@ -541,7 +544,7 @@ int batch_solve(lsg_batch* b, const double* f, double* x, const lsg_solver_opts*
             S.dot<double, double>(r, r, S.rr64.as<double>(), st);
             BT_TRY(cudaMemsetAsync(S.S.pending, 0, 4, st));
             kb_outer<<<nb(count), kThreads, 0, st>>>(count, S.S, S.rr64.as<double>(), S.ff.as<double>(), eps * eps,
-                                                     S.outer_conv.as<int32_t>(), S.outer_its.as<int32_t>());
+                                                     itol, S.outer_conv.as<int32_t>(), S.outer_its.as<int32_t>());
             BT_TRY(cudaMemcpyAsync(S.pend_h, S.S.pending, 4, cudaMemcpyDeviceToHost, st));
             BT_TRY(cudaStreamSynchronize(st));
             launches += batch_matvec_launches(b) + 6;
@@ -549,11 +552,10 @@ int batch_solve(lsg_batch* b, const double* f, double* x, const lsg_solver_opts*
             ++outer_rounds;
             kb_scale_f32<<<b->nchunks, kThreads, 0, st>>>(S.ch(), S.S.scale, r, S.r32.as<float>());
             BT_TRY(cudaMemsetAsync(S.e32.p, 0, n * 4, st));
-            kb_fill<<<nb(count), kThreads, 0, st>>>(count, S.S.stop, itol * itol);
             rc = S.start<float>(S.r32.as<float>(), S.d32.as<float>(), S.h32.as<float>(), z32, 1, itol, st);
             if (rc) break;
             int ran = 0;
-            S.stall = 100;
+            S.stall = 400;  // long: PCG residual 2-norms are not monotone
             rc = S.loop<float>(S.e32.as<float>(), S.r32.as<float>(), S.g32.as<float>(), S.d32.as<float>(),
                                S.h32.as<float>(), z32, 1, itol, inner, graph, st, &ran, &launches);
             S.stall = 0;

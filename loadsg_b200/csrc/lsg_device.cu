@@ -1798,6 +1798,8 @@ struct Solver {
     Pinned pin;
 };
 
+constexpr int kInnerStallWindow = 400;  // iterations without a 10 % residual gain
+
 int solver_init(Solver& S, bool fp32) {
     int64_t n = S.n;
     size_t* t = &S.bytes;
@@ -1881,7 +1883,9 @@ int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int
     // stall_window > 0 (inner FP32 solves of the refinement): stop once the
     // recursive residual has not dropped below 0.9 x its best value for that
     // many iterations -- FP32 cannot reduce it further, the outer FP64
-    // residual takes over
+    // residual takes over.  The window is long because the 2-norm of a PCG
+    // residual is not monotone: it can sit above its best for a hundred
+    // iterations while the error still falls.
     double best = S.pin.h[5];
     int best_it = 0;
     for (int i = 1; i <= maxit; ++i) {
@@ -1914,12 +1918,14 @@ int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int
 }
 
 template <typename V>
-int cg_start(Solver& S, const V* f, V* x, V* r, V* d, V* h, const V* z, cudaStream_t st) {
+int cg_start(Solver& S, const V* f, V* x, V* r, V* d, V* h, const V* z, cudaStream_t st, bool x_zero = false) {
     int64_t n = S.n;
     double* s = S.s.as<double>();
     CUDA_TRY(cudaMemsetAsync(r, 0, n * sizeof(V), st));
-    int rc = std::is_same<V, double>::value ? lsg_internal_matvec64(S.op, (const double*)x, (double*)r, st)
-                                            : lsg_internal_matvec32(S.op, (const float*)x, (float*)r, st);
+    // A x of an all-zero x is exactly zero: skip the product
+    int rc = x_zero ? 0
+                    : std::is_same<V, double>::value ? lsg_internal_matvec64(S.op, (const double*)x, (double*)r, st)
+                                                     : lsg_internal_matvec32(S.op, (const float*)x, (float*)r, st);
     if (rc) return rc;
     k_sub<V><<<nblk(n), 256, 0, st>>>(n, f, r);
     CUDA_TRY(cudaMemsetAsync(h, 0, n * sizeof(V), st));
@@ -1973,6 +1979,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
     double eps = o->eps;
     cudaEventRecord(ev0, st);
     double ff = rc ? 0.0 : host_dot(S, f, f, st);
+    const bool x_zero = !rc && host_dot(S, x, x, st) == 0.0;  // zero initial guess (the common case)
     if (!rc && o->precision == LSG_FP64) {
         DBuf x0;  // initial guess, kept for the fallback of a learned diagonal
         if (!rc && o->precond == 2) {
@@ -1980,7 +1987,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             rc = x0.alloc(n * sizeof(double), &dummy);
             if (!rc) CUDA_TRY(cudaMemcpyAsync(x0.p, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
         }
-        if (!rc) rc = cg_start<double>(S, f, x, S.r.as<double>(), S.d.as<double>(), S.h.as<double>(), zdiag, st);
+        if (!rc) rc = cg_start<double>(S, f, x, S.r.as<double>(), S.d.as<double>(), S.h.as<double>(), zdiag, st, x_zero);
         int its = 0;
         double rr = 0.0;
         if (!rc)
@@ -2022,7 +2029,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
         int slow_steps = 0;
         for (outer = 0; outer < maxit && total < maxit; ++outer) {
             CUDA_TRY(cudaMemsetAsync(r, 0, n * 8, st));
-            rc = lsg_internal_matvec64(op, x, r, st);
+            rc = (outer == 0 && x_zero) ? 0 : lsg_internal_matvec64(op, x, r, st);
             if (rc) break;
             k_sub<double><<<nblk(n), 256, 0, st>>>(n, f, r);
             double rr = host_dot(S, r, r, st);
@@ -2037,9 +2044,10 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
                 k_to_f32<<<nblk(n), 256, 0, st>>>(n, op->diag.as<double>(), S.z32.as<float>());
                 z32 = S.z32.as<float>();
             }
-            // refinement that stopped making progress (with the exact diagonal): give up
+            // refinement that stopped making progress (six steps in a row that did not
+            // halve the residual): give up
             if (rr_prev > 0 && rr > 0.25 * rr_prev) {
-                if (++slow_steps >= 3) { rc = fail(LSG_E_NOCONV, "iterative refinement stagnated"); break; }
+                if (++slow_steps >= 6) { rc = fail(LSG_E_NOCONV, "iterative refinement stagnated"); break; }
             } else {
                 slow_steps = 0;
             }
@@ -2063,8 +2071,11 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, s + 5);
             int its = 0;
             double lrr = 0.0;
-            rc = cg_loop<float>(S, e32, r32, S.g32.as<float>(), d32, h32, z32, 0.0, 1, itol * itol, inner,
-                                o->use_graph != 0, st, &its, &lrr, &R.kernel_launches, 100);
+            // inner reduction: itol, or only 0.1 x the factor still missing to the
+            // target when that is looser (the last refinement step needs little)
+            const double istep = std::max(itol, std::min(0.5, 0.1 * std::sqrt(eps * eps * ff / rr)));
+            rc = cg_loop<float>(S, e32, r32, S.g32.as<float>(), d32, h32, z32, 0.0, 1, istep * istep, inner,
+                                o->use_graph != 0, st, &its, &lrr, &R.kernel_launches, kInnerStallWindow);
             R.kernel_launches += matvec_launches(op->plan) + 12;
             if (rc) break;
             total += its;
