@@ -1980,6 +1980,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
     cudaEventRecord(ev0, st);
     double ff = rc ? 0.0 : host_dot(S, f, f, st);
     const bool x_zero = !rc && host_dot(S, x, x, st) == 0.0;  // zero initial guess (the common case)
+    double final_rr = -1.0;  // FP64 residual of the final x when the refinement measured it
     if (!rc && o->precision == LSG_FP64) {
         DBuf x0;  // initial guess, kept for the fallback of a learned diagonal
         if (!rc && o->precond == 2) {
@@ -2034,7 +2035,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             k_sub<double><<<nblk(n), 256, 0, st>>>(n, f, r);
             double rr = host_dot(S, r, r, st);
             if (!std::isfinite(rr)) { rc = fail(LSG_E_NOCONV, "non-finite residual"); break; }
-            if (rr <= eps * eps * ff) break;
+            if (rr <= eps * eps * ff) { final_rr = rr; break; }  // x is final: this is its residual
             // a refinement step that did not halve the residual with the learned
             // diagonal: switch to the exact Jacobi diagonal
             if (o->precond == 2 && !R.fell_back && rr_prev > 0 && rr > 0.25 * rr_prev) {
@@ -2100,15 +2101,19 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
     }
     cudaEventRecord(ev1, st);
     if (!rc) {
-        // true relative residual in FP64
-        double* r = S.r.as<double>();
-        cudaMemsetAsync(r, 0, n * 8, st);
-        rc = lsg_internal_matvec64(op, x, r, st);
-        if (!rc) {
-            k_sub<double><<<nblk(n), 256, 0, st>>>(n, f, r);
-            double rr = host_dot(S, r, r, st);
-            R.rel_residual = ff > 0 ? std::sqrt(rr / ff) : std::sqrt(rr);
+        // true relative residual in FP64 (the refinement's last residual when it
+        // was taken of the final x)
+        double rr = final_rr;
+        if (rr < 0.0) {
+            double* r = S.r.as<double>();
+            cudaMemsetAsync(r, 0, n * 8, st);
+            rc = lsg_internal_matvec64(op, x, r, st);
+            if (!rc) {
+                k_sub<double><<<nblk(n), 256, 0, st>>>(n, f, r);
+                rr = host_dot(S, r, r, st);
+            }
         }
+        if (!rc) R.rel_residual = ff > 0 ? std::sqrt(rr / ff) : std::sqrt(rr);
     }
     cudaStreamSynchronize(st);
     float ms = 0.f;

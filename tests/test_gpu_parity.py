@@ -201,3 +201,38 @@ def test_mass_solve_l2_projection(precision):
     og = oracle.OracleGrid(g.points, g.active)
     r = f - og.matvec(prob.family, prob.params[:prob.nparams], x, form=1) * g.active
     assert np.linalg.norm(r) <= 2e-10 * np.linalg.norm(f)
+
+
+EDGE_GRIDS = [("single point d=1", 1, 0, None), ("single point d=8", 8, 0, None), ("d=1 level 8", 1, 8, None),
+              ("d=1 adaptive", 1, 4, (3, 0.3, "corner")), ("d=7 level 2", 7, 2, None), ("d=8 level 1", 8, 1, None),
+              ("d=2 adaptive plane", 2, 3, (4, 0.2, "plane"))]
+
+
+@pytest.mark.parametrize("name,d,level,adapt", EDGE_GRIDS, ids=[e[0] for e in EDGE_GRIDS])
+def test_edge_grids_match_oracle(name, d, level, adapt):
+    """Extremes of the path: one-point grids, d = 1, d = 7 and 8, deep 1D
+    refinement: matvec (FP64 and FP32), diagonal and a Jacobi CG solve against
+    the oracle."""
+    import torch
+    g = lsg.AdaptiveSparseGrid.regular(d, level) if adapt is None else \
+        lsg.AdaptiveSparseGrid.adaptive(d, level, *adapt)
+    params = [1.0, 0.5] + [1.0] * d
+    prob = lsg.MidpointDiffusion(lsg.COEF_SINPROD, params)
+    m = lsg.MatrixVectorHomogen(g, prob)
+    o = oracle.OracleGrid(g.points, g.active)
+    rng = np.random.default_rng(d + 10 * level)
+    x = rng.uniform(-1, 1, g.n)
+    y = np.zeros(g.n)
+    m.multiplication(x, y, prob)
+    yo = o.matvec(lsg.COEF_SINPROD, params, x)
+    assert rel(y, yo) < 1e-12
+    x32 = torch.tensor(x, dtype=torch.float32, device="cuda")
+    y32 = torch.zeros_like(x32)
+    m.multiplication_device(x32.data_ptr(), y32.data_ptr(), lsg.FP32)
+    torch.cuda.synchronize()
+    assert rel(y32.double().cpu().numpy(), yo) < 2e-5
+    assert rel(m.diagonal(prob), o.diag(lsg.COEF_SINPROD, params)) < 1e-12
+    f = rng.uniform(-1, 1, g.n) * g.active
+    xs = np.zeros(g.n)
+    rep = lsg.CG.solveHomogen(1e-10, xs, f, m, prob, criterion=1, precision=lsg.FP64)
+    assert rep["converged"] == 1 and rep["rel_residual"] <= 1e-10
