@@ -158,10 +158,11 @@ int lsg_set_learned_diag(lsg_operator *op, const double *diag);
  * D = b * s.  No counterpart in the reference (its CG always uses the exact
  * Jacobi diagonal, applications/cg_method.h:805); solves that stall with D
  * fall back to the exact diagonal (lsg_solve_report.fell_back).
- * Features (F = 7d + 2 floats per point, storage order): t_j / 8, x_j,
+ * Features (F = 7d + 5 floats per point, storage order): t_j / 8, x_j,
  * next-to-boundary flags, log a(x), sum_j t_j / (8d),
- * log a(x +- h_j e_j) - log a(x) with h_j = 2^-t_j, and per dim two flags:
- * the same-depth point two level steps left / right exists. */
+ * log a(x +- h_j e_j) - log a(x) with h_j = 2^-t_j, per dim two flags (the
+ * same-depth point two level steps left / right exists), and mean, min and
+ * max of log a - log a(x) over the midpoints of the 2^d surrounding cells. */
 typedef struct lsg_mlp lsg_mlp;
 /* params: lsg_mlp_num_params(F) floats, layout W1[64][F] b1[64] W2[64][64] b2
  * W3[64][64] b3 W4[64] b4; BF16-rounded weights, FP32 accumulation. */
@@ -177,7 +178,7 @@ int lsg_mlp_gradient(lsg_mlp *m, const float *X, const float *Y, int64_t rows, f
 /* one Adam step (beta 0.9/0.999) on that loss */
 int lsg_mlp_train_step(lsg_mlp *m, const float *X, const float *Y, int64_t rows, float lr, float *loss);
 const char *lsg_mlp_last_error(void);
-/* features (device, n x (7d+2) floats) and the cheap base diagonal (device, n doubles) */
+/* features (device, n x (7d+5) floats) and the cheap base diagonal (device, n doubles) */
 int lsg_operator_features(lsg_operator *op, float *feat, void *stream);
 int lsg_operator_base_diag(lsg_operator *op, double *base, void *stream);
 /* D = base * softplus(mlp(features)) at active points, installed for precond = 2 */

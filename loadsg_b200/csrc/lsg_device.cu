@@ -757,15 +757,16 @@ __global__ void k_diag(DevPlan P, const double* __restrict__ acell, double* __re
 
 
 // ----------------------------------------------------------------------------- learned diagonal
-// Features of point k for the diagonal MLP (F = 7d + 2): depths t_j / 8,
+// Features of point k for the diagonal MLP (F = 7d + 5): depths t_j / 8,
 // coordinates x_j, next-to-boundary flags, log a(x), sum_j t_j / (8 d), the
-// log-coefficient differences log a(x +- h_j e_j) - log a(x), h_j = 2^-t_j, and
-// whether the same-depth points two level steps left / right exist (nbmask).
+// log-coefficient differences log a(x +- h_j e_j) - log a(x), h_j = 2^-t_j,
+// whether the same-depth points two level steps left / right exist (nbmask),
+// and mean / min / max of log a - log a(x) over the 2^d surrounding cell midpoints.
 __global__ void k_features(DevPlan P, int family, const double* __restrict__ params, const uint16_t* __restrict__ nbmask,
                            float* __restrict__ feat) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= P.n) return;
-    int d = P.d, F = 7 * d + 2;
+    int d = P.d, F = 7 * d + 5;
     float* f = feat + k * F;
     double x[lsg::kMaxDim], h[lsg::kMaxDim];
     int tsum = 0;
@@ -794,6 +795,20 @@ __global__ void k_features(DevPlan P, int family, const double* __restrict__ par
     }
     const uint16_t m = nbmask[k];
     for (int j = 0; j < 2 * d; ++j) f[5 * d + 2 + j] = ((m >> j) & 1) ? 1.f : 0.f;
+    // log a at the midpoints of the 2^d level-T cells around the point (the
+    // cells that weigh most in its diagonal): mean, min, max relative to log a(x)
+    double sum = 0.0, lo = 1e300, hi = -1e300;
+    for (int b = 0; b < (1 << d); ++b) {
+        double xm[lsg::kMaxDim];
+        for (int j = 0; j < d; ++j) xm[j] = x[j] + ((b >> j) & 1 ? 0.5 : -0.5) * h[j];
+        double v = log(fmax(lsg_coef_eval_dev(family, params, d, xm), 1e-300)) - la;
+        sum += v;
+        lo = fmin(lo, v);
+        hi = fmax(hi, v);
+    }
+    f[7 * d + 2] = (float)(sum / (1 << d));
+    f[7 * d + 3] = (float)lo;
+    f[7 * d + 4] = (float)hi;
 }
 
 // Cheap diagonal a(x_k) * psi_k^T K_ref psi_k for a constant coefficient on a
@@ -2422,7 +2437,7 @@ extern "C" int lsg_operator_install_learned(lsg_operator* op, lsg_mlp* m, void* 
     if (!op || !m) return fail(LSG_E_INVALID, "null argument");
     if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
     int64_t n = op->plan.n;
-    int F = 7 * op->plan.d + 2;
+    int F = 7 * op->plan.d + 5;
     size_t* tot = &op->dev_bytes;
     int rc = 0;
     if (!op->feat.p) rc |= op->feat.alloc((size_t)n * F * sizeof(float), tot);

@@ -30,7 +30,7 @@ H = 64
 
 
 def n_features(d):
-    return 7 * d + 2
+    return 7 * d + 5
 
 
 def n_params(F):
