@@ -232,9 +232,9 @@ __global__ void kb_stop(int count, Scal s, const double* __restrict__ ff, double
 }
 
 // IR: outer convergence on the FP64 residual, per-grid scale 1/||r|| (0 when done)
-// the inner stop for grids still refining: reduce by itol, or only by 0.1 x the
-// factor still missing to the target when that is looser (the last step of a
-// refinement needs little)
+// the inner stop for grids still refining: when this step can reach the
+// target (the missing factor within 10x of itol) aim at 0.5 x that factor,
+// otherwise reduce by itol (the single-grid refinement's rule)
 __global__ void kb_outer(int count, Scal s, const double* __restrict__ rr64, const double* __restrict__ ff, double eps2,
                          double itol, int32_t* __restrict__ outer_conv, int32_t* __restrict__ outer_its) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -246,7 +246,8 @@ __global__ void kb_outer(int count, Scal s, const double* __restrict__ rr64, con
     else {
         s.scale[i] = 1.0 / sqrt(rr);
         outer_its[i] += 1;
-        double t = fmax(itol, fmin(0.5, 0.1 * sqrt(eps2 * ff[i] / rr)));
+        double t = 0.5 * sqrt(eps2 * ff[i] / rr);
+        t = t >= 0.1 * itol ? fmin(0.5, fmax(t, 0.1 * itol)) : itol;
         s.stop[i] = t * t;
     }
     s.conv[i] = done ? 1 : 0;  // inner CG runs only on grids still refining

@@ -1815,6 +1815,15 @@ struct Solver {
 
 constexpr int kInnerStallWindow = 400;  // iterations without a 10 % residual gain
 
+// Inner reduction of one refinement step, given the factor `need` (< 1) by
+// which the residual still has to shrink: when this step can reach the target
+// (need within 10x of itol) aim at 0.5 need, which lands below the target
+// with margin and costs little when need is large; otherwise reduce by itol.
+inline double inner_step_tol(double itol, double need) {
+    double t = 0.5 * need;
+    return t >= 0.1 * itol ? std::min(0.5, std::max(t, 0.1 * itol)) : itol;
+}
+
 int solver_init(Solver& S, bool fp32) {
     int64_t n = S.n;
     size_t* t = &S.bytes;
@@ -2087,9 +2096,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, s + 5);
             int its = 0;
             double lrr = 0.0;
-            // inner reduction: itol, or only 0.1 x the factor still missing to the
-            // target when that is looser (the last refinement step needs little)
-            const double istep = std::max(itol, std::min(0.5, 0.1 * std::sqrt(eps * eps * ff / rr)));
+            const double istep = inner_step_tol(itol, std::sqrt(eps * eps * ff / rr));
             rc = cg_loop<float>(S, e32, r32, S.g32.as<float>(), d32, h32, z32, 0.0, 1, istep * istep, inner,
                                 o->use_graph != 0, st, &its, &lrr, &R.kernel_launches, kInnerStallWindow);
             R.kernel_launches += matvec_launches(op->plan) + 12;
