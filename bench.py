@@ -374,14 +374,26 @@ def main():
 
     stream = torch.cuda.current_stream().cuda_stream
 
-    def solve(precision, precond):
+    failed = []  # solves that ended in a library error: logged and reported, the line still prints
+
+    def guarded(fn, what):
+        try:
+            return fn()
+        except lsg.LsgError as e:
+            log(f"{what} failed: {e}")
+            failed.append(f"{what}: {e}")
+            return None
+
+    def solve(precision, precond, what="solve"):
         x.zero_()
-        return lsg.CG.solve_device(m, f.data_ptr(), x.data_ptr(), opts(precision, precond), stream)
+        return guarded(lambda: lsg.CG.solve_device(m, f.data_ptr(), x.data_ptr(), opts(precision, precond), stream),
+                       what)
 
     log(f"preconditioner setup: jacobi {jacobi_ms} ms, learned {learned_ms} ms")
     for _ in range(args.warmup):
-        rep = solve(lsg.FP32, precond)
-        log(f"warm-up solve: {rep['seconds']:.2f}s, {rep['iterations']} iterations")
+        rep = solve(lsg.FP32, precond, "warm-up solve")
+        if rep:
+            log(f"warm-up solve: {rep['seconds']:.2f}s, {rep['iterations']} iterations")
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -391,8 +403,10 @@ def main():
         torch.cuda.synchronize()
         ev0.record()
         for _ in range(args.steps):
-            reps.append(solve(lsg.FP32, precond))
-            log(f"timed solve: {reps[-1]['iterations']} iterations, {reps[-1]['outer_iterations']} refinement steps")
+            rep = solve(lsg.FP32, precond, "timed solve")
+            if rep:
+                reps.append(rep)
+                log(f"timed solve: {rep['iterations']} iterations, {rep['outer_iterations']} refinement steps")
         ev1.record()
         torch.cuda.synchronize()
     step_s = max_over_ranks(ev0.elapsed_time(ev1) / 1e3 / args.steps, dist, dev)
@@ -400,19 +414,21 @@ def main():
     # plain FP64 CG on the same instance (the comparison the metric names; the
     # reference's CG is always Jacobi-preconditioned), and FP32+IR with Jacobi
     log(f"timed: {step_s:.2f}s per solve")
-    rep64 = solve(lsg.FP64, 0)
-    log(f"FP64 CG: {rep64['seconds']:.2f}s")
-    rep_jac = solve(lsg.FP32, 0) if precond != 0 else reps[-1]
-    log(f"FP32+IR Jacobi: {rep_jac['seconds']:.2f}s")
+    rep64 = solve(lsg.FP64, 0, "FP64 CG") or {}
+    log(f"FP64 CG: {rep64.get('seconds')}s")
+    rep_jac = (solve(lsg.FP32, 0, "FP32+IR Jacobi") or {}) if precond != 0 else reps[-1] if reps else {}
+    log(f"FP32+IR Jacobi: {rep_jac.get('seconds')}s")
     # end to end through the C-ABI with host buffers
     xh = np.zeros(g.n)
     torch.cuda.synchronize()
     te = time.perf_counter()
     for _ in range(args.steps):
         xh[:] = 0.0
-        rep_e2e = lsg.CG.solveHomogen(1e-10, xh, f_host, m, prob, criterion=1, precision=lsg.FP32, max_iter=3000,
-                                      precond=precond, inner_iter=1000, inner_tol=1e-5)
-        log(f"e2e solve: {rep_e2e['iterations']} iterations, {rep_e2e['outer_iterations']} refinement steps")
+        rep_e2e = guarded(lambda: lsg.CG.solveHomogen(1e-10, xh, f_host, m, prob, criterion=1, precision=lsg.FP32,
+                                                      max_iter=3000, precond=precond, inner_iter=1000,
+                                                      inner_tol=1e-5), "e2e solve")
+        if rep_e2e:
+            log(f"e2e solve: {rep_e2e['iterations']} iterations, {rep_e2e['outer_iterations']} refinement steps")
     e2e_s = (time.perf_counter() - te) / args.steps
     log(f"e2e: {e2e_s:.2f}s per solve")
 
@@ -436,7 +452,8 @@ def main():
     # over the 21 phase-B launches of one FP32 matvec)
     traffic = 2.23e9 if args.workload == "d6_adaptive_corner" else None
 
-    batch = None if args.no_batch else batch_leg(lsg, torch, dev, stream, count=args.batch_grids)
+    batch = None if args.no_batch else guarded(lambda: batch_leg(lsg, torch, dev, stream, count=args.batch_grids),
+                                               "batch leg")
 
     if rank != 0:
         if dist:
@@ -444,6 +461,7 @@ def main():
             dist.destroy_process_group()
         return
     cpu = None if args.no_cpu_baseline or world > 1 else cpu_reference_sample(args)
+    last = reps[-1] if reps else {}
     line = {
         "metric": METRIC, "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -451,13 +469,13 @@ def main():
         "config": {"workload": args.workload, "description": desc, "n_points": g.n, "n_active": g.getDOFS(),
                    "tolerance": 1e-10, "precond": ["jacobi", "none", "learned"][precond],
                    "parallelism": f"replicas x{world}", "l2": "working set larger than L2 (126 MB)"},
-        "iterations": reps[-1]["iterations"], "outer_iterations": reps[-1]["outer_iterations"],
-        "rel_residual": reps[-1]["rel_residual"],
-        "fp64_cg": {"seconds": rep64["seconds"], "iterations": rep64["iterations"],
-                    "rel_residual": rep64["rel_residual"]},
-        "speedup_vs_fp64_cg": rep64["seconds"] / step_s if step_s > 0 else None,
-        "fp32_ir_jacobi": {"seconds": rep_jac["seconds"], "iterations": rep_jac["iterations"],
-                           "rel_residual": rep_jac["rel_residual"]},
+        "iterations": last.get("iterations"), "outer_iterations": last.get("outer_iterations"),
+        "rel_residual": last.get("rel_residual"), "failed_solves": failed,
+        "fp64_cg": {"seconds": rep64.get("seconds"), "iterations": rep64.get("iterations"),
+                    "rel_residual": rep64.get("rel_residual")},
+        "speedup_vs_fp64_cg": rep64["seconds"] / step_s if rep64 and step_s > 0 else None,
+        "fp32_ir_jacobi": {"seconds": rep_jac.get("seconds"), "iterations": rep_jac.get("iterations"),
+                           "rel_residual": rep_jac.get("rel_residual")},
         "preconditioner_setup_ms": {"jacobi_exact_diag": jacobi_ms, "learned": learned_ms},
         "tuning": {"setting": tune_setting, "matvec_ms_fp32": tune_ms, "matvec_ms_fp32_default": tune_default_ms},
         "matvec": {"fp32_ms": ms32[4], "fp64_ms": ms64[4], "fp32_gbs": by32[4] / (ms32[4] * 1e-3) / 1e9,

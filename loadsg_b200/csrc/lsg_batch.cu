@@ -329,7 +329,7 @@ struct BSolver {
     int32_t* pend_h = nullptr;
     Scal S{};
     ~BSolver() { if (pend_h) cudaFreeHost(pend_h); }
-    int init(bool fp32) {
+    int init(bool fp32, cudaStream_t st) {
         int rc = 0;
         rc |= r.alloc(n * 8);
         rc |= g.alloc(n * 8);
@@ -368,7 +368,7 @@ struct BSolver {
         S.best_it = f + 3 * count;
         S.pending = f + 4 * count;
         for (Buf* bf : {&r, &g, &d, &h, &sc, &flags, &outer_conv, &outer_its, &r32, &g32, &d32, &h32, &e32})
-            if (bf->p) BT_TRY(cudaMemset(bf->p, 0, bf->bytes));
+            if (bf->p) BT_TRY(cudaMemsetAsync(bf->p, 0, bf->bytes, st));  // on the solver's stream
         return 0;
     }
     const Chunk* ch() const { return B->chunks.as<Chunk>(); }
@@ -490,7 +490,7 @@ int batch_solve(lsg_batch* b, const double* f, double* x, const lsg_solver_opts*
     S.B = b;
     S.count = count;
     S.n = n;
-    int rc = S.init(fp32);
+    int rc = S.init(fp32, st);
     if (rc) return rc;
     // diagonal of every grid, side by side in batch order
     const double* z = nullptr;

@@ -1824,7 +1824,7 @@ inline double inner_step_tol(double itol, double need) {
     return t >= 0.1 * itol ? std::min(0.5, std::max(t, 0.1 * itol)) : itol;
 }
 
-int solver_init(Solver& S, bool fp32) {
+int solver_init(Solver& S, bool fp32, cudaStream_t st) {
     int64_t n = S.n;
     size_t* t = &S.bytes;
     int rc = 0;
@@ -1843,9 +1843,11 @@ int solver_init(Solver& S, bool fp32) {
         rc |= S.z32.alloc(n * 4, t);
     }
     if (rc) return LSG_E_CUDA;
-    // every vector starts at zero (fresh VectorSparseG), hanging entries included
+    // every vector starts at zero (fresh VectorSparseG), hanging entries
+    // included; zeroed on the solver's own stream, which does not wait for
+    // work on the legacy default stream
     for (DBuf* b : {&S.r, &S.g, &S.d, &S.h, &S.s, &S.r32, &S.g32, &S.d32, &S.h32, &S.e32, &S.z32})
-        if (b->p) CUDA_TRY(cudaMemset(b->p, 0, b->bytes));
+        if (b->p) CUDA_TRY(cudaMemsetAsync(b->p, 0, b->bytes, st));
     return 0;
 }
 
@@ -1990,7 +1992,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
     int64_t n = S.n;
     lsg_solve_report R;
     memset(&R, 0, sizeof R);
-    int rc = solver_init(S, o->precision == LSG_FP32);
+    int rc = solver_init(S, o->precision == LSG_FP32, st);
     if (!rc) rc = prepare<double>(op);
     if (!rc && o->precision == LSG_FP32) rc = prepare<float>(op);
     const double* zdiag = nullptr;
