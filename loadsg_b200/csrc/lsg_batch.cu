@@ -234,9 +234,11 @@ __global__ void kb_stop(int count, Scal s, const double* __restrict__ ff, double
 // IR: outer convergence on the FP64 residual, per-grid scale 1/||r|| (0 when done)
 // the inner stop for grids still refining: when this step can reach the
 // target (the missing factor within 10x of itol) aim at 0.5 x that factor,
-// otherwise reduce by itol (the single-grid refinement's rule)
+// or 0.1 x after a step that did not halve the residual, otherwise reduce by
+// itol (the single-grid refinement's rule); rr_prev[i] keeps the last residual
 __global__ void kb_outer(int count, Scal s, const double* __restrict__ rr64, const double* __restrict__ ff, double eps2,
-                         double itol, int32_t* __restrict__ outer_conv, int32_t* __restrict__ outer_its) {
+                         double itol, int32_t* __restrict__ outer_conv, int32_t* __restrict__ outer_its,
+                         double* __restrict__ rr_prev) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     double rr = rr64[i];
@@ -246,7 +248,9 @@ __global__ void kb_outer(int count, Scal s, const double* __restrict__ rr64, con
     else {
         s.scale[i] = 1.0 / sqrt(rr);
         outer_its[i] += 1;
-        double t = 0.5 * sqrt(eps2 * ff[i] / rr);
+        const double margin = rr_prev[i] > 0.0 && rr > 0.25 * rr_prev[i] ? 0.1 : 0.5;
+        rr_prev[i] = rr;
+        double t = margin * sqrt(eps2 * ff[i] / rr);
         t = t >= 0.1 * itol ? fmin(0.5, fmax(t, 0.1 * itol)) : itol;
         s.stop[i] = t * t;
     }
@@ -325,7 +329,7 @@ struct BSolver {
     int stall = 0;  // stall window of the current loop (0: off)
     Buf r, g, d, h, z, part, sc, flags, ff, rr64;
     Buf r32, g32, d32, h32, e32, z32;
-    Buf outer_conv, outer_its;
+    Buf outer_conv, outer_its, rr_prev;
     int32_t* pend_h = nullptr;
     Scal S{};
     ~BSolver() { if (pend_h) cudaFreeHost(pend_h); }
@@ -342,6 +346,7 @@ struct BSolver {
         rc |= rr64.alloc((size_t)count * 8);
         rc |= outer_conv.alloc((size_t)count * 4);
         rc |= outer_its.alloc((size_t)count * 4);
+        rc |= rr_prev.alloc((size_t)count * 8);
         if (fp32) {
             rc |= r32.alloc(n * 4);
             rc |= g32.alloc(n * 4);
@@ -367,7 +372,8 @@ struct BSolver {
         S.bad = f + 2 * count;
         S.best_it = f + 3 * count;
         S.pending = f + 4 * count;
-        for (Buf* bf : {&r, &g, &d, &h, &sc, &flags, &outer_conv, &outer_its, &r32, &g32, &d32, &h32, &e32})
+        for (Buf* bf :
+             {&r, &g, &d, &h, &sc, &flags, &outer_conv, &outer_its, &rr_prev, &r32, &g32, &d32, &h32, &e32})
             if (bf->p) BT_TRY(cudaMemsetAsync(bf->p, 0, bf->bytes, st));  // on the solver's stream
         return 0;
     }
@@ -545,7 +551,8 @@ int batch_solve(lsg_batch* b, const double* f, double* x, const lsg_solver_opts*
             S.dot<double, double>(r, r, S.rr64.as<double>(), st);
             BT_TRY(cudaMemsetAsync(S.S.pending, 0, 4, st));
             kb_outer<<<nb(count), kThreads, 0, st>>>(count, S.S, S.rr64.as<double>(), S.ff.as<double>(), eps * eps,
-                                                     itol, S.outer_conv.as<int32_t>(), S.outer_its.as<int32_t>());
+                                                     itol, S.outer_conv.as<int32_t>(), S.outer_its.as<int32_t>(),
+                                                     S.rr_prev.as<double>());
             BT_TRY(cudaMemcpyAsync(S.pend_h, S.S.pending, 4, cudaMemcpyDeviceToHost, st));
             BT_TRY(cudaStreamSynchronize(st));
             launches += batch_matvec_launches(b) + 6;

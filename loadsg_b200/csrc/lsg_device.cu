@@ -1817,10 +1817,11 @@ constexpr int kInnerStallWindow = 400;  // iterations without a 10 % residual ga
 
 // Inner reduction of one refinement step, given the factor `need` (< 1) by
 // which the residual still has to shrink: when this step can reach the target
-// (need within 10x of itol) aim at 0.5 need, which lands below the target
-// with margin and costs little when need is large; otherwise reduce by itol.
-inline double inner_step_tol(double itol, double need) {
-    double t = 0.5 * need;
+// (need within 10x of itol) aim at `margin` x need -- 0.5 lands below the
+// target with margin and costs little when need is large, and a step after
+// one that fell short aims at 0.1 -- otherwise reduce by itol.
+inline double inner_step_tol(double itol, double need, double margin) {
+    double t = margin * need;
     return t >= 0.1 * itol ? std::min(0.5, std::max(t, 0.1 * itol)) : itol;
 }
 
@@ -2098,7 +2099,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             k_dot_final<<<1, 1024, 0, st>>>(S.part.as<double>(), kRedBlocks, s + 5);
             int its = 0;
             double lrr = 0.0;
-            const double istep = inner_step_tol(itol, std::sqrt(eps * eps * ff / rr));
+            const double istep = inner_step_tol(itol, std::sqrt(eps * eps * ff / rr), slow_steps ? 0.1 : 0.5);
             rc = cg_loop<float>(S, e32, r32, S.g32.as<float>(), d32, h32, z32, 0.0, 1, istep * istep, inner,
                                 o->use_graph != 0, st, &its, &lrr, &R.kernel_launches, kInnerStallWindow);
             R.kernel_launches += matvec_launches(op->plan) + 12;
