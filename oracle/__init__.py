@@ -42,6 +42,8 @@ def lib():
         L.lsgo_cg.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_double, ctypes.c_int, P]
         L.lsgo_nodal_by_prew.argtypes = [P, P, P]
         L.lsgo_set_form.argtypes = [P, ctypes.c_int]
+        L.lsgo_hierarchize_boundary.argtypes = [P, P]
+        L.lsgo_boundary_rhs.argtypes = [P, P, ctypes.c_int, P, P]
         _LIB = L
     return _LIB
 
@@ -142,6 +144,26 @@ class OracleGrid:
         Av = self.matvec(0, [1.0], v, form=0 if h1 else 1)
         act = np.asarray(self.active) > 0
         return float(np.sqrt(np.sum(v[act] * Av[act])))
+
+    def hierarchize_boundary(self, u):
+        """CalcHierarchicalBasisForRHS (MatrixVectorMultiplication/RHS.cpp:6-41)
+        on a grid with boundary points: returns the transformed copy of u."""
+        u = np.array(u, np.float64)
+        if lib().lsgo_hierarchize_boundary(self._h, _ptr(u)) != 0:
+            raise ValueError("a boundary point lacks a 1D parent")
+        return u
+
+    def boundary_rhs(self, ngrid, kind, hier, y=None):
+        """InHomoBoundaryRHSHierarchical (RHS.cpp:697-1008) onto this grid from
+        the hierarchical boundary coefficients hier of ngrid (a grid with
+        boundary points): kind 0 multiply (gradients), 1 multiply_mass, 2
+        multiply_mass_coeff (weight prod (1 - x_k^2)).  Active entries of y are
+        written, the others keep their values (0 for a fresh y)."""
+        hier = np.ascontiguousarray(hier, np.float64)
+        y = np.zeros(self.n) if y is None else np.array(y, np.float64)
+        if lib().lsgo_boundary_rhs(self._h, ngrid._h, kind, _ptr(hier), _ptr(y)) != 0:
+            raise ValueError("oracle boundary right-hand side failed")
+        return y
 
     def cg(self, family, params, f, eps, maxit=500, x0=None):
         lib().lsgo_set_form(self._h, 0)

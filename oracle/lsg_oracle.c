@@ -739,3 +739,125 @@ int lsgo_nodal_by_prew(lsgo_grid *g, const double *prew, double *u) {
 }
 
 void lsgo_set_form(lsgo_grid *g, int form) { g->form = form; }
+
+/* ------------------------------------------------------------ boundary-data right-hand sides
+ * MatrixVectorMultiplication/RHS.cpp and RHS.h:278-427.  The second grid ng
+ * holds boundary points (a 1D index 0 or 1 in some dimension, depth 0 there). */
+
+/* CalcHierarchicalBasisForRHS (RHS.cpp:6-41): per dimension, every boundary
+ * point with depth > 0 in it loses half the sum of its two 1D parents; the
+ * points are visited finest depth first, so a parent still holds the value of
+ * the previous dimension's pass when its sons read it. */
+int lsgo_hierarchize_boundary(lsgo_grid *ng, double *u) {
+    int d = ng->d;
+    for (int dd = 0; dd < d; ++dd)
+        for (int t = ng->maxdep[dd]; t >= 1; --t)
+            for (int64_t k = 0; k < ng->n; ++k) {
+                const int32_t *I = ng->pts + k * d;
+                int boundary = 0;
+                for (int q = 0; q < d; ++q) boundary |= !interior1(I[q]);
+                if (!boundary || ng->dep[k * d + dd] != t) continue;
+                int64_t l = nbr(ng, k, dd, 0), r = nbr(ng, k, dd, 1);
+                if (l < 0 || r < 0) return -1;  /* the reference needs both parents */
+                u[k] = u[k] - 0.5 * (u[l] + u[r]);
+            }
+    return 0;
+}
+
+/* integral over [a,b] of (mp x + cp)(mq x + cq) by its antiderivative, and the
+ * same with the weight (1 - x^2): RHS.cpp:47-54 and :285-300, evaluated in the
+ * reference's order (the form loses digits to cancellation on fine levels). */
+static double bd_int(double a, double b, double mp, double mq, double cp, double cq) {
+    double t1 = (1.0 / 3.0 * b * b * b * mp * mq) - (1.0 / 3.0 * a * a * a * mp * mq);
+    double t2 = (0.5 * b * b * mp * cq) - (0.5 * a * a * mp * cq);
+    double t3 = (0.5 * b * b * mq * cp) - (0.5 * a * a * mq * cp);
+    double t4 = (b - a) * cp * cq;
+    return t1 + t2 + t3 + t4;
+}
+static double bd_int_w(double a, double b, double mp, double mq, double cp, double cq) {
+    double r1 = bd_int(a, b, mp, mq, cp, cq);
+    double t1 = (1.0 / 5.0 * b * b * b * b * b * mp * mq) - (1.0 / 5.0 * a * a * a * a * a * mp * mq);
+    double t2 = (0.25 * b * b * b * b * mp * cq) - (0.25 * a * a * a * a * mp * cq);
+    double t3 = (0.25 * b * b * b * b * mq * cp) - (0.25 * a * a * a * a * mq * cp);
+    double t4 = (1.0 / 3.0 * b * b * b * cp * cq) - (1.0 / 3.0 * a * a * a * cp * cq);
+    double r2 = t1 + t2 + t3 + t4;
+    return r1 - r2;
+}
+
+/* One dimension of CalcIntegral / CalcIntegral_mass / CalcIntegral_coeff
+ * (RHS.cpp:56-283, :314-503, :505-695): the hat of p (1D index ip, width 2^-tp)
+ * against the hat of q (1D index iq, width 2^-tq, only its half inside [0,1]
+ * at a boundary index), summed over the four pairs of linear pieces in the
+ * order left-left, left-right, right-left, right-right.  kind 0: product of
+ * the functions, 1: of their derivatives, 2: of the functions weighted by
+ * (1 - x^2). */
+static double bd_factor(int32_t ip, int tp, int32_t iq, int tq, int kind) {
+    double mpl = (double)(1u << tp), mql = (double)(1u << tq);
+    double hp = 1.0 / mpl, hq = 1.0 / mql, xp = coord1(ip), xq = coord1(iq);
+    double mp[2] = {mpl, -1.0 * mpl}, mq[2] = {mql, -1.0 * mql};
+    double cp[2] = {-(xp - hp) / hp, +(xp + hp) / hp}, cq[2] = {-(xq - hq) / hq, +(xq + hq) / hq};
+    double lp[2] = {xp - hp, xp}, rp[2] = {xp, xp + hp}, lq[2] = {xq - hq, xq}, rq[2] = {xq, xq + hq};
+    double s = 0.0;
+    for (int sp = 0; sp < 2; ++sp)
+        for (int sq = 0; sq < 2; ++sq) {
+            double v = 0.0;
+            int skip = (iq == 0 && sq == 0) || (iq == 1 && sq == 1);
+            if (!skip && !(rp[sp] < lq[sq]) && !(rq[sq] < lp[sp])) {
+                double a = lq[sq] > lp[sp] ? lq[sq] : lp[sp];
+                double b = rp[sp] < rq[sq] ? rp[sp] : rq[sq];
+                if (kind == 1) v = (b - a) * mp[sp] * mq[sq];
+                else if (kind == 0) v = bd_int(a, b, mp[sp], mq[sq], cp[sp], cq[sq]);
+                else v = bd_int_w(a, b, mp[sp], mq[sq], cp[sp], cq[sq]);
+            }
+            s = s + v;  /* ll + lr + rl + rr, left to right */
+        }
+    return s;
+}
+
+/* InHomoBoundaryRHSHierarchical::multiply / multiply_mass / multiply_mass_coeff
+ * (RHS.cpp:697-1008): for every depth T of g, nodal values at the points of
+ * depth <= T, sum over the boundary points b of ng of I(p at level T, b) hier[b]
+ * (depth-list order of ng, storage order within a depth), then
+ * ConvertToPrewavelet2 at the active points of depth T (RHS.h:397-420). */
+int lsgo_boundary_rhs(lsgo_grid *g, lsgo_grid *ng, int kind, const double *hier, double *y) {
+    int d = g->d;
+    if (ng->d != d || kind < 0 || kind > 2) return -1;
+    double *nodal = (double *)malloc(sizeof(double) * (size_t)g->n);
+    if (!nodal) return -1;
+    for (int t = 0; t < g->nD; ++t) {
+        const int32_t *T = g->D + t * d;
+        for (int64_t k = 0; k < g->n; ++k) {
+            nodal[k] = 0.0;
+            if (!depth_le(g->dep + k * d, T, d)) continue;
+            const int32_t *P = g->pts + k * d;
+            double sum = 0.0;
+            for (int u = 0; u < ng->nD; ++u) {
+                const int32_t *TH = ng->D + u * d;
+                int boundary = 0;
+                for (int q = 0; q < d; ++q) boundary |= TH[q] == 0;
+                if (!boundary) continue;
+                for (int64_t e = ng->ex_off[u]; e < ng->ex_off[u + 1]; ++e) {
+                    int64_t b = ng->ex[e];
+                    const int32_t *Q = ng->pts + b * d;
+                    double val;
+                    if (kind == 0) {  /* CalcIntegral: sum over the derivative dimension */
+                        val = 0.0;
+                        for (int o = 0; o < d; ++o) {
+                            double prod = 1.0;
+                            for (int q = 0; q < d; ++q) prod *= bd_factor(P[q], T[q], Q[q], TH[q], q == o ? 1 : 0);
+                            val += prod;
+                        }
+                    } else {
+                        val = 1.0;
+                        for (int q = 0; q < d; ++q) val *= bd_factor(P[q], T[q], Q[q], TH[q], kind == 1 ? 0 : 2);
+                    }
+                    sum += val * hier[b];
+                }
+            }
+            nodal[k] = sum;
+        }
+        convert_prew(g, t, nodal, y);
+    }
+    free(nodal);
+    return 0;
+}

@@ -50,4 +50,14 @@ void lsgo_set_form(lsgo_grid *g, int form);
  * u = values at every point of the expansion sum_i prew_i psi_i (all points). */
 int lsgo_nodal_by_prew(lsgo_grid *g, const double *prew, double *u);
 
+/* Boundary-data right-hand sides (MatrixVectorMultiplication/RHS.cpp, RHS.h).
+ * ng is a grid with boundary points (completeNeumannGrid).
+ * lsgo_hierarchize_boundary: CalcHierarchicalBasisForRHS on u (ng's storage
+ * order), in place at the boundary points.  lsgo_boundary_rhs: y at the active
+ * points of g = InHomoBoundaryRHSHierarchical::multiply (kind 0),
+ * multiply_mass (1) or multiply_mass_coeff (2) of the hierarchical boundary
+ * coefficients hier (ng's storage order); other entries of y are untouched. */
+int lsgo_hierarchize_boundary(lsgo_grid *ng, double *u);
+int lsgo_boundary_rhs(lsgo_grid *g, lsgo_grid *ng, int kind, const double *hier, double *y);
+
 #endif

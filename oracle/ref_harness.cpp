@@ -366,6 +366,55 @@ int main(int argc, char **argv) {
         dump("x.f64", x);
         g_meta << "iterations " << it << "\nrelres " << sqrt(rr / ff) << "\nsolve_seconds " << secs
                << "\nprecond_seconds " << tp << "\n";
+    } else if (cmd == "bdrhs") {
+        // Boundary-data right-hand sides (MatrixVectorMultiplication/RHS.h:278-427,
+        // RHS.cpp:6-41,697-1008): a second grid with boundary points, built like
+        // the first and then completeNeumannGrid (sparseGrid.cc:654-677); boundary
+        // values g = family gfam at the boundary points, 0 inside;
+        // CalcHierarchicalBasisForRHS(g), then InHomoBoundaryRHSHierarchical
+        // multiply / multiply_mass / multiply_mass_coeff onto this grid.
+        AdaptiveSparseGrid ngrid;
+        build_grid(ngrid);
+        ngrid.completeNeumannGrid();
+        unsigned long NN = ngrid.getMaximalOccupiedSecondTable();
+        int gfam = atoi(opt("gfam", "1").c_str());
+        std::vector<double> gp = parse_list(opt("gp", "1,0.5,1,1,1,1,1,1,1,1"));
+        gp.resize(LSG_COEF_MAXPARAM, 0.0);
+        std::vector<int32_t> nidx(NN * D);
+        std::vector<uint8_t> nact(NN);
+        std::vector<double> g(NN, 0.0);
+        for (unsigned long k = 0; k < NN; ++k) {
+            IndexDimension I = ngrid.getIndexOfTable(k);
+            double x[D];
+            bool boundary = false;
+            for (int d = 0; d < D; ++d) {
+                nidx[k * D + d] = I.getIndex(d);
+                x[d] = I.coordinate(d);
+                if (I.getIndex(d) < 2) boundary = true;
+            }
+            nact[k] = ngrid.getActiveTable()[k] ? 1 : 0;
+            if (boundary) g[k] = lsg_coef_eval(gfam, gp.data(), D, x);
+        }
+        dump("npoints.i32", nidx);
+        dump("nactive.u8", nact);
+        dump("g.f64", g);
+        VectorSparseG gv(ngrid), yv(grid);
+        set_vec(gv, g);
+        CalcHierarchicalBasisForRHS(gv);
+        dump("g_hier.f64", get_vec(gv, NN));
+        InHomoBoundaryRHSHierarchical rhs(grid);
+        auto t0 = std::chrono::steady_clock::now();
+        yv = 0.0;
+        rhs.multiply(gv, yv);
+        double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        dump("y_stiff.f64", get_vec(yv, N));
+        yv = 0.0;
+        rhs.multiply_mass(gv, yv);
+        dump("y_mass.f64", get_vec(yv, N));
+        yv = 0.0;
+        rhs.multiply_mass_coeff(gv, yv);
+        dump("y_coeff.f64", get_vec(yv, N));
+        g_meta << "NN " << NN << "\nstiff_seconds " << secs << "\n";
     } else if (cmd == "prew2nodal" || cmd == "nodal2prew") {
         // prew2nodal: u = calcNodalByPrew(x); nodal2prew: p = calcPrewByNodal(x)
         std::vector<double> x = read_f64(opt("x", ""), N);

@@ -9,7 +9,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+_ALL = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+# operator fixtures (matvec, diagonal, CG, transforms) and boundary-data
+# right-hand-side fixtures (bd_*: a grid with boundary points beside the grid)
+GOLDEN = [p for p in _ALL if not os.path.basename(p).startswith("bd_")]
+GOLDEN_BD = [p for p in _ALL if os.path.basename(p).startswith("bd_")]
 
 
 def pytest_configure(config):

@@ -10,11 +10,18 @@ reference.
     python tests/golden/make_golden.py [--refsrc /path/to/library/source] [--only NAME]
     python tests/golden/make_golden.py --cmds prew2nodal,nodal2prew   # add commands to existing fixtures
 
+    python tests/golden/make_golden.py --bd        # boundary-data right-hand sides -> bd_<name>.npz
+
 prew2nodal / nodal2prew run calcNodalByPrew / calcPrewByNodal on the fixture's
 x (BasisTransformations/BasisTransformations.cpp:486-545,670-706); mass /
 massdiag use the midpoint plugin with the Q1 mass matrix, helmholtz the
 reference's own HelmHoltz stencil (stencils/Stencil.h:873-919); h1norm /
 l2norm are H1::getValue / L2::getValue (applications/H1_Norm.cpp) of x.
+The bd_ fixtures hold a second grid with boundary points (the same build,
+then completeNeumannGrid), boundary values g of a coefficient family, g after
+CalcHierarchicalBasisForRHS, and InHomoBoundaryRHSHierarchical's multiply /
+multiply_mass / multiply_mass_coeff onto the first grid
+(MatrixVectorMultiplication/RHS.cpp:6-41,697-1008).
 """
 import argparse
 import os
@@ -49,6 +56,18 @@ CASES = [
     ("d8_L2", 8, "level=2", EXPSIN6, ["tables", "matvec", "poisson", "prew2nodal", "nodal2prew"]),
     # the CPU-runnable configuration: d = 3, level 7 (7,423 points), a = 1 + 0.5 prod sin(pi x_i)
     ("d3_L7", 3, "level=7", SINPROD, ["matvec", "poisson", "diag", "cg"]),
+]
+
+
+# boundary-data right-hand sides: name, d, grid args, boundary-value family (g)
+BD_CASES = [
+    ("bd_d2_L5", 2, "level=5", SIN2PI),
+    ("bd_d2_adapt", 2, "level=3 refine=2 theta=0.6 target=corner", EXPSIN6),
+    ("bd_d3_L4", 3, "level=4", SIN2PI),
+    ("bd_d3_adapt", 3, "level=2 refine=3 theta=0.6 target=corner", EXPSIN6),
+    ("bd_d4_L3", 4, "level=3", EXPSIN6),
+    ("bd_d5_L2", 5, "level=2", SIN2PI),
+    ("bd_d6_L2", 6, "level=2", EXPSIN6),
 ]
 
 
@@ -151,12 +170,40 @@ def add_commands(name, d, gridargs, coef, cmds, refsrc):
     print(f"{name}: added {cmds}")
 
 
+def make_bd_case(name, d, gridargs, gcoef, refsrc):
+    run(["make", "-s", "-C", ORACLE, "ref", f"D={d}", f"REFSRC={refsrc}", "-j8"])
+    exe = os.path.join(ORACLE, "_ref", f"d{d}", "ref_harness")
+    fam, params = gcoef
+    args = gridargs.split() + [f"gfam={fam}", "gp=" + ",".join(repr(float(p)) for p in params)]
+    out = {"d": np.int32(d), "g_family": np.int32(fam), "g_params": np.array(params, np.float64),
+           "gridargs": np.array(gridargs)}
+    with tempfile.TemporaryDirectory() as tmp:
+        for c in ("grid", "bdrhs"):
+            run([exe, c, tmp] + args)
+            meta, arrs = read_meta(os.path.join(tmp, f"meta_{c}.txt"))
+            out.update(load_arrays(tmp, arrs, ""))
+            for k, v in meta.items():
+                if k != "ok":
+                    out[f"{c}_meta_{k}"] = np.float64(float(v))
+    out["npoints"] = out["npoints"].reshape(-1, d)
+    out["points"] = out["points"].reshape(-1, d)
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"{name}: N={len(out['active'])} NN={len(out['nactive'])} -> {os.path.getsize(path)} bytes")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--refsrc", default="/root/reference/library/source")
     ap.add_argument("--only", default=None)
     ap.add_argument("--cmds", default=None, help="comma list: add these commands to existing fixtures")
+    ap.add_argument("--bd", action="store_true", help="the boundary-data right-hand-side fixtures")
     a = ap.parse_args()
+    if a.bd:
+        for case in BD_CASES:
+            if not a.only or case[0] == a.only:
+                make_bd_case(*case, refsrc=a.refsrc)
+        return
     for case in CASES:
         if a.only and case[0] != a.only:
             continue
