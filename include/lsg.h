@@ -208,6 +208,33 @@ int lsg_calc_prew_by_nodal_device(lsg_operator *op, double *prew, const double *
 int lsg_h1_norm(lsg_operator *op, const double *u, double *value);
 int lsg_l2_norm(lsg_operator *op, const double *u, double *value);
 
+/* ---- boundary-data right-hand sides (MatrixVectorMultiplication/RHS.h:278-427,
+ * RHS.cpp:6-41,697-1008).  The boundary values g live on a second grid that
+ * holds boundary points (a 1D index 0 or 1 in some dimension), e.g. the
+ * operator's grid completed by completeNeumannGrid (lsg_grid_adaptive, bit 64
+ * of `complete`); nn points, nn x d 1D indices in that grid's storage order.
+ * lsg_hierarchize_boundary: CalcHierarchicalBasisForRHS in place on u (nn
+ * host doubles): every boundary point loses half the sum of its 1D parents,
+ * dimension by dimension, finest depth first; interior entries are untouched;
+ * LSG_E_INVALID when a parent is missing from the grid.
+ * lsg_boundary_rhs: rhs at the active points of the operator's grid =
+ * InHomoBoundaryRHSHierarchical::multiply (LSG_BDRHS_GRADIENT: integrals of
+ * grad psi_i . grad g), multiply_mass (LSG_BDRHS_MASS: psi_i g) or
+ * multiply_mass_coeff (LSG_BDRHS_MASS_COEFF: psi_i g prod_k (1 - x_k^2)) of
+ * the hierarchical coefficients `hier` of the second grid (only its boundary
+ * points are read); other entries of rhs keep their values.  Results equal the
+ * reference's to the bit.  Host arrays; the _device form takes hier and rhs
+ * in device memory (points stay on the host) and runs on `stream`.  The
+ * operator needs no coefficient; its tables are built on first use. */
+#define LSG_BDRHS_GRADIENT 0
+#define LSG_BDRHS_MASS 1
+#define LSG_BDRHS_MASS_COEFF 2
+int lsg_hierarchize_boundary(int32_t d, int64_t nn, const int32_t *points, double *u);
+int lsg_boundary_rhs(lsg_operator *op, int32_t kind, int64_t nn, const int32_t *points, const double *hier,
+                     double *rhs);
+int lsg_boundary_rhs_device(lsg_operator *op, int32_t kind, int64_t nn, const int32_t *points, const double *hier,
+                            double *rhs, void *stream);
+
 /* ---- launch parameters of the matvec and the autotuner that picks them.
  * The defaults suit large d=5/6 grids; lsg_operator_autotune times matvecs of
  * this operator over a candidate set per parameter (coordinate descent, two
@@ -296,7 +323,11 @@ int lsg_grid_regular(int32_t d, int32_t level, int32_t *points, int64_t capacity
  * last completion stage (addPoints2, sgrid/GridGeneration.cpp:333-392) tests
  * pairs of points; it runs only on grids of at most 40000 points (above that
  * it is skipped: on every corner/plane refinement tested up to 41k points it
- * added nothing).  Pass points = active = NULL to query *n. */
+ * added nothing).  `complete` 1 runs every stage; a larger value is a bit
+ * mask of stages (2, 4, 8: the completion passes, 16: hanging nodes, 32:
+ * addPoints2), and bit 64 adds completeNeumannGrid (sgrid/sparseGrid.cc:
+ * 654-740) at the end: the boundary points of a grid for boundary data.
+ * Pass points = active = NULL to query *n. */
 int lsg_grid_adaptive(int32_t d, int32_t level, int32_t refine, double theta, int32_t target, int32_t complete,
                       int32_t *points, uint8_t *active, int64_t capacity, int64_t *n);
 

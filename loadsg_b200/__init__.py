@@ -125,6 +125,9 @@ def lib():
             "lsg_grid_regular": (ctypes.c_int, [I32, I32, P, I64, P]),
             "lsg_grid_adaptive": (ctypes.c_int, [I32, I32, I32, D, I32, I32, P, P, I64, P]),
             "lsg_operator_set_form": (ctypes.c_int, [P, I32]),
+            "lsg_hierarchize_boundary": (ctypes.c_int, [I32, I64, P, P]),
+            "lsg_boundary_rhs": (ctypes.c_int, [P, I32, I64, P, P, P]),
+            "lsg_boundary_rhs_device": (ctypes.c_int, [P, I32, I64, P, P, P, P]),
             "lsg_h1_norm": (ctypes.c_int, [P, P, P]),
             "lsg_l2_norm": (ctypes.c_int, [P, P, P]),
             "lsg_calc_nodal_by_prew": (ctypes.c_int, [P, P, P]),
@@ -202,6 +205,26 @@ class AdaptiveSparseGrid:
                                        ctypes.byref(n)))
         return cls(pts, act)
 
+    @classmethod
+    def neumann(cls, d, level, refine=0, theta=0.5, target="corner"):
+        """The grid of `regular` (refine = 0) or `adaptive` with the same
+        arguments, then completeNeumannGrid (sgrid/sparseGrid.cc:654-740): its
+        boundary points, all active, in the reference's storage order.  This is
+        the second grid that boundary data g live on."""
+        t = {"corner": 0, "plane": 1}[target]
+        mask = (0x3E if refine > 0 else 0) | 64
+        n = ctypes.c_int64(0)
+        _check(lib().lsg_grid_adaptive(d, level, refine, theta, t, mask, None, None, 0, ctypes.byref(n)))
+        pts = np.zeros((n.value, d), np.int32)
+        act = np.zeros(n.value, np.uint8)
+        _check(lib().lsg_grid_adaptive(d, level, refine, theta, t, mask, _ptr(pts), _ptr(act), n.value,
+                                       ctypes.byref(n)))
+        return cls(pts, act)
+
+    def boundary_mask(self):
+        """Points with a 1D index 0 or 1 (coordinate 0 or 1) in some dimension."""
+        return (self.points < 2).any(axis=1)
+
     def getMaximalOccupiedSecondTable(self):
         return self.n
 
@@ -211,8 +234,9 @@ class AdaptiveSparseGrid:
     def coordinates(self):
         """Coordinates of all points (IndexOneD::coordinate, indices/index.h:718-730)."""
         idx = self.points.astype(np.int64)
-        t = np.floor(np.log2(idx)).astype(np.int64)
-        return (2 * (idx - (1 << t)) + 1) / (2.0 ** t)
+        t = np.floor(np.log2(np.maximum(idx, 2))).astype(np.int64)
+        x = (2 * (idx - (1 << t)) + 1) / (2.0 ** t)
+        return np.where(idx < 2, idx.astype(np.float64), x)  # boundary indices 0, 1 sit at 0, 1
 
 
 FORM_STIFFNESS, FORM_MASS = 0, 1
@@ -450,6 +474,59 @@ def calcNodalByPrew_device(prew_ptr, u_ptr, matrix, stream=0):
 def calcPrewByNodal_device(prew_ptr, u_ptr, matrix, stream=0):
     _check(lib().lsg_calc_prew_by_nodal_device(matrix._h, ctypes.c_void_p(prew_ptr), ctypes.c_void_p(u_ptr),
                                                ctypes.c_void_p(stream)))
+
+
+# --------------------------------------------------------------------------- boundary data
+BDRHS_GRADIENT, BDRHS_MASS, BDRHS_MASS_COEFF = 0, 1, 2
+
+
+def CalcHierarchicalBasisForRHS(u, grid):
+    """CalcHierarchicalBasisForRHS(u) (MatrixVectorMultiplication/RHS.cpp:6-41),
+    in place on the host array u of the grid with boundary points `grid`: the
+    boundary values become hierarchical coefficients (interior entries are left
+    alone).  The reference's vector carries its grid; here it is passed."""
+    if u.dtype != np.float64 or not u.flags.c_contiguous or u.shape != (grid.n,):
+        raise ValueError("u must be a contiguous float64 array of the grid's length")
+    _check(lib().lsg_hierarchize_boundary(grid.d, grid.n, _ptr(grid.points), _ptr(u)))
+
+
+class InHomoBoundaryRHSHierarchical:
+    """InHomoBoundaryRHSHierarchical (MatrixVectorMultiplication/RHS.h:278-427):
+    products of the prewavelets of `matrix`'s grid with boundary data given by
+    hierarchical coefficients on `boundary_grid` (a grid with boundary points,
+    e.g. AdaptiveSparseGrid.neumann).  The reference constructs it from the
+    interior grid and reads the boundary grid from the coefficient vector."""
+
+    def __init__(self, matrix, boundary_grid):
+        self.matrix = matrix
+        self.boundary_grid = boundary_grid
+
+    def _run(self, kind, hierarchical, dirichlet):
+        bg = self.boundary_grid
+        h = np.ascontiguousarray(hierarchical, np.float64)
+        if h.shape != (bg.n,):
+            raise ValueError("hierarchical must have one value per boundary-grid point")
+        if dirichlet.dtype != np.float64 or not dirichlet.flags.c_contiguous or dirichlet.shape != (self.matrix.grid.n,):
+            raise ValueError("dirichlet must be a contiguous float64 array of the grid's length")
+        _check(lib().lsg_boundary_rhs(self.matrix._h, kind, bg.n, _ptr(bg.points), _ptr(h), _ptr(dirichlet)))
+
+    def multiply(self, hierarchical, dirichlet):
+        """RHS.cpp:697-774: dirichlet[active] = integral grad psi_i . grad g."""
+        self._run(BDRHS_GRADIENT, hierarchical, dirichlet)
+
+    def multiply_mass(self, hierarchical, dirichlet):
+        """RHS.cpp:776-852: dirichlet[active] = integral psi_i g."""
+        self._run(BDRHS_MASS, hierarchical, dirichlet)
+
+    def multiply_mass_coeff(self, hierarchical, dirichlet):
+        """RHS.cpp:854-1008: dirichlet[active] = integral psi_i g prod_k (1 - x_k^2)."""
+        self._run(BDRHS_MASS_COEFF, hierarchical, dirichlet)
+
+    def multiply_device(self, kind, hier_ptr, dirichlet_ptr, stream=0):
+        """Device form: hier (boundary-grid length) and dirichlet in device memory."""
+        bg = self.boundary_grid
+        _check(lib().lsg_boundary_rhs_device(self.matrix._h, kind, bg.n, _ptr(bg.points), ctypes.c_void_p(hier_ptr),
+                                             ctypes.c_void_p(dirichlet_ptr), ctypes.c_void_p(stream)))
 
 
 class H1:

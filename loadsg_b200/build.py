@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "liblsg.so")
 BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["lsg_device.cu", "lsg_batch.cu", "lsg_basis.cu", "lsg_mlp.cu", "lsg_plan.cpp", "lsg_grid.cpp", "lsg_gridgen.cpp"]
+SOURCES = ["lsg_device.cu", "lsg_batch.cu", "lsg_basis.cu", "lsg_bdrhs.cu", "lsg_mlp.cu", "lsg_plan.cpp", "lsg_grid.cpp", "lsg_gridgen.cpp"]
 
 
 def nvcc():

@@ -1017,6 +1017,7 @@ struct lsg_operator {
     std::vector<int64_t> level_need;  // per phase-B level: largest vector of any item
     lsg_tuning tune{256, 8, 4, 512, 12288, 256};  // launch parameters (lsg_operator_autotune)
     std::shared_ptr<void> basis;      // basis-transform tables (lsg_basis.cu), built on first use
+    std::shared_ptr<void> bdrhs;      // boundary right-hand-side tables (lsg_bdrhs.cu), built on first use
     DBuf cell_order;                  // phase-B items ordered by slab size (k_cells)
     std::vector<int32_t> cell_class_off;  // size classes in cell_order
     std::vector<int64_t> cell_class_n;    // largest N_T per class
@@ -1440,6 +1441,7 @@ int matvec64_unit(lsg_operator* op, int form, const double* x, double* y, cudaSt
     return rc;
 }
 std::shared_ptr<void>& basis_slot(lsg_operator* op) { return op->basis; }
+std::shared_ptr<void>& bdrhs_slot(lsg_operator* op) { return op->bdrhs; }
 int autotune(lsg_operator* op, int32_t precision, int32_t reps) {
     return lsg_operator_autotune(op, precision, reps, nullptr, nullptr, nullptr);
 }

@@ -167,6 +167,38 @@ void complete_without_boundary(Grid& g) {
     }
 }
 
+// completeNeumannGrid = completeGrid (sparseGrid.cc:654-740): passes over the
+// table in which every active point adds (or activates) its two same-level
+// neighbours in each dimension where its depth is > 0, boundary points
+// included, and the opposite boundary point in each dimension where its depth
+// is 0.  Only a newly added point asks for another pass, as in the reference.
+void complete_neumann(Grid& g) {
+    int d = g.d;
+    std::vector<int32_t> I(d), J(d);
+    for (bool changed = true; changed;) {
+        changed = false;
+        int64_t end = g.n();
+        for (int64_t i = 0; i < end; ++i) {
+            if (!g.act[i]) continue;
+            memcpy(I.data(), g.P(i), sizeof(int32_t) * d);
+            for (int k = 0; k < d; ++k) {
+                J = I;
+                if (I[k] > 1) {
+                    J[k] = next_left1(I[k]);
+                    changed |= g.add_active(J.data());
+                    J[k] = next_right1(I[k]);
+                    changed |= g.add_active(J.data());
+                } else {
+                    J[k] = 1;
+                    changed |= g.add_active(J.data());
+                    J[k] = 0;
+                    changed |= g.add_active(J.data());
+                }
+            }
+        }
+    }
+}
+
 // valid 1D stencil positions of an interior index i at its depth t
 // (nextFive without weights): c, c-1, c+1, c-2, c+2 in level-t coordinates
 int stencil_pos(int32_t i, int64_t* pos) {
@@ -422,6 +454,7 @@ extern "C" int lsg_grid_adaptive(int32_t d, int32_t level, int32_t refine, doubl
     // to LSG_PAIRWISE_MAX points; on every corner and plane refinement tested
     // (d = 2..6, up to 41k points) it added no point, so larger grids skip it.
     if ((mask & 32) && g.n() <= LSG_PAIRWISE_MAX) add_points2(g);
+    if (mask & 64) complete_neumann(g);
     *n = g.n();
     L.d = d; L.level = level; L.refine = refine; L.theta = theta; L.target = target; L.complete = complete;
     L.pts = g.pts;

@@ -140,3 +140,19 @@ def test_adaptive_generator_reproduces_reference(golden):
                                         kv.get("target", "corner"))
     assert np.array_equal(g.points, golden["points"])
     assert np.array_equal(g.active, golden["active"])
+
+
+@pytest.mark.parametrize("path", __import__("conftest").GOLDEN_BD,
+                         ids=lambda p: os.path.basename(p)[:-4])
+def test_neumann_generator_reproduces_reference(path):
+    """completeNeumannGrid (sgrid/sparseGrid.cc:654-740) restated in
+    lsg_gridgen.cpp: the boundary grid of every boundary-data fixture, points
+    and storage order equal to the reference's."""
+    z = np.load(path)
+    kv = dict(a.split("=") for a in str(z["gridargs"]).split())
+    g = lsg.AdaptiveSparseGrid.neumann(int(z["d"]), int(kv["level"]), int(kv.get("refine", 0)),
+                                       float(kv.get("theta", 0.5)), kv.get("target", "corner"))
+    assert np.array_equal(g.points, z["npoints"])
+    assert np.array_equal(g.active, z["nactive"])
+    assert g.boundary_mask().any() and np.all(g.coordinates()[g.points == 0] == 0.0)
+    assert np.all(g.coordinates()[g.points == 1] == 1.0)
