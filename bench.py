@@ -173,6 +173,67 @@ def cpu_reference_sample(args):
             "sample_seconds": secs, "sample_points": n, "per_dof_us": secs / n * 1e6}
 
 
+def boundary_rhs_leg(lsg, torch, stream, reference=True):
+    """Boundary-data right-hand sides (InHomoBoundaryRHSHierarchical,
+    MatrixVectorMultiplication/RHS.cpp:697-1008, and CalcHierarchicalBasisForRHS,
+    RHS.cpp:6-41) on d = 3 regular grids of level 5 and 7 with their boundary
+    grids (completeNeumannGrid), boundary data g = exp(0.3 sin(pi x0) - 0.2 x1 +
+    x2^2).  Device times (CUDA events, mean of 3 after a call that builds the
+    tables) per form, and the host-buffer call of all three forms; the
+    reference's own forms (oracle/_ref) run on level 5, the largest level it
+    finishes in seconds."""
+    out = {}
+    for L in (5, 7):
+        g = lsg.AdaptiveSparseGrid.regular(3, L)
+        ng = lsg.AdaptiveSparseGrid.neumann(3, L)
+        x = ng.coordinates()
+        b = ng.boundary_mask()
+        gv = np.where(b, np.exp(0.3 * np.sin(np.pi * x[:, 0]) - 0.2 * x[:, 1] + x[:, 2] ** 2), 0.0)
+        m = lsg.MatrixVectorHomogen(g)
+        rhs = lsg.InHomoBoundaryRHSHierarchical(m, ng)
+        t0 = time.perf_counter()
+        lsg.CalcHierarchicalBasisForRHS(gv, ng)
+        hier_ms = (time.perf_counter() - t0) * 1e3
+        y = np.zeros(g.n)
+        rhs.multiply(gv, y)  # builds the tables
+        hd = torch.tensor(gv, device="cuda")
+        yd = torch.zeros(g.n, dtype=torch.float64, device="cuda")
+        ms = []
+        for kind in (lsg.BDRHS_GRADIENT, lsg.BDRHS_MASS, lsg.BDRHS_MASS_COEFF):
+            rhs.multiply_device(kind, hd.data_ptr(), yd.data_ptr(), stream)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(3):
+                rhs.multiply_device(kind, hd.data_ptr(), yd.data_ptr(), stream)
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1) / 3)
+        t0 = time.perf_counter()
+        for meth in (rhs.multiply, rhs.multiply_mass, rhs.multiply_mass_coeff):
+            meth(gv, y)
+        e2e_ms = (time.perf_counter() - t0) * 1e3
+        out[f"d3_L{L}"] = {"points": g.n, "boundary_points": int(b.sum()), "hierarchize_host_call_ms": hier_ms,
+                           "gradient_ms": ms[0], "mass_ms": ms[1], "mass_coeff_ms": ms[2],
+                           "three_forms_host_call_ms": e2e_ms}
+        log(f"boundary rhs d=3 L{L}: {g.n} points, {int(b.sum())} boundary points, device ms {ms}")
+    exe = os.path.join(ROOT, "oracle", "_ref", "d3", "ref_harness")
+    if reference and os.path.exists(exe):
+        cores = host_cores()
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_WAIT_POLICY="PASSIVE")
+        with tempfile.TemporaryDirectory() as tmp:
+            try:
+                subprocess.run([exe, "bdrhs", tmp, "level=5", "gfam=4", "gp=1,0.5"], check=True, capture_output=True,
+                               env=env, timeout=300)
+                meta = dict(l.split()[:2] for l in open(os.path.join(tmp, "meta_bdrhs.txt")) if len(l.split()) >= 2)
+                out["reference_d3_L5"] = {"threads": cores, "gradient_s": float(meta["stiff_seconds"]),
+                                          "mass_s": float(meta["mass_seconds"]),
+                                          "mass_coeff_s": float(meta["coeff_seconds"])}
+            except (subprocess.SubprocessError, KeyError, OSError) as e:
+                out["reference_d3_L5"] = {"unavailable": str(e)[:200]}
+    return out
+
+
 def max_over_ranks(x, dist, device):
     """The slowest rank's value (replicas: the job takes as long as its slowest GPU)."""
     if dist is None:
@@ -291,6 +352,7 @@ def main():
     ap.add_argument("--workload", default="d6_adaptive_corner")
     ap.add_argument("--precond", type=int, default=2, help="0 Jacobi, 1 none, 2 learned diagonal")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-bdrhs", action="store_true", help="skip the boundary-data right-hand-side leg")
     ap.add_argument("--batch-grids", type=int, default=48, help="grids in the batch leg")
     ap.add_argument("--batch-only", action="store_true", help="run only the batch leg (one JSON line)")
     ap.add_argument("--sweep", action="store_true",
@@ -454,6 +516,9 @@ def main():
 
     batch = None if args.no_batch else guarded(lambda: batch_leg(lsg, torch, dev, stream, count=args.batch_grids),
                                                "batch leg")
+    bdrhs = None if args.no_bdrhs else guarded(
+        lambda: boundary_rhs_leg(lsg, torch, stream, reference=not args.no_cpu_baseline and world == 1 and rank == 0),
+        "boundary rhs leg")
 
     if rank != 0:
         if dist:
@@ -493,6 +558,8 @@ def main():
     }
     if batch is not None:
         line["batch"] = batch
+    if bdrhs is not None:
+        line["boundary_rhs"] = bdrhs
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line))

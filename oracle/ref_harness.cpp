@@ -403,18 +403,26 @@ int main(int argc, char **argv) {
         CalcHierarchicalBasisForRHS(gv);
         dump("g_hier.f64", get_vec(gv, NN));
         InHomoBoundaryRHSHierarchical rhs(grid);
+        auto since = [](std::chrono::steady_clock::time_point t) {
+            return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+        };
         auto t0 = std::chrono::steady_clock::now();
         yv = 0.0;
         rhs.multiply(gv, yv);
-        double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        double secs = since(t0);
         dump("y_stiff.f64", get_vec(yv, N));
         yv = 0.0;
+        t0 = std::chrono::steady_clock::now();
         rhs.multiply_mass(gv, yv);
+        double secs_mass = since(t0);
         dump("y_mass.f64", get_vec(yv, N));
         yv = 0.0;
+        t0 = std::chrono::steady_clock::now();
         rhs.multiply_mass_coeff(gv, yv);
+        double secs_coeff = since(t0);
         dump("y_coeff.f64", get_vec(yv, N));
-        g_meta << "NN " << NN << "\nstiff_seconds " << secs << "\n";
+        g_meta << "NN " << NN << "\nstiff_seconds " << secs << "\nmass_seconds " << secs_mass
+               << "\ncoeff_seconds " << secs_coeff << "\n";
     } else if (cmd == "prew2nodal" || cmd == "nodal2prew") {
         // prew2nodal: u = calcNodalByPrew(x); nodal2prew: p = calcPrewByNodal(x)
         std::vector<double> x = read_f64(opt("x", ""), N);
