@@ -65,6 +65,34 @@ public:
             AddPoint(I);
         }
     }
+    // completeNeumannGrid (sgrid/sparseGrid.cc:654-740): passes in which every
+    // active point adds (or activates) its same-level neighbours where its
+    // depth is > 0 and the opposite boundary point where it is 0; only a newly
+    // added point asks for another pass.  Adds the grid's boundary points.
+    void completeNeumannGrid() {
+        for (bool changed = true; changed;) {
+            changed = false;
+            int64_t end = getMaximalOccupiedSecondTable();
+            for (int64_t i = 0; i < end; ++i) {
+                if (!active_[i]) continue;
+                const Index I = getIndexOfTable(i);
+                for (int k = 0; k < D; ++k) {
+                    Index J = I;
+                    if (I[k] > 1) {
+                        J[k] = I[k] >> (__builtin_ctz((unsigned)I[k]) + 1);
+                        changed |= AddPoint(J);
+                        J[k] = I[k] >> (__builtin_ctz(~(unsigned)I[k]) + 1);
+                        changed |= AddPoint(J);
+                    } else {
+                        J[k] = 1;
+                        changed |= AddPoint(J);
+                        J[k] = 0;
+                        changed |= AddPoint(J);
+                    }
+                }
+            }
+        }
+    }
     int64_t getMaximalOccupiedSecondTable() const { return (int64_t)active_.size(); }
     Index getIndexOfTable(int64_t k) const {
         Index I;
@@ -88,7 +116,8 @@ private:
 template <int D>
 class VectorSparseG {
 public:
-    explicit VectorSparseG(const AdaptiveSparseGrid<D>& g) : data_(g.getMaximalOccupiedSecondTable(), 0.0) {}
+    explicit VectorSparseG(const AdaptiveSparseGrid<D>& g) : grid_(&g), data_(g.getMaximalOccupiedSecondTable(), 0.0) {}
+    const AdaptiveSparseGrid<D>* getSparseGrid() const { return grid_; }
     double getValue(int64_t k) const { return data_[k]; }
     void setValue(int64_t k, double v) { data_[k] = v; }
     double* getDatatableVector() { return data_.data(); }
@@ -97,6 +126,7 @@ public:
     void operator=(double v) { std::fill(data_.begin(), data_.end(), v); }
 
 private:
+    const AdaptiveSparseGrid<D>* grid_;
     std::vector<double> data_;
 };
 
@@ -180,5 +210,40 @@ template <int D>
 inline void calcPrewByNodal(VectorSparseG<D>& prew, const VectorSparseG<D>& u, MatrixVectorHomogen<D>& matrix) {
     check(lsg_calc_prew_by_nodal(matrix.handle(), prew.getDatatableVector(), u.getDatatableVector()));
 }
+
+// CalcHierarchicalBasisForRHS(u) (MatrixVectorMultiplication/RHS.cpp:6-41):
+// u lives on a grid with boundary points; its boundary values become
+// hierarchical coefficients.
+template <int D>
+inline void CalcHierarchicalBasisForRHS(VectorSparseG<D>& u) {
+    const AdaptiveSparseGrid<D>& g = *u.getSparseGrid();
+    check(lsg_hierarchize_boundary(D, g.getMaximalOccupiedSecondTable(), g.points(), u.getDatatableVector()));
+}
+
+// InHomoBoundaryRHSHierarchical (MatrixVectorMultiplication/RHS.h:278-427):
+// the reference is constructed from the interior grid; here from its operator.
+// The boundary grid comes with the coefficient vector, as in the reference.
+template <int D>
+class InHomoBoundaryRHSHierarchical {
+public:
+    explicit InHomoBoundaryRHSHierarchical(MatrixVectorHomogen<D>& matrix) : m_(matrix) {}
+    void multiply(const VectorSparseG<D>& hierarchical, VectorSparseG<D>& dirichlet) {
+        run(LSG_BDRHS_GRADIENT, hierarchical, dirichlet);
+    }
+    void multiply_mass(const VectorSparseG<D>& hierarchical, VectorSparseG<D>& dirichlet) {
+        run(LSG_BDRHS_MASS, hierarchical, dirichlet);
+    }
+    void multiply_mass_coeff(const VectorSparseG<D>& hierarchical, VectorSparseG<D>& dirichlet) {
+        run(LSG_BDRHS_MASS_COEFF, hierarchical, dirichlet);
+    }
+
+private:
+    void run(int32_t kind, const VectorSparseG<D>& h, VectorSparseG<D>& y) {
+        const AdaptiveSparseGrid<D>& bg = *h.getSparseGrid();
+        check(lsg_boundary_rhs(m_.handle(), kind, bg.getMaximalOccupiedSecondTable(), bg.points(),
+                               h.getDatatableVector(), y.getDatatableVector()));
+    }
+    MatrixVectorHomogen<D>& m_;
+};
 
 }  // namespace lsg

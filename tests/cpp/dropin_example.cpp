@@ -28,7 +28,25 @@ int main() {
     lsg::calcPrewByNodal<3>(back, u, m);
     double dmax = 0;
     for (int64_t k = 0; k < x.size(); ++k) dmax = std::fmax(dmax, std::fabs(back.getValue(k) - x.getValue(k)));
-    std::printf("N=%lld iterations=%d relres=%.3e transform round trip %.3e\n",
-                (long long)grid.getMaximalOccupiedSecondTable(), it, std::sqrt(rr / ff), dmax);
-    return (std::sqrt(rr / ff) < 1e-8 && dmax < 1e-10) ? 0 : 1;
+    // boundary data g = 1 (PDE_Poisson_InHomRHS::SetUp, applications/PDE.cpp):
+    // its extension is the constant 1, so the gradient form vanishes and the
+    // mass form at the root (the level-1 hat) is 2^-3
+    lsg::AdaptiveSparseGrid<3> bgrid;
+    bgrid.AddRecursiveSonsOfPoint(5);
+    bgrid.completeNeumannGrid();
+    lsg::VectorSparseG<3> g(bgrid), rhs(grid), mass(grid);
+    for (int64_t k = 0; k < bgrid.getMaximalOccupiedSecondTable(); ++k) {
+        auto I = bgrid.getIndexOfTable(k);
+        bool boundary = I[0] < 2 || I[1] < 2 || I[2] < 2;
+        g.setValue(k, boundary ? 1.0 : 0.0);
+    }
+    lsg::CalcHierarchicalBasisForRHS<3>(g);
+    lsg::InHomoBoundaryRHSHierarchical<3> bd(m);
+    bd.multiply(g, rhs);
+    bd.multiply_mass(g, mass);
+    double gmax = 0;
+    for (int64_t k = 0; k < rhs.size(); ++k) gmax = std::fmax(gmax, std::fabs(rhs.getValue(k)));
+    std::printf("N=%lld iterations=%d relres=%.3e transform round trip %.3e boundary: |grad| %.3e root mass %.6f\n",
+                (long long)grid.getMaximalOccupiedSecondTable(), it, std::sqrt(rr / ff), dmax, gmax, mass.getValue(0));
+    return (std::sqrt(rr / ff) < 1e-8 && dmax < 1e-10 && gmax < 1e-10 && mass.getValue(0) == 0.125) ? 0 : 1;
 }
