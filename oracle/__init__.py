@@ -44,6 +44,7 @@ def lib():
         L.lsgo_set_form.argtypes = [P, ctypes.c_int]
         L.lsgo_hierarchize_boundary.argtypes = [P, P]
         L.lsgo_boundary_rhs.argtypes = [P, P, ctypes.c_int, P, P]
+        L.lsgo_hierarchize.argtypes = [P, P, ctypes.c_int]
         _LIB = L
     return _LIB
 
@@ -164,6 +165,44 @@ class OracleGrid:
         if lib().lsgo_boundary_rhs(self._h, ngrid._h, kind, _ptr(hier), _ptr(y)) != 0:
             raise ValueError("oracle boundary right-hand side failed")
         return y
+
+    def hierarchize(self, u):
+        """CalcHierarchicalBasis(u) (BasisTransformations.cpp:390-409): a copy."""
+        u = np.array(u, np.float64)
+        lib().lsgo_hierarchize(self._h, _ptr(u), -1)
+        return u
+
+    def dehierarchize(self, u):
+        """CalcNodalBasis(u) (BasisTransformations.cpp:174-198): a copy."""
+        u = np.array(u, np.float64)
+        lib().lsgo_hierarchize(self._h, _ptr(u), +1)
+        return u
+
+    def pde_rhs(self, ngrid, f, g, helmholtz=False):
+        """PDE_Poisson_InHomRHS::SetUp (applications/PDE.cpp:9-52), or with
+        helmholtz PDE_Helmholtz_VariableCoeff::SetUp (PDE.h:62-114): the
+        right-hand side on this grid of -lap u (+ c u) = f, u = g on the
+        boundary, for f on every point of ngrid (a grid with boundary points)
+        and g on its boundary points.  Composed from the restated pieces;
+        the inverse transform is the dense one of prew_by_nodal (small grids)."""
+        fh = ngrid.hierarchize(f)
+        interior = (ngrid.points >= 2).all(axis=1) & (ngrid.active > 0)
+        fd = np.zeros(self.n)
+        for k in np.nonzero(interior)[0]:
+            j = self.lookup(ngrid.points[k])
+            if j >= 0:
+                fd[j] = fh[k]
+        fh[interior] = 0.0
+        fd = self.dehierarchize(fd)
+        prew = self.prew_by_nodal(fd)
+        rhs = self.matvec(0, [1.0], prew, form=1)  # HelmHoltz (Stencil.h:873-919)
+        act = self.active > 0
+        rhs[act] = rhs[act] + self.boundary_rhs(ngrid, 1, fh)[act]
+        gh = ngrid.hierarchize_boundary(g)
+        rhs[act] = rhs[act] - self.boundary_rhs(ngrid, 0, gh)[act]
+        if helmholtz:
+            rhs[act] = rhs[act] - self.boundary_rhs(ngrid, 2, gh)[act]
+        return rhs
 
     def cg(self, family, params, f, eps, maxit=500, x0=None):
         lib().lsgo_set_form(self._h, 0)

@@ -861,3 +861,14 @@ int lsgo_boundary_rhs(lsgo_grid *g, lsgo_grid *ng, int kind, const double *hier,
     free(nodal);
     return 0;
 }
+
+/* CalcHierarchicalBasis(u) (BasisTransformations.cpp:390-409) and
+ * CalcNodalBasis(u) (:174-198) over the whole grid: active points only, an
+ * absent neighbour reads 0; grids with boundary points included. */
+int lsgo_hierarchize(lsgo_grid *g, double *u, int sign) {
+    int *order = subgrid_order(g);
+    if (!order) return -1;
+    hier_sweep(g, order, u, NULL, sign < 0 ? -1 : +1);
+    free(order);
+    return 0;
+}

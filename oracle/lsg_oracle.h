@@ -59,5 +59,8 @@ int lsgo_nodal_by_prew(lsgo_grid *g, const double *prew, double *u);
  * coefficients hier (ng's storage order); other entries of y are untouched. */
 int lsgo_hierarchize_boundary(lsgo_grid *ng, double *u);
 int lsgo_boundary_rhs(lsgo_grid *g, lsgo_grid *ng, int kind, const double *hier, double *y);
+/* sign -1: CalcHierarchicalBasis(u) (BasisTransformations.cpp:390-409);
+ * sign +1: CalcNodalBasis(u) (:174-198); in place, active points only. */
+int lsgo_hierarchize(lsgo_grid *g, double *u, int sign);
 
 #endif

@@ -423,6 +423,74 @@ int main(int argc, char **argv) {
         dump("y_coeff.f64", get_vec(yv, N));
         g_meta << "NN " << NN << "\nstiff_seconds " << secs << "\nmass_seconds " << secs_mass
                << "\ncoeff_seconds " << secs_coeff << "\n";
+    } else if (cmd == "pdesetup") {
+        // Right-hand sides of problems with boundary data (applications/PDE.h,
+        // PDE.cpp): f (family ffam) on every point of the grid with boundary
+        // points, g (family gfam) on its boundary points; PDE_Poisson_InHomRHS
+        // and PDE_Helmholtz_VariableCoeff SetUp, plus the two transforms they
+        // use on their own: CalcHierarchicalBasis of f on that grid and
+        // CalcNodalBasis of x on this one (BasisTransformations.cpp:174-198,390-409).
+        AdaptiveSparseGrid ngrid;
+        build_grid(ngrid);
+        ngrid.completeNeumannGrid();
+        unsigned long NN = ngrid.getMaximalOccupiedSecondTable();
+        auto fam_vals = [&](const char *fk, const char *pk, bool boundary_only) {
+            int fam = atoi(opt(fk, "1").c_str());
+            std::vector<double> p = parse_list(opt(pk, "1,0.5,1,1,1,1,1,1,1,1"));
+            p.resize(LSG_COEF_MAXPARAM, 0.0);
+            std::vector<double> v(NN, 0.0);
+            for (unsigned long k = 0; k < NN; ++k) {
+                IndexDimension I = ngrid.getIndexOfTable(k);
+                double x[D];
+                bool boundary = false;
+                for (int d = 0; d < D; ++d) {
+                    x[d] = I.coordinate(d);
+                    if (I.getIndex(d) < 2) boundary = true;
+                }
+                if (boundary || !boundary_only) v[k] = lsg_coef_eval(fam, p.data(), D, x);
+            }
+            return v;
+        };
+        std::vector<double> f = fam_vals("ffam", "fp", false), g = fam_vals("gfam", "gp", true);
+        std::vector<int32_t> nidx(NN * D);
+        std::vector<uint8_t> nact(NN);
+        for (unsigned long k = 0; k < NN; ++k) {
+            IndexDimension I = ngrid.getIndexOfTable(k);
+            for (int d = 0; d < D; ++d) nidx[k * D + d] = I.getIndex(d);
+            nact[k] = ngrid.getActiveTable()[k] ? 1 : 0;
+        }
+        dump("npoints.i32", nidx);
+        dump("nactive.u8", nact);
+        dump("f.f64", f);
+        dump("g.f64", g);
+        VectorSparseG fh(ngrid);
+        set_vec(fh, f);
+        CalcHierarchicalBasis(fh);
+        dump("f_hier.f64", get_vec(fh, NN));
+        std::vector<double> x = read_f64(opt("x", ""), N);
+        VectorSparseG xv(grid);
+        set_vec(xv, x);
+        CalcNodalBasis(xv);
+        dump("x_nodal.f64", get_vec(xv, N));
+        MultiLevelAdaptiveSparseGrid mgrid(&grid);
+        MatrixVectorHomogen m(grid, mgrid, true, false);
+        for (int which = 0; which < 2; ++which) {
+            VectorSparseG fv(ngrid), gv(ngrid);
+            set_vec(fv, f);
+            set_vec(gv, g);
+            std::vector<double> rhs;
+            if (which == 0) {
+                PDE_Poisson_InHomRHS pde(ngrid, grid, m);
+                pde.SetUp(fv, gv);
+                rhs = get_vec(pde.getRHS(), N);
+            } else {
+                PDE_Helmholtz_VariableCoeff pde(ngrid, grid, m);
+                pde.SetUp(fv, gv);
+                rhs = get_vec(pde.getRHS(), N);
+            }
+            dump(which == 0 ? "rhs_poisson.f64" : "rhs_helmholtz.f64", rhs);
+        }
+        g_meta << "NN " << NN << "\n";
     } else if (cmd == "prew2nodal" || cmd == "nodal2prew") {
         // prew2nodal: u = calcNodalByPrew(x); nodal2prew: p = calcPrewByNodal(x)
         std::vector<double> x = read_f64(opt("x", ""), N);

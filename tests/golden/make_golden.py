@@ -11,6 +11,7 @@ reference.
     python tests/golden/make_golden.py --cmds prew2nodal,nodal2prew   # add commands to existing fixtures
 
     python tests/golden/make_golden.py --bd        # boundary-data right-hand sides -> bd_<name>.npz
+    python tests/golden/make_golden.py --pde       # PDE_*::SetUp right-hand sides -> pde_<name>.npz
 
 prew2nodal / nodal2prew run calcNodalByPrew / calcPrewByNodal on the fixture's
 x (BasisTransformations/BasisTransformations.cpp:486-545,670-706); mass /
@@ -21,7 +22,12 @@ The bd_ fixtures hold a second grid with boundary points (the same build,
 then completeNeumannGrid), boundary values g of a coefficient family, g after
 CalcHierarchicalBasisForRHS, and InHomoBoundaryRHSHierarchical's multiply /
 multiply_mass / multiply_mass_coeff onto the first grid
-(MatrixVectorMultiplication/RHS.cpp:6-41,697-1008).
+(MatrixVectorMultiplication/RHS.cpp:6-41,697-1008).  The pde_ fixtures
+hold f on every point and g on the boundary points of that second grid, the
+right-hand sides of PDE_Poisson_InHomRHS::SetUp and
+PDE_Helmholtz_VariableCoeff::SetUp (applications/PDE.cpp, PDE.h), and the
+transforms they use: CalcHierarchicalBasis of f on the second grid and
+CalcNodalBasis of x on the first (BasisTransformations.cpp:174-198,390-409).
 """
 import argparse
 import os
@@ -68,6 +74,16 @@ BD_CASES = [
     ("bd_d4_L3", 4, "level=3", EXPSIN6),
     ("bd_d5_L2", 5, "level=2", SIN2PI),
     ("bd_d6_L2", 6, "level=2", EXPSIN6),
+]
+
+
+# right-hand sides of problems with boundary data (PDE_Poisson_InHomRHS,
+# PDE_Helmholtz_VariableCoeff): name, d, grid args, f family, g family
+PDE_CASES = [
+    ("pde_d2_L4", 2, "level=4", SIN2PI, EXPSIN6),
+    ("pde_d2_adapt", 2, "level=2 refine=2 theta=0.6 target=corner", EXPSIN6, SIN2PI),
+    ("pde_d3_L3", 3, "level=3", EXPSIN6, SIN2PI),
+    ("pde_d4_L2", 4, "level=2", SIN2PI, EXPSIN6),
 ]
 
 
@@ -192,13 +208,42 @@ def make_bd_case(name, d, gridargs, gcoef, refsrc):
     print(f"{name}: N={len(out['active'])} NN={len(out['nactive'])} -> {os.path.getsize(path)} bytes")
 
 
+def make_pde_case(name, d, gridargs, fcoef, gcoef, refsrc):
+    run(["make", "-s", "-C", ORACLE, "ref", f"D={d}", f"REFSRC={refsrc}", "-j8"])
+    exe = os.path.join(ORACLE, "_ref", f"d{d}", "ref_harness")
+    lst = lambda c: ",".join(repr(float(p)) for p in c[1])
+    args = gridargs.split() + [f"ffam={fcoef[0]}", "fp=" + lst(fcoef), f"gfam={gcoef[0]}", "gp=" + lst(gcoef)]
+    out = {"d": np.int32(d), "gridargs": np.array(gridargs)}
+    with tempfile.TemporaryDirectory() as tmp:
+        run([exe, "grid", tmp] + args)
+        meta, arrs = read_meta(os.path.join(tmp, "meta_grid.txt"))
+        out.update(load_arrays(tmp, arrs, ""))
+        x = np.random.default_rng(sum(map(ord, name))).uniform(-1.0, 1.0, int(meta["N"]))
+        x.tofile(os.path.join(tmp, "x_in.f64"))
+        out["x"] = x
+        run([exe, "pdesetup", tmp] + args + [f"x={tmp}/x_in.f64"])
+        meta, arrs = read_meta(os.path.join(tmp, "meta_pdesetup.txt"))
+        out.update(load_arrays(tmp, arrs, ""))
+    out["npoints"] = out["npoints"].reshape(-1, d)
+    out["points"] = out["points"].reshape(-1, d)
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"{name}: N={len(out['active'])} NN={len(out['nactive'])} -> {os.path.getsize(path)} bytes")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--refsrc", default="/root/reference/library/source")
     ap.add_argument("--only", default=None)
     ap.add_argument("--cmds", default=None, help="comma list: add these commands to existing fixtures")
     ap.add_argument("--bd", action="store_true", help="the boundary-data right-hand-side fixtures")
+    ap.add_argument("--pde", action="store_true", help="the PDE right-hand-side (SetUp) fixtures")
     a = ap.parse_args()
+    if a.pde:
+        for case in PDE_CASES:
+            if not a.only or case[0] == a.only:
+                make_pde_case(*case, refsrc=a.refsrc)
+        return
     if a.bd:
         for case in BD_CASES:
             if not a.only or case[0] == a.only:

@@ -73,3 +73,32 @@ def test_missing_parent_is_an_error():
     ng = OracleGrid(pts[keep], act[keep])
     with pytest.raises(ValueError):
         ng.hierarchize_boundary(np.ones(keep.sum()))
+
+
+# ---------------------------------------------------------------- PDE_*::SetUp
+from conftest import GOLDEN_PDE  # noqa: E402
+
+
+@pytest.fixture(params=GOLDEN_PDE, ids=[os.path.basename(p)[:-4] for p in GOLDEN_PDE])
+def pde(request):
+    z = np.load(request.param)
+    return {k: z[k] for k in z.files}
+
+
+def test_transforms_bit_exact(pde):
+    """CalcHierarchicalBasis on the grid with boundary points and CalcNodalBasis
+    on the interior grid (BasisTransformations.cpp:174-198,390-409)."""
+    g, ng = grids(pde)
+    assert np.array_equal(ng.hierarchize(pde["f"]), pde["f_hier"])
+    assert np.array_equal(g.dehierarchize(pde["x"]), pde["x_nodal"])
+
+
+@pytest.mark.parametrize("helmholtz", [False, True], ids=["poisson", "helmholtz"])
+def test_pde_setup_rhs(pde, helmholtz):
+    """PDE_Poisson_InHomRHS::SetUp / PDE_Helmholtz_VariableCoeff::SetUp
+    composed from the oracle's pieces: 1e-14 relative to the reference (the
+    inverse basis transform is a dense solve here)."""
+    g, ng = grids(pde)
+    y = g.pde_rhs(ng, pde["f"], pde["g"], helmholtz=helmholtz)
+    ref = pde["rhs_helmholtz" if helmholtz else "rhs_poisson"]
+    assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max()
