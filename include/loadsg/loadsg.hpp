@@ -246,4 +246,43 @@ private:
     MatrixVectorHomogen<D>& m_;
 };
 
+// CalcHierarchicalBasis(u) / CalcNodalBasis(u)
+// (BasisTransformations/BasisTransformations.cpp:390-409, :174-198) on the
+// vector's own grid, boundary points allowed.
+template <int D>
+inline void CalcHierarchicalBasis(VectorSparseG<D>& u) {
+    const AdaptiveSparseGrid<D>& g = *u.getSparseGrid();
+    check(lsg_hierarchize(D, g.getMaximalOccupiedSecondTable(), g.points(), g.getActiveTable(), u.getDatatableVector()));
+}
+template <int D>
+inline void CalcNodalBasis(VectorSparseG<D>& u) {
+    const AdaptiveSparseGrid<D>& g = *u.getSparseGrid();
+    check(lsg_dehierarchize(D, g.getMaximalOccupiedSecondTable(), g.points(), g.getActiveTable(), u.getDatatableVector()));
+}
+
+// PDE_Poisson_InHomRHS / PDE_Helmholtz_VariableCoeff (applications/PDE.h,
+// PDE.cpp): the right-hand side on the interior grid of a problem with
+// boundary data; SetUp transforms f and g in place as the reference does.
+template <int D, int32_t KIND>
+class PDE_InHomRHS {
+public:
+    PDE_InHomRHS(AdaptiveSparseGrid<D>& n_grid, AdaptiveSparseGrid<D>& d_grid, MatrixVectorHomogen<D>& matrix)
+        : ngrid_(n_grid), f_dirichlet_(d_grid), matrix_(matrix) {}
+    void SetUp(VectorSparseG<D>& f_neumann, VectorSparseG<D>& g_neumann) {
+        check(lsg_pde_boundary_rhs(matrix_.handle(), KIND, ngrid_.getMaximalOccupiedSecondTable(), ngrid_.points(),
+                                   ngrid_.getActiveTable(), f_neumann.getDatatableVector(),
+                                   g_neumann.getDatatableVector(), f_dirichlet_.getDatatableVector()));
+    }
+    VectorSparseG<D>& getRHS() { return f_dirichlet_; }
+
+private:
+    AdaptiveSparseGrid<D>& ngrid_;
+    VectorSparseG<D> f_dirichlet_;
+    MatrixVectorHomogen<D>& matrix_;
+};
+template <int D>
+using PDE_Poisson_InHomRHS = PDE_InHomRHS<D, LSG_PDE_POISSON>;
+template <int D>
+using PDE_Helmholtz_VariableCoeff = PDE_InHomRHS<D, LSG_PDE_HELMHOLTZ>;
+
 }  // namespace lsg

@@ -235,6 +235,28 @@ int lsg_boundary_rhs(lsg_operator *op, int32_t kind, int64_t nn, const int32_t *
 int lsg_boundary_rhs_device(lsg_operator *op, int32_t kind, int64_t nn, const int32_t *points, const double *hier,
                             double *rhs, void *stream);
 
+/* CalcHierarchicalBasis(u) / CalcNodalBasis(u) (BasisTransformations/
+ * BasisTransformations.cpp:390-409, :174-198) on any grid, boundary points
+ * included: in place on u (n host doubles in storage order), dimension by
+ * dimension; active points only, an absent 1D neighbour reads 0. */
+int lsg_hierarchize(int32_t d, int64_t n, const int32_t *points, const uint8_t *active, double *u);
+int lsg_dehierarchize(int32_t d, int64_t n, const int32_t *points, const uint8_t *active, double *u);
+
+/* Right-hand side of -lap u = f (LSG_PDE_POISSON, PDE_Poisson_InHomRHS::SetUp,
+ * applications/PDE.cpp:9-52) or -lap u + c u = f with c = prod_k (1 - x_k^2)
+ * (LSG_PDE_HELMHOLTZ, PDE_Helmholtz_VariableCoeff::SetUp, PDE.h:62-114),
+ * u = g on the boundary, on the operator's grid: rhs = <f_inner, psi_i> +
+ * <f_boundary, psi_i> - <grad g, grad psi_i> (- <c g, psi_i>).  f holds values
+ * at every point, g at the boundary points of the grid with boundary points
+ * (nn points, nn x d 1D indices, its active flags); rhs gets n values (0 at
+ * hanging points).  As in the reference, f and g are transformed in place:
+ * f to hierarchical coefficients with its interior entries moved out (0), g
+ * to hierarchical boundary coefficients.  Host arrays; no coefficient needed. */
+#define LSG_PDE_POISSON 0
+#define LSG_PDE_HELMHOLTZ 1
+int lsg_pde_boundary_rhs(lsg_operator *op, int32_t kind, int64_t nn, const int32_t *npoints, const uint8_t *nactive,
+                         double *f, double *g, double *rhs);
+
 /* ---- launch parameters of the matvec and the autotuner that picks them.
  * The defaults suit large d=5/6 grids; lsg_operator_autotune times matvecs of
  * this operator over a candidate set per parameter (coordinate descent, two

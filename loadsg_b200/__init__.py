@@ -128,6 +128,9 @@ def lib():
             "lsg_hierarchize_boundary": (ctypes.c_int, [I32, I64, P, P]),
             "lsg_boundary_rhs": (ctypes.c_int, [P, I32, I64, P, P, P]),
             "lsg_boundary_rhs_device": (ctypes.c_int, [P, I32, I64, P, P, P, P]),
+            "lsg_hierarchize": (ctypes.c_int, [I32, I64, P, P, P]),
+            "lsg_dehierarchize": (ctypes.c_int, [I32, I64, P, P, P]),
+            "lsg_pde_boundary_rhs": (ctypes.c_int, [P, I32, I64, P, P, P, P, P]),
             "lsg_h1_norm": (ctypes.c_int, [P, P, P]),
             "lsg_l2_norm": (ctypes.c_int, [P, P, P]),
             "lsg_calc_nodal_by_prew": (ctypes.c_int, [P, P, P]),
@@ -527,6 +530,64 @@ class InHomoBoundaryRHSHierarchical:
         bg = self.boundary_grid
         _check(lib().lsg_boundary_rhs_device(self.matrix._h, kind, bg.n, _ptr(bg.points), ctypes.c_void_p(hier_ptr),
                                              ctypes.c_void_p(dirichlet_ptr), ctypes.c_void_p(stream)))
+
+
+def _grid_vector(u, grid):
+    if u.dtype != np.float64 or not u.flags.c_contiguous or u.shape != (grid.n,):
+        raise ValueError("u must be a contiguous float64 array of the grid's length")
+
+
+def CalcHierarchicalBasis(u, grid):
+    """CalcHierarchicalBasis(u) (BasisTransformations/BasisTransformations.cpp:390-409)
+    in place on the host array u of `grid` (boundary points allowed): nodal
+    values to hierarchical coefficients at the active points."""
+    _grid_vector(u, grid)
+    _check(lib().lsg_hierarchize(grid.d, grid.n, _ptr(grid.points), _ptr(grid.active), _ptr(u)))
+
+
+def CalcNodalBasis(u, grid):
+    """CalcNodalBasis(u) (BasisTransformations.cpp:174-198): the inverse of
+    CalcHierarchicalBasis, in place."""
+    _grid_vector(u, grid)
+    _check(lib().lsg_dehierarchize(grid.d, grid.n, _ptr(grid.points), _ptr(grid.active), _ptr(u)))
+
+
+PDE_POISSON, PDE_HELMHOLTZ = 0, 1
+
+
+class PDE_Poisson_InHomRHS:
+    """PDE_Poisson_InHomRHS (applications/PDE.h:16-31, PDE.cpp:9-52): the
+    right-hand side on the interior grid of -lap u = f with u = g on the
+    boundary, reduced to zero boundary values.  neumann_grid holds boundary
+    points (AdaptiveSparseGrid.neumann), dirichlet_grid is the grid of
+    `matrix`.  SetUp(f_neumann, g_neumann) takes f at every point and g at the
+    boundary points of neumann_grid (host arrays, transformed in place as in
+    the reference); getRHS() returns the right-hand side (0 at hanging points)."""
+
+    kind = PDE_POISSON
+
+    def __init__(self, neumann_grid, dirichlet_grid, matrix):
+        if dirichlet_grid.n != matrix.grid.n or dirichlet_grid.d != neumann_grid.d:
+            raise ValueError("dirichlet_grid must be the grid of matrix, of the same dimension as neumann_grid")
+        self.neumann_grid, self.dirichlet_grid, self.matrix = neumann_grid, dirichlet_grid, matrix
+        self.f_dirichlet = np.zeros(dirichlet_grid.n)
+
+    def SetUp(self, f_neumann, g_neumann):
+        ng = self.neumann_grid
+        _grid_vector(f_neumann, ng)
+        _grid_vector(g_neumann, ng)
+        _check(lib().lsg_pde_boundary_rhs(self.matrix._h, self.kind, ng.n, _ptr(ng.points), _ptr(ng.active),
+                                          _ptr(f_neumann), _ptr(g_neumann), _ptr(self.f_dirichlet)))
+
+    def getRHS(self):
+        return self.f_dirichlet
+
+
+class PDE_Helmholtz_VariableCoeff(PDE_Poisson_InHomRHS):
+    """PDE_Helmholtz_VariableCoeff (applications/PDE.h:47-120): -lap u + c u = f
+    with c(x) = prod_k (1 - x_k^2) and u = g on the boundary."""
+
+    kind = PDE_HELMHOLTZ
 
 
 class H1:

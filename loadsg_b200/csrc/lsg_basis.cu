@@ -392,6 +392,12 @@ int host_call(lsg_operator* op, const double* in, double* out, bool to_nodal) {
 
 }  // namespace
 
+namespace lsg_internal {
+int prew_by_nodal_dev(lsg_operator* op, double* prew, const double* u, cudaStream_t st) {
+    return prew_by_nodal(op, prew, u, st);
+}
+}  // namespace lsg_internal
+
 extern "C" {
 
 int lsg_calc_nodal_by_prew_device(lsg_operator* op, const double* prew, double* u, void* stream) {

@@ -59,6 +59,7 @@ struct DevArr {
     DevArr() = default;
     DevArr(const DevArr&) = delete;
     DevArr& operator=(const DevArr&) = delete;
+    DevArr(DevArr&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
     ~DevArr() { if (p) cudaFree(p); }
     int alloc(size_t b) {
         if (p) { cudaFree(p); p = nullptr; }
@@ -290,14 +291,6 @@ __global__ void k_gather(int64_t n, const int64_t* __restrict__ idx, const doubl
     if (i < n) dst[i] = src[idx[i]];
 }
 
-// CalcHierarchicalBasisForRHS, one (dimension, depth) step: u[k] -= (u[l] + u[r]) / 2
-__global__ void k_bd_hier(int64_t n, const int64_t* __restrict__ klr, double* __restrict__ u) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int64_t k = klr[3 * i], l = klr[3 * i + 1], r = klr[3 * i + 2];
-    u[k] = S(u[k], M(0.5, A(u[l], u[r])));
-}
-
 // ------------------------------------------------------------------ per-operator tables
 struct BdState {
     int d = 0;
@@ -472,60 +465,152 @@ int check_points(int d, int64_t nn, const int32_t* pts) {
     return 0;
 }
 
-}  // namespace
+// (De)hierarchization sweeps: per dimension, one (point, left, right) list per
+// depth in that dimension, finest first (hierarchization) or coarsest first
+// (dehierarchization).  Points of equal depth in a dimension never read each
+// other there, so each list is one launch.
+//   kBoundary: the boundary points, each needs both 1D parents
+//              (CalcHierarchicalBasisForRHS, RHS.cpp:6-41);
+//   kActive:   the active points, an absent neighbour reads 0 (the expression
+//              assignments of CalcHierarchicalBasis / CalcNodalBasis,
+//              BasisTransformations.cpp:174-198,390-409).
+enum class SweepSet { kBoundary, kActive };
 
-extern "C" {
-
-int lsg_hierarchize_boundary(int32_t d, int64_t nn, const int32_t* points, double* u) {
-    if (d < 1 || d > lsg::kMaxDim || nn < 0 || (nn > 0 && (!points || !u)))
-        return fail_msg(LSG_E_INVALID, "bad argument");
-    if (nn == 0) return 0;
-    int rc = check_points(d, nn, points);
-    if (rc) return rc;
+int build_sweeps(int d, int64_t n, const int32_t* pts, const uint8_t* act, SweepSet set, bool fine_first,
+                 std::vector<std::vector<int64_t>>& steps) {
     PointMap pm;
-    pm.build(d, points, nn);
+    pm.build(d, pts, n);
     std::vector<int32_t> J(d);
-    // per dimension, per depth from the finest: (point, left parent, right parent)
-    std::vector<std::vector<int64_t>> steps;
     for (int q = 0; q < d; ++q) {
         int maxt = 0;
-        for (int64_t k = 0; k < nn; ++k) maxt = std::max(maxt, h_depth1(points[k * d + q]));
-        for (int t = maxt; t >= 1; --t) {
+        for (int64_t k = 0; k < n; ++k) maxt = std::max(maxt, h_depth1(pts[k * d + q]));
+        for (int s = 0; s < maxt; ++s) {
+            const int t = fine_first ? maxt - s : s + 1;
             std::vector<int64_t> klr;
-            for (int64_t k = 0; k < nn; ++k) {
-                const int32_t* I = points + k * d;
-                bool boundary = false;
-                for (int j = 0; j < d; ++j) boundary |= I[j] < 2;
-                if (!boundary || h_depth1(I[q]) != t) continue;
+            for (int64_t k = 0; k < n; ++k) {
+                const int32_t* I = pts + k * d;
+                if (h_depth1(I[q]) != t) continue;
+                if (set == SweepSet::kBoundary) {
+                    bool boundary = false;
+                    for (int j = 0; j < d; ++j) boundary |= I[j] < 2;
+                    if (!boundary) continue;
+                } else if (!act[k]) {
+                    continue;
+                }
                 memcpy(J.data(), I, d * sizeof(int32_t));
                 J[q] = h_left1(I[q]);
                 int64_t l = pm.find(J.data());
                 J[q] = h_right1(I[q]);
                 int64_t r = pm.find(J.data());
-                if (l < 0 || r < 0) return fail_msg(LSG_E_INVALID, "a boundary point lacks a 1D parent in the grid");
+                if (set == SweepSet::kBoundary && (l < 0 || r < 0))
+                    return fail_msg(LSG_E_INVALID, "a boundary point lacks a 1D parent in the grid");
                 klr.insert(klr.end(), {k, l, r});
             }
             if (!klr.empty()) steps.push_back(std::move(klr));
         }
     }
+    return 0;
+}
+
+// u[k] -/+= (u[l] + u[r]) / 2 over one list; an absent neighbour reads 0
+__global__ void k_bd_sweep(int64_t n, const int64_t* __restrict__ klr, double* __restrict__ u, int sign) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t k = klr[3 * i], l = klr[3 * i + 1], r = klr[3 * i + 2];
+    double s = M(0.5, A(l >= 0 ? u[l] : 0.0, r >= 0 ? u[r] : 0.0));
+    u[k] = sign < 0 ? S(u[k], s) : A(u[k], s);
+}
+
+// tables: one device list per step, owned by the caller until the stream is done
+int run_sweeps(const std::vector<std::vector<int64_t>>& steps, double* u, int sign, std::vector<DevArr>& tables,
+               cudaStream_t st) {
+    size_t base = tables.size();
+    tables.resize(base + steps.size());
+    for (size_t i = 0; i < steps.size(); ++i) {
+        int rc = tables[base + i].upload(steps[i], st);
+        if (rc) return rc;
+        int64_t n = (int64_t)steps[i].size() / 3;
+        k_bd_sweep<<<nblk(n), 256, 0, st>>>(n, tables[base + i].as<int64_t>(), u, sign);
+    }
+    BD_TRY(cudaGetLastError());
+    return 0;
+}
+
+// boundary points of a grid in the reference's summation order, their 1D
+// indices dimension-major, and the gather of a coefficient vector into that order
+struct BoundarySet {
+    int64_t nb = 0;
+    DevArr dq, di;
+    int build(int d, int64_t nn, const int32_t* pts, cudaStream_t st) {
+        std::vector<int64_t> b = boundary_order(d, nn, pts);
+        nb = (int64_t)b.size();
+        std::vector<int32_t> bq((size_t)nb * d);
+        for (int64_t i = 0; i < nb; ++i)
+            for (int q = 0; q < d; ++q) bq[(size_t)q * nb + i] = pts[b[i] * d + q];
+        int rc = dq.upload(bq, st);
+        rc = rc ? rc : di.upload(b, st);
+        if (rc) return rc;
+        BD_TRY(cudaStreamSynchronize(st));  // the host vectors go out of scope
+        return 0;
+    }
+    void gather(const double* src, double* dst, cudaStream_t st) const {
+        if (nb > 0) k_gather<<<nblk(nb), 256, 0, st>>>(nb, di.as<int64_t>(), src, dst);
+    }
+};
+
+__global__ void k_split_interior(int64_t n, const int64_t* __restrict__ kj, double* __restrict__ f,
+                                 double* __restrict__ fd) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t k = kj[2 * i], j = kj[2 * i + 1];
+    if (j >= 0) fd[j] = f[k];
+    f[k] = 0.0;
+}
+
+__global__ void k_add_active(int64_t n, const uint8_t* __restrict__ act, double* __restrict__ y,
+                             const double* __restrict__ x, int sign) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n && act[i]) y[i] = sign < 0 ? S(y[i], x[i]) : A(y[i], x[i]);
+}
+
+int hierarchize_host(int32_t d, int64_t n, const int32_t* points, const uint8_t* active, double* u, SweepSet set,
+                     int sign) {
+    if (d < 1 || d > lsg::kMaxDim || n < 0 || (n > 0 && (!points || !u || (set == SweepSet::kActive && !active))))
+        return fail_msg(LSG_E_INVALID, "bad argument");
+    if (n == 0) return 0;
+    int rc = check_points(d, n, points);
+    if (rc) return rc;
+    std::vector<std::vector<int64_t>> steps;
+    rc = build_sweeps(d, n, points, active, set, sign < 0, steps);
+    if (rc) return rc;
     cudaStream_t st;
     BD_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     struct Guard { cudaStream_t s; ~Guard() { cudaStreamDestroy(s); } } guard{st};
     DevArr du;
-    std::vector<double> hu(u, u + nn);
+    std::vector<double> hu(u, u + n);
+    std::vector<DevArr> tables;
     rc = du.upload(hu, st);
+    rc = rc ? rc : run_sweeps(steps, du.as<double>(), sign, tables, st);
     if (rc) return rc;
-    std::vector<DevArr> tables(steps.size());
-    for (size_t i = 0; i < steps.size(); ++i) {
-        rc = tables[i].upload(steps[i], st);
-        if (rc) return rc;
-        int64_t n = (int64_t)steps[i].size() / 3;
-        k_bd_hier<<<nblk(n), 256, 0, st>>>(n, tables[i].as<int64_t>(), du.as<double>());
-    }
-    BD_TRY(cudaGetLastError());
-    BD_TRY(cudaMemcpyAsync(u, du.p, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BD_TRY(cudaMemcpyAsync(u, du.p, n * sizeof(double), cudaMemcpyDeviceToHost, st));
     BD_TRY(cudaStreamSynchronize(st));
     return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lsg_hierarchize_boundary(int32_t d, int64_t nn, const int32_t* points, double* u) {
+    return hierarchize_host(d, nn, points, nullptr, u, SweepSet::kBoundary, -1);
+}
+
+int lsg_hierarchize(int32_t d, int64_t n, const int32_t* points, const uint8_t* active, double* u) {
+    return hierarchize_host(d, n, points, active, u, SweepSet::kActive, -1);
+}
+
+int lsg_dehierarchize(int32_t d, int64_t n, const int32_t* points, const uint8_t* active, double* u) {
+    return hierarchize_host(d, n, points, active, u, SweepSet::kActive, +1);
 }
 
 int lsg_boundary_rhs_device(lsg_operator* op, int32_t kind, int64_t nn, const int32_t* points, const double* hier,
@@ -536,18 +621,11 @@ int lsg_boundary_rhs_device(lsg_operator* op, int32_t kind, int64_t nn, const in
     int rc = check_points(d, nn, points);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    std::vector<int64_t> b = boundary_order(d, nn, points);
-    const int64_t nb = (int64_t)b.size();
-    std::vector<int32_t> bq((size_t)nb * d);
-    std::vector<int64_t> bi(b);
-    for (int64_t i = 0; i < nb; ++i)
-        for (int q = 0; q < d; ++q) bq[(size_t)q * nb + i] = points[b[i] * d + q];
-    DevArr dq, di, dh;
-    if ((rc = dq.upload(bq, st)) || (rc = di.upload(bi, st)) || (rc = dh.alloc(std::max<int64_t>(nb, 1) * 8)))
-        return rc;
-    // the coefficients of the boundary points, in boundary order
-    if (nb > 0) k_gather<<<nblk(nb), 256, 0, st>>>(nb, di.as<int64_t>(), hier, dh.as<double>());
-    rc = boundary_rhs_run(op, kind, nb, dq.as<int32_t>(), dh.as<double>(), rhs, st);
+    BoundarySet B;
+    DevArr dh;
+    if ((rc = B.build(d, nn, points, st)) || (rc = dh.alloc(std::max<int64_t>(B.nb, 1) * 8))) return rc;
+    B.gather(hier, dh.as<double>(), st);
+    rc = boundary_rhs_run(op, kind, B.nb, B.dq.as<int32_t>(), dh.as<double>(), rhs, st);
     if (rc) return rc;
     BD_TRY(cudaStreamSynchronize(st));  // the device tables go out of scope
     return 0;
@@ -564,6 +642,81 @@ int lsg_boundary_rhs(lsg_operator* op, int32_t kind, int64_t nn, const int32_t* 
     rc = lsg_boundary_rhs_device(op, kind, nn, points, dh.as<double>(), dr.as<double>(), nullptr);
     if (rc) return rc;
     BD_TRY(cudaMemcpy(rhs, dr.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int lsg_pde_boundary_rhs(lsg_operator* op, int32_t kind, int64_t nn, const int32_t* npoints, const uint8_t* nactive,
+                         double* f, double* g, double* rhs) {
+    if (!op || nn < 1 || !npoints || !nactive || !f || !g || !rhs) return fail_msg(LSG_E_INVALID, "null argument");
+    if (kind != LSG_PDE_POISSON && kind != LSG_PDE_HELMHOLTZ) return fail_msg(LSG_E_INVALID, "bad kind");
+    const lsg::Plan& P = lsg_internal::plan(op);
+    if (P.inst_n_off.size() != 2) return fail_msg(LSG_E_INVALID, "boundary right-hand sides take a single-grid operator");
+    const int d = P.d;
+    const int64_t n = P.n;
+    int rc = check_points(d, nn, npoints);
+    if (rc) return rc;
+    // host tables: the three sweeps and the interior points shared by both grids
+    std::vector<std::vector<int64_t>> sw_f, sw_fd, sw_g;
+    if ((rc = build_sweeps(d, nn, npoints, nactive, SweepSet::kActive, true, sw_f)) ||
+        (rc = build_sweeps(d, n, P.pts.data(), P.act.data(), SweepSet::kActive, false, sw_fd)) ||
+        (rc = build_sweeps(d, nn, npoints, nullptr, SweepSet::kBoundary, true, sw_g)))
+        return rc;
+    PointMap pm;
+    pm.build(d, P.pts.data(), n);
+    std::vector<int64_t> kj;
+    for (int64_t k = 0; k < nn; ++k) {
+        const int32_t* I = npoints + k * d;
+        bool interior = nactive[k] != 0;
+        for (int q = 0; q < d; ++q) interior &= I[q] >= 2;
+        if (interior) kj.insert(kj.end(), {k, pm.find(I)});
+    }
+    cudaStream_t st;
+    BD_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct Guard { cudaStream_t s; ~Guard() { cudaStreamDestroy(s); } } guard{st};
+    BoundarySet B;
+    DevArr df, dg, dfd, dprew, drhs, dy, dbh, dkj;
+    std::vector<DevArr> tables;
+    std::vector<double> hf(f, f + nn), hg(g, g + nn);
+    if ((rc = B.build(d, nn, npoints, st)) || (rc = df.upload(hf, st)) || (rc = dg.upload(hg, st)) ||
+        (rc = dkj.upload(kj, st)) || (rc = dfd.alloc(n * 8)) || (rc = dprew.alloc(n * 8)) ||
+        (rc = drhs.alloc(n * 8)) || (rc = dy.alloc(n * 8)) || (rc = dbh.alloc(std::max<int64_t>(B.nb, 1) * 8)))
+        return rc;
+    double *F = df.as<double>(), *G = dg.as<double>(), *FD = dfd.as<double>(), *R = drhs.as<double>(),
+           *Y = dy.as<double>();
+    const uint8_t* act = lsg_internal::active(op);
+    // f in the hierarchical basis of the boundary grid; its interior part moves
+    // to this grid and back to nodal values (PDE.cpp:12-33)
+    BD_TRY(cudaMemsetAsync(FD, 0, n * 8, st));
+    if ((rc = run_sweeps(sw_f, F, -1, tables, st))) return rc;
+    int64_t nkj = (int64_t)kj.size() / 2;
+    if (nkj > 0) k_split_interior<<<nblk(nkj), 256, 0, st>>>(nkj, dkj.as<int64_t>(), F, FD);
+    if ((rc = run_sweeps(sw_fd, FD, +1, tables, st))) return rc;
+    // <f_inner, psi_i>: prewavelet coefficients, then the coefficient-1 mass product (HelmHoltz)
+    if ((rc = lsg_internal::prew_by_nodal_dev(op, dprew.as<double>(), FD, st))) return rc;
+    BD_TRY(cudaMemsetAsync(R, 0, n * 8, st));
+    if ((rc = lsg_internal::matvec64_unit(op, LSG_FORM_MASS, dprew.as<double>(), R, st))) return rc;
+    // + <f_boundary, psi_i> (multiply_mass of the boundary coefficients of f)
+    B.gather(F, dbh.as<double>(), st);
+    BD_TRY(cudaMemsetAsync(Y, 0, n * 8, st));
+    if ((rc = boundary_rhs_run(op, LSG_BDRHS_MASS, B.nb, B.dq.as<int32_t>(), dbh.as<double>(), Y, st))) return rc;
+    k_add_active<<<nblk(n), 256, 0, st>>>(n, act, R, Y, +1);
+    // - <grad g, grad psi_i> (- <c g, psi_i> for the Helmholtz problem)
+    if ((rc = run_sweeps(sw_g, G, -1, tables, st))) return rc;
+    B.gather(G, dbh.as<double>(), st);
+    BD_TRY(cudaMemsetAsync(Y, 0, n * 8, st));
+    if ((rc = boundary_rhs_run(op, LSG_BDRHS_GRADIENT, B.nb, B.dq.as<int32_t>(), dbh.as<double>(), Y, st))) return rc;
+    k_add_active<<<nblk(n), 256, 0, st>>>(n, act, R, Y, -1);
+    if (kind == LSG_PDE_HELMHOLTZ) {
+        BD_TRY(cudaMemsetAsync(Y, 0, n * 8, st));
+        if ((rc = boundary_rhs_run(op, LSG_BDRHS_MASS_COEFF, B.nb, B.dq.as<int32_t>(), dbh.as<double>(), Y, st)))
+            return rc;
+        k_add_active<<<nblk(n), 256, 0, st>>>(n, act, R, Y, -1);
+    }
+    BD_TRY(cudaGetLastError());
+    BD_TRY(cudaMemcpyAsync(rhs, R, n * 8, cudaMemcpyDeviceToHost, st));
+    BD_TRY(cudaMemcpyAsync(f, F, nn * 8, cudaMemcpyDeviceToHost, st));
+    BD_TRY(cudaMemcpyAsync(g, G, nn * 8, cudaMemcpyDeviceToHost, st));
+    BD_TRY(cudaStreamSynchronize(st));
     return 0;
 }
 

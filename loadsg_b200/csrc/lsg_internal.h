@@ -33,6 +33,8 @@ int autotune(lsg_operator* op, int32_t precision, int32_t reps);
 int matvec64_unit(lsg_operator* op, int form, const double* x, double* y, cudaStream_t st);
 // per-operator state of the basis transforms (lsg_basis.cu)
 std::shared_ptr<void>& basis_slot(lsg_operator* op);
+// calcPrewByNodal on device vectors (lsg_basis.cu)
+int prew_by_nodal_dev(lsg_operator* op, double* prew, const double* u, cudaStream_t st);
 // per-operator tables of the boundary-data right-hand sides (lsg_bdrhs.cu)
 std::shared_ptr<void>& bdrhs_slot(lsg_operator* op);
 

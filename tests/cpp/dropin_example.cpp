@@ -46,6 +46,16 @@ int main() {
     bd.multiply_mass(g, mass);
     double gmax = 0;
     for (int64_t k = 0; k < rhs.size(); ++k) gmax = std::fmax(gmax, std::fabs(rhs.getValue(k)));
+    // the whole right-hand side of -lap u = 0, u = 1 on the boundary: zero
+    lsg::VectorSparseG<3> f0(bgrid), g1(bgrid);
+    for (int64_t k = 0; k < bgrid.getMaximalOccupiedSecondTable(); ++k) {
+        auto I = bgrid.getIndexOfTable(k);
+        g1.setValue(k, (I[0] < 2 || I[1] < 2 || I[2] < 2) ? 1.0 : 0.0);
+    }
+    lsg::PDE_Poisson_InHomRHS<3> pde(bgrid, grid, m);
+    pde.SetUp(f0, g1);
+    for (int64_t k = 0; k < grid.getMaximalOccupiedSecondTable(); ++k)
+        gmax = std::fmax(gmax, std::fabs(pde.getRHS().getValue(k)));
     std::printf("N=%lld iterations=%d relres=%.3e transform round trip %.3e boundary: |grad| %.3e root mass %.6f\n",
                 (long long)grid.getMaximalOccupiedSecondTable(), it, std::sqrt(rr / ff), dmax, gmax, mass.getValue(0));
     return (std::sqrt(rr / ff) < 1e-8 && dmax < 1e-10 && gmax < 1e-10 && mass.getValue(0) == 0.125) ? 0 : 1;

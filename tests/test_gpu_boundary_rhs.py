@@ -132,3 +132,49 @@ def test_errors():
     y = np.full(g.n, 3.0)
     lsg.InHomoBoundaryRHSHierarchical(m, inner).multiply(np.ones(inner.n), y)
     assert np.all(y[g.active > 0] == 0.0) and np.all(y[g.active == 0] == 3.0)
+
+
+# ---------------------------------------------------------------- PDE_*::SetUp
+from conftest import GOLDEN_PDE  # noqa: E402
+
+
+@pytest.fixture(params=GOLDEN_PDE, ids=[os.path.basename(p)[:-4] for p in GOLDEN_PDE])
+def pde(request):
+    z = np.load(request.param)
+    return {k: z[k] for k in z.files}
+
+
+def test_transforms_match_reference(pde):
+    """CalcHierarchicalBasis on the grid with boundary points, CalcNodalBasis
+    on the interior grid: bit-exact."""
+    g = lsg.AdaptiveSparseGrid(pde["points"], pde["active"])
+    ng = lsg.AdaptiveSparseGrid(pde["npoints"], pde["nactive"])
+    f = pde["f"].copy()
+    lsg.CalcHierarchicalBasis(f, ng)
+    assert np.array_equal(f, pde["f_hier"])
+    x = pde["x"].copy()
+    lsg.CalcNodalBasis(x, g)
+    assert np.array_equal(x, pde["x_nodal"])
+    lsg.CalcHierarchicalBasis(x, g)  # and back
+    assert np.abs(x - pde["x"]).max() < 1e-13
+
+
+@pytest.mark.parametrize("cls,key", [(lsg.PDE_Poisson_InHomRHS, "rhs_poisson"),
+                                     (lsg.PDE_Helmholtz_VariableCoeff, "rhs_helmholtz")], ids=["poisson", "helmholtz"])
+def test_pde_setup_matches_reference(pde, cls, key):
+    """The whole SetUp against the reference's: 1e-12 relative (the inverse
+    basis transform and the mass product carry the matvec's 1e-13 rounding);
+    f and g come back transformed as the reference leaves them."""
+    g = lsg.AdaptiveSparseGrid(pde["points"], pde["active"])
+    ng = lsg.AdaptiveSparseGrid(pde["npoints"], pde["nactive"])
+    m = lsg.MatrixVectorHomogen(g)
+    p = cls(ng, g, m)
+    f, gv = pde["f"].copy(), pde["g"].copy()
+    p.SetUp(f, gv)
+    ref = pde[key]
+    assert np.abs(p.getRHS() - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert np.all(p.getRHS()[g.active == 0] == 0.0)
+    interior = (ng.points >= 2).all(axis=1)
+    assert np.array_equal(f[~interior], pde["f_hier"][~interior]) and not f[interior].any()
+    on = OracleGrid(ng.points, ng.active)
+    assert np.array_equal(gv, on.hierarchize_boundary(pde["g"]))
