@@ -213,9 +213,16 @@ def boundary_rhs_leg(lsg, torch, stream, reference=True):
         for meth in (rhs.multiply, rhs.multiply_mass, rhs.multiply_mass_coeff):
             meth(gv, y)
         e2e_ms = (time.perf_counter() - t0) * 1e3
+        # the whole right-hand side of -lap u = f, u = g on the boundary (PDE_Poisson_InHomRHS::SetUp)
+        fv = np.exp(-x[:, 0] * x[:, 1]) + x[:, 2]
+        gb = np.where(b, np.exp(0.3 * np.sin(np.pi * x[:, 0]) - 0.2 * x[:, 1] + x[:, 2] ** 2), 0.0)
+        pde = lsg.PDE_Poisson_InHomRHS(ng, g, m)
+        t0 = time.perf_counter()
+        pde.SetUp(fv, gb)
+        setup_ms = (time.perf_counter() - t0) * 1e3
         out[f"d3_L{L}"] = {"points": g.n, "boundary_points": int(b.sum()), "hierarchize_host_call_ms": hier_ms,
                            "gradient_ms": ms[0], "mass_ms": ms[1], "mass_coeff_ms": ms[2],
-                           "three_forms_host_call_ms": e2e_ms}
+                           "three_forms_host_call_ms": e2e_ms, "pde_poisson_setup_host_call_ms": setup_ms}
         log(f"boundary rhs d=3 L{L}: {g.n} points, {int(b.sum())} boundary points, device ms {ms}")
     exe = os.path.join(ROOT, "oracle", "_ref", "d3", "ref_harness")
     if reference and os.path.exists(exe):
