@@ -204,40 +204,43 @@ __device__ double hat_factor(double xp, double hp, double mp, int32_t iq) {
 // points' 1D indices dimension-major (bq[k * nb + b]).
 // KIND 0: CalcIntegral (sum over the derivative dimension of the products),
 // 1: CalcIntegral_mass, 2: CalcIntegral_coeff.
+// bsup[(2k) * nb + b], bsup[(2k+1) * nb + b]: the support of boundary point b
+// in dimension k, [lo, hi] in units of 2^-30 (exact: depths are at most 30)
+constexpr double kSupUnit = 1073741824.0;  // 2^30
+
 template <int D, int KIND>
 __global__ void __launch_bounds__(256) k_bd_nodal(int64_t ne, const int32_t* __restrict__ ej,
                                                   const int8_t* __restrict__ et, int64_t nb,
-                                                  const int32_t* __restrict__ bq, const double* __restrict__ bh,
-                                                  double* __restrict__ z) {
+                                                  const int32_t* __restrict__ bq, const int32_t* __restrict__ bsup,
+                                                  const double* __restrict__ bh, double* __restrict__ z) {
     const int lane = threadIdx.x & 31;
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t e = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < ne; e += nwarps) {
         double xp[D], hp[D], mp[D];
+        int32_t plo[D], phi[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) {
             int t = et[e * D + k];
             mp[k] = (double)(1 << t);
             hp[k] = 1.0 / mp[k];
             xp[k] = d_coord1(ej[e * D + k]);
+            plo[k] = (int32_t)((xp[k] - hp[k]) * kSupUnit);
+            phi[k] = (int32_t)((xp[k] + hp[k]) * kSupUnit);
         }
         double sum = 0.0;
         for (int64_t base = 0; base < nb; base += 32) {
             const int64_t b = base + lane;
             bool hit = b < nb;
             double c = 0.0;
-            int32_t iq[D];
+            // the supports must overlap with positive length in every dimension;
+            // otherwise each piece integral is exactly zero
 #pragma unroll
-            for (int k = 0; k < D; ++k) {
-                iq[k] = hit ? bq[k * nb + b] : 2;
-                // supports must overlap with positive length in every dimension;
-                // otherwise each piece integral is exactly zero
-                int tq = d_depth1(iq[k]);
-                double hq = 1.0 / (double)(1 << tq), xq = d_coord1(iq[k]);
-                double lo = fmax(xp[k] - hp[k], iq[k] == 0 ? xq : xq - hq);
-                double hi = fmin(xp[k] + hp[k], iq[k] == 1 ? xq : xq + hq);
-                hit = hit && lo < hi;
-            }
+            for (int k = 0; k < D; ++k)
+                if (hit) hit = plo[k] < bsup[(2 * k + 1) * nb + b] && bsup[(2 * k) * nb + b] < phi[k];
             if (hit) {
+                int32_t iq[D];
+#pragma unroll
+                for (int k = 0; k < D; ++k) iq[k] = bq[k * nb + b];
                 double val;
                 if (KIND == 0) {
                     double fv[D], fg[D];
@@ -415,36 +418,37 @@ std::vector<int64_t> boundary_order(int d, int64_t nn, const int32_t* pts) {
 }
 
 template <int D>
-int launch_nodal(int kind, const BdState& S, int64_t nb, const int32_t* bq, const double* bh, cudaStream_t st) {
+int launch_nodal(int kind, const BdState& S, int64_t nb, const int32_t* bq, const int32_t* bsup, const double* bh,
+                 cudaStream_t st) {
     int64_t warps = S.ne;
     unsigned grid = (unsigned)std::min<int64_t>((warps + 7) / 8, 148 * 64);
     if (grid == 0) return 0;
     const int32_t* ej = S.ej.as<int32_t>();
     const int8_t* et = S.et.as<int8_t>();
     double* z = S.z.as<double>();
-    if (kind == LSG_BDRHS_GRADIENT) k_bd_nodal<D, 0><<<grid, 256, 0, st>>>(S.ne, ej, et, nb, bq, bh, z);
-    else if (kind == LSG_BDRHS_MASS) k_bd_nodal<D, 1><<<grid, 256, 0, st>>>(S.ne, ej, et, nb, bq, bh, z);
-    else k_bd_nodal<D, 2><<<grid, 256, 0, st>>>(S.ne, ej, et, nb, bq, bh, z);
+    if (kind == LSG_BDRHS_GRADIENT) k_bd_nodal<D, 0><<<grid, 256, 0, st>>>(S.ne, ej, et, nb, bq, bsup, bh, z);
+    else if (kind == LSG_BDRHS_MASS) k_bd_nodal<D, 1><<<grid, 256, 0, st>>>(S.ne, ej, et, nb, bq, bsup, bh, z);
+    else k_bd_nodal<D, 2><<<grid, 256, 0, st>>>(S.ne, ej, et, nb, bq, bsup, bh, z);
     return 0;
 }
 
 // bh: hierarchical coefficients of the boundary points, in boundary order (device)
-int boundary_rhs_run(lsg_operator* op, int32_t kind, int64_t nb, const int32_t* bq, const double* bh, double* rhs,
-                     cudaStream_t st) {
+int boundary_rhs_run(lsg_operator* op, int32_t kind, int64_t nb, const int32_t* bq, const int32_t* bsup,
+                     const double* bh, double* rhs, cudaStream_t st) {
     BdState* Sp = nullptr;
     int rc = ensure_state(op, &Sp, st);
     if (rc) return rc;
     const BdState& S = *Sp;
     if (S.ne > 0 && nb > 0) {
         switch (S.d) {
-        case 1: rc = launch_nodal<1>(kind, S, nb, bq, bh, st); break;
-        case 2: rc = launch_nodal<2>(kind, S, nb, bq, bh, st); break;
-        case 3: rc = launch_nodal<3>(kind, S, nb, bq, bh, st); break;
-        case 4: rc = launch_nodal<4>(kind, S, nb, bq, bh, st); break;
-        case 5: rc = launch_nodal<5>(kind, S, nb, bq, bh, st); break;
-        case 6: rc = launch_nodal<6>(kind, S, nb, bq, bh, st); break;
-        case 7: rc = launch_nodal<7>(kind, S, nb, bq, bh, st); break;
-        case 8: rc = launch_nodal<8>(kind, S, nb, bq, bh, st); break;
+        case 1: rc = launch_nodal<1>(kind, S, nb, bq, bsup, bh, st); break;
+        case 2: rc = launch_nodal<2>(kind, S, nb, bq, bsup, bh, st); break;
+        case 3: rc = launch_nodal<3>(kind, S, nb, bq, bsup, bh, st); break;
+        case 4: rc = launch_nodal<4>(kind, S, nb, bq, bsup, bh, st); break;
+        case 5: rc = launch_nodal<5>(kind, S, nb, bq, bsup, bh, st); break;
+        case 6: rc = launch_nodal<6>(kind, S, nb, bq, bsup, bh, st); break;
+        case 7: rc = launch_nodal<7>(kind, S, nb, bq, bsup, bh, st); break;
+        case 8: rc = launch_nodal<8>(kind, S, nb, bq, bsup, bh, st); break;
         default: return fail_msg(LSG_E_INVALID, "unsupported dimension");
         }
     } else if (S.ne > 0) {
@@ -540,14 +544,29 @@ int run_sweeps(const std::vector<std::vector<int64_t>>& steps, double* u, int si
 // indices dimension-major, and the gather of a coefficient vector into that order
 struct BoundarySet {
     int64_t nb = 0;
-    DevArr dq, di;
+    DevArr dq, dsup, di;
     int build(int d, int64_t nn, const int32_t* pts, cudaStream_t st) {
         std::vector<int64_t> b = boundary_order(d, nn, pts);
         nb = (int64_t)b.size();
-        std::vector<int32_t> bq((size_t)nb * d);
+        std::vector<int32_t> bq((size_t)nb * d), sup((size_t)nb * d * 2);
         for (int64_t i = 0; i < nb; ++i)
-            for (int q = 0; q < d; ++q) bq[(size_t)q * nb + i] = pts[b[i] * d + q];
+            for (int q = 0; q < d; ++q) {
+                int32_t iq = pts[b[i] * d + q];
+                bq[(size_t)q * nb + i] = iq;
+                // support in units of 2^-30: [0, 1] for the boundary indices (their
+                // half inside the domain), [2j, 2j + 2] 2^-t for index 2^t + j
+                int64_t lo = 0, hi = (int64_t)1 << 30;
+                if (iq >= 2) {
+                    int t = h_depth1(iq);
+                    int64_t j = iq - ((int64_t)1 << t), s = (int64_t)1 << (30 - t);
+                    lo = 2 * j * s;
+                    hi = (2 * j + 2) * s;
+                }
+                sup[(size_t)(2 * q) * nb + i] = (int32_t)lo;
+                sup[(size_t)(2 * q + 1) * nb + i] = (int32_t)hi;
+            }
         int rc = dq.upload(bq, st);
+        rc = rc ? rc : dsup.upload(sup, st);
         rc = rc ? rc : di.upload(b, st);
         if (rc) return rc;
         BD_TRY(cudaStreamSynchronize(st));  // the host vectors go out of scope
@@ -625,7 +644,7 @@ int lsg_boundary_rhs_device(lsg_operator* op, int32_t kind, int64_t nn, const in
     DevArr dh;
     if ((rc = B.build(d, nn, points, st)) || (rc = dh.alloc(std::max<int64_t>(B.nb, 1) * 8))) return rc;
     B.gather(hier, dh.as<double>(), st);
-    rc = boundary_rhs_run(op, kind, B.nb, B.dq.as<int32_t>(), dh.as<double>(), rhs, st);
+    rc = boundary_rhs_run(op, kind, B.nb, B.dq.as<int32_t>(), B.dsup.as<int32_t>(), dh.as<double>(), rhs, st);
     if (rc) return rc;
     BD_TRY(cudaStreamSynchronize(st));  // the device tables go out of scope
     return 0;
@@ -698,18 +717,21 @@ int lsg_pde_boundary_rhs(lsg_operator* op, int32_t kind, int64_t nn, const int32
     // + <f_boundary, psi_i> (multiply_mass of the boundary coefficients of f)
     B.gather(F, dbh.as<double>(), st);
     BD_TRY(cudaMemsetAsync(Y, 0, n * 8, st));
-    if ((rc = boundary_rhs_run(op, LSG_BDRHS_MASS, B.nb, B.dq.as<int32_t>(), dbh.as<double>(), Y, st))) return rc;
+    rc = boundary_rhs_run(op, LSG_BDRHS_MASS, B.nb, B.dq.as<int32_t>(), B.dsup.as<int32_t>(), dbh.as<double>(), Y, st);
+    if (rc) return rc;
     k_add_active<<<nblk(n), 256, 0, st>>>(n, act, R, Y, +1);
     // - <grad g, grad psi_i> (- <c g, psi_i> for the Helmholtz problem)
     if ((rc = run_sweeps(sw_g, G, -1, tables, st))) return rc;
     B.gather(G, dbh.as<double>(), st);
     BD_TRY(cudaMemsetAsync(Y, 0, n * 8, st));
-    if ((rc = boundary_rhs_run(op, LSG_BDRHS_GRADIENT, B.nb, B.dq.as<int32_t>(), dbh.as<double>(), Y, st))) return rc;
+    rc = boundary_rhs_run(op, LSG_BDRHS_GRADIENT, B.nb, B.dq.as<int32_t>(), B.dsup.as<int32_t>(), dbh.as<double>(), Y, st);
+    if (rc) return rc;
     k_add_active<<<nblk(n), 256, 0, st>>>(n, act, R, Y, -1);
     if (kind == LSG_PDE_HELMHOLTZ) {
         BD_TRY(cudaMemsetAsync(Y, 0, n * 8, st));
-        if ((rc = boundary_rhs_run(op, LSG_BDRHS_MASS_COEFF, B.nb, B.dq.as<int32_t>(), dbh.as<double>(), Y, st)))
-            return rc;
+        rc = boundary_rhs_run(op, LSG_BDRHS_MASS_COEFF, B.nb, B.dq.as<int32_t>(), B.dsup.as<int32_t>(),
+                              dbh.as<double>(), Y, st);
+        if (rc) return rc;
         k_add_active<<<nblk(n), 256, 0, st>>>(n, act, R, Y, -1);
     }
     BD_TRY(cudaGetLastError());
