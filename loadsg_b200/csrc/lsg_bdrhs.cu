@@ -178,8 +178,10 @@ __device__ double hat_factor(double xp, double hp, double mp, int32_t iq) {
     double lp[2] = {S(xp, hp), xp}, rp[2] = {xp, A(xp, hp)};
     double lq[2] = {S(xq, hq), xq}, rq[2] = {xq, A(xq, hq)};
     double mps[2] = {mp, M(-1.0, mp)}, mqs[2] = {mq, M(-1.0, mq)};
-    double cps[2] = {-__ddiv_rn(S(xp, hp), hp), __ddiv_rn(A(xp, hp), hp)};
-    double cqs[2] = {-__ddiv_rn(S(xq, hq), hq), __ddiv_rn(A(xq, hq), hq)};
+    // (x -+ h) / h of the reference: h is a power of two, so the quotient is
+    // the exact product with 1/h = m (same bits, no division)
+    double cps[2] = {-M(S(xp, hp), mp), M(A(xp, hp), mp)};
+    double cqs[2] = {-M(S(xq, hq), mq), M(A(xq, hq), mq)};
     double s = 0.0;
 #pragma unroll
     for (int sp = 0; sp < 2; ++sp)
