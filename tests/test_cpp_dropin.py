@@ -19,6 +19,21 @@ def build_example(tmp_path):
     return exe
 
 
+def test_header_neumann_completion_matches_generator(tmp_path):
+    """completeNeumannGrid of the C++ drop-in equals the library's generator
+    (itself pinned to the reference's storage order), point for point."""
+    import numpy as np
+    exe = str(tmp_path / "neumann_grid")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "neumann_grid.cpp"), lsg.LIB_PATH,
+                    "-Wl,-rpath," + os.path.dirname(lsg.LIB_PATH), "-o", exe], check=True, capture_output=True)
+    for level in (3, 5):
+        out = subprocess.run([exe, str(level)], check=True, capture_output=True, text=True).stdout
+        rows = np.array([list(map(int, line.split())) for line in out.splitlines()], np.int64)
+        g = lsg.AdaptiveSparseGrid.neumann(3, level)
+        assert np.array_equal(rows[:, 1:], g.points) and np.array_equal(rows[:, 0], g.active)
+
+
 def test_dropin_header_compiles_and_links(tmp_path):
     assert os.path.exists(build_example(tmp_path))
 
