@@ -211,6 +211,37 @@ inline void calcPrewByNodal(VectorSparseG<D>& prew, const VectorSparseG<D>& u, M
     check(lsg_calc_prew_by_nodal(matrix.handle(), prew.getDatatableVector(), u.getDatatableVector()));
 }
 
+// H1::getValue / L2::getValue (applications/H1_Norm.cpp): the H1 seminorm and
+// the L2 norm of the function with nodal values u.  The reference constructs
+// them from (grid, mgrid); here from the grid's operator (any coefficient:
+// the norms use a = 1 and leave the operator's own coefficient in place).
+template <int D>
+class H1 {
+public:
+    explicit H1(MatrixVectorHomogen<D>& matrix) : m_(matrix) {}
+    double getValue(const VectorSparseG<D>& u) {
+        double v = 0.0;
+        check(lsg_h1_norm(m_.handle(), u.getDatatableVector(), &v));
+        return v;
+    }
+
+private:
+    MatrixVectorHomogen<D>& m_;
+};
+template <int D>
+class L2 {
+public:
+    explicit L2(MatrixVectorHomogen<D>& matrix) : m_(matrix) {}
+    double getValue(const VectorSparseG<D>& u) {
+        double v = 0.0;
+        check(lsg_l2_norm(m_.handle(), u.getDatatableVector(), &v));
+        return v;
+    }
+
+private:
+    MatrixVectorHomogen<D>& m_;
+};
+
 // CalcHierarchicalBasisForRHS(u) (MatrixVectorMultiplication/RHS.cpp:6-41):
 // u lives on a grid with boundary points; its boundary values become
 // hierarchical coefficients.

@@ -28,6 +28,9 @@ int main() {
     lsg::calcPrewByNodal<3>(back, u, m);
     double dmax = 0;
     for (int64_t k = 0; k < x.size(); ++k) dmax = std::fmax(dmax, std::fabs(back.getValue(k) - x.getValue(k)));
+    // norms of the solution's nodal values (H1::getValue / L2::getValue)
+    double h1 = lsg::H1<3>(m).getValue(u), l2 = lsg::L2<3>(m).getValue(u);
+    if (!(h1 > 0.0 && l2 > 0.0 && std::isfinite(h1) && std::isfinite(l2))) return 2;
     // boundary data g = 1 (PDE_Poisson_InHomRHS::SetUp, applications/PDE.cpp):
     // its extension is the constant 1, so the gradient form vanishes and the
     // mass form at the root (the level-1 hat) is 2^-3
