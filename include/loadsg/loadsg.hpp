@@ -65,6 +65,21 @@ public:
             AddPoint(I);
         }
     }
+    // completeDirichletGrid (sgrid/sparseGrid.cc:771-787): the missing interior
+    // points and the hanging nodes of this point set, added in the
+    // reference's order (lsg_grid_complete).
+    void completeDirichletGrid() {
+        const int64_t n = getMaximalOccupiedSecondTable();
+        int64_t m = 0;
+        check(lsg_grid_complete(D, n, points_.data(), active_.data(), 1, nullptr, nullptr, 0, &m));
+        std::vector<int32_t> pts(m * D);
+        std::vector<uint8_t> act(m);
+        check(lsg_grid_complete(D, n, points_.data(), active_.data(), 1, pts.data(), act.data(), m, &m));
+        points_.swap(pts);
+        active_.swap(act);
+        where_.clear();
+        for (int64_t k = 0; k < m; ++k) where_[getIndexOfTable(k)] = k;
+    }
     // completeNeumannGrid (sgrid/sparseGrid.cc:654-740): passes in which every
     // active point adds (or activates) its same-level neighbours where its
     // depth is > 0 and the opposite boundary point where it is 0; only a newly

@@ -353,6 +353,15 @@ int lsg_grid_regular(int32_t d, int32_t level, int32_t *points, int64_t capacity
 int lsg_grid_adaptive(int32_t d, int32_t level, int32_t refine, double theta, int32_t target, int32_t complete,
                       int32_t *points, uint8_t *active, int64_t capacity, int64_t *n);
 
+/* Completion of a caller's grid (points n x d in storage order, active flags):
+ * `complete` as for lsg_grid_adaptive (1: completeDirichletGrid,
+ * sgrid/sparseGrid.cc:771-787, with its hanging nodes; 64:
+ * completeNeumannGrid).  The given points keep their order and flags; added
+ * points follow in the reference's insertion order.  Pass out_points =
+ * out_active = NULL to query *n_out. */
+int lsg_grid_complete(int32_t d, int64_t n, const int32_t *points, const uint8_t *active, int32_t complete,
+                      int32_t *out_points, uint8_t *out_active, int64_t capacity, int64_t *n_out);
+
 const char *lsg_last_error(void);
 
 #ifdef __cplusplus

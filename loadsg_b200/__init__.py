@@ -128,6 +128,7 @@ def lib():
             "lsg_hierarchize_boundary": (ctypes.c_int, [I32, I64, P, P]),
             "lsg_boundary_rhs": (ctypes.c_int, [P, I32, I64, P, P, P]),
             "lsg_boundary_rhs_device": (ctypes.c_int, [P, I32, I64, P, P, P, P]),
+            "lsg_grid_complete": (ctypes.c_int, [I32, I64, P, P, I32, P, P, I64, P]),
             "lsg_hierarchize": (ctypes.c_int, [I32, I64, P, P, P]),
             "lsg_dehierarchize": (ctypes.c_int, [I32, I64, P, P, P]),
             "lsg_pde_boundary_rhs": (ctypes.c_int, [P, I32, I64, P, P, P, P, P]),
@@ -223,6 +224,27 @@ class AdaptiveSparseGrid:
         _check(lib().lsg_grid_adaptive(d, level, refine, theta, t, mask, _ptr(pts), _ptr(act), n.value,
                                        ctypes.byref(n)))
         return cls(pts, act)
+
+    def _complete(self, mask):
+        n = ctypes.c_int64(0)
+        _check(lib().lsg_grid_complete(self.d, self.n, _ptr(self.points), _ptr(self.active), mask, None, None, 0,
+                                       ctypes.byref(n)))
+        pts = np.zeros((n.value, self.d), np.int32)
+        act = np.zeros(n.value, np.uint8)
+        _check(lib().lsg_grid_complete(self.d, self.n, _ptr(self.points), _ptr(self.active), mask, _ptr(pts),
+                                       _ptr(act), n.value, ctypes.byref(n)))
+        self.points, self.active, self.n = pts, act, n.value
+
+    def completeDirichletGrid(self):
+        """AdaptiveSparseGrid::completeDirichletGrid (sgrid/sparseGrid.cc:771-787),
+        in place: the missing interior points and the hanging nodes of this
+        point set, added in the reference's order."""
+        self._complete(1)
+
+    def completeNeumannGrid(self):
+        """AdaptiveSparseGrid::completeNeumannGrid (sgrid/sparseGrid.cc:654-740),
+        in place: neighbours and boundary points of the active points."""
+        self._complete(64)
 
     def boundary_mask(self):
         """Points with a 1D index 0 or 1 (coordinate 0 or 1) in some dimension."""

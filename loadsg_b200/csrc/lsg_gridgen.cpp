@@ -402,6 +402,38 @@ struct LastGrid {
 thread_local LastGrid g_last;
 }  // namespace
 
+// Completes a caller's grid: the points (n x d, in storage order, with their
+// active flags) are taken as they are, then the completion stages of
+// `complete` run on them and the result is returned in the same way as
+// lsg_grid_adaptive returns its grid.
+extern "C" int lsg_grid_complete(int32_t d, int64_t n, const int32_t* points, const uint8_t* active,
+                                 int32_t complete, int32_t* out_points, uint8_t* out_active, int64_t capacity,
+                                 int64_t* n_out) {
+    if (d < 1 || d > 8 || n < 0 || (n > 0 && (!points || !active)) || !n_out) return LSG_E_INVALID;
+    Grid g(d);
+    for (int64_t k = 0; k < n; ++k) {
+        const int32_t* I = points + k * d;
+        for (int j = 0; j < d; ++j)
+            if (I[j] < 0) return LSG_E_INVALID;
+        if (g.find(I) >= 0) return LSG_E_INVALID;  // duplicate point
+        g.append(I, active[k] != 0);
+    }
+    int mask = complete == 1 ? 0x3e : complete;
+    if (mask & 2) complete_without_boundary(g);
+    if (mask & 4) complete_tensor(g);
+    if (mask & 8) complete_without_boundary(g);
+    if (mask & 16) add_hanging(g);
+    if ((mask & 32) && g.n() <= LSG_PAIRWISE_MAX) add_points2(g);
+    if (mask & 64) complete_neumann(g);
+    *n_out = g.n();
+    if (out_points || out_active) {
+        if (capacity < g.n()) return LSG_E_INVALID;
+        if (out_points) memcpy(out_points, g.pts.data(), g.pts.size() * sizeof(int32_t));
+        if (out_active) memcpy(out_active, g.act.data(), g.act.size());
+    }
+    return 0;
+}
+
 extern "C" int lsg_grid_adaptive(int32_t d, int32_t level, int32_t refine, double theta, int32_t target,
                                  int32_t complete, int32_t* points, uint8_t* active, int64_t capacity, int64_t* n) {
     if (d < 1 || d > 8 || level < 0 || level > 24 || refine < 0 || !n) return LSG_E_INVALID;

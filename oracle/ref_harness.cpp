@@ -491,6 +491,25 @@ int main(int argc, char **argv) {
             dump(which == 0 ? "rhs_poisson.f64" : "rhs_helmholtz.f64", rhs);
         }
         g_meta << "NN " << NN << "\n";
+    } else if (cmd == "complete") {
+        // A caller's grid completed by the reference: the points of file `pts`
+        // (np x D int32) added with AddPoint in order, then completeDirichletGrid
+        // (mode=dirichlet, sgrid/sparseGrid.cc:771-787) or completeNeumannGrid
+        // (mode=neumann, :654-740).  The grid built from level=... is not used.
+        long np = atol(opt("np", "0").c_str());
+        std::vector<int32_t> in(np * D);
+        FILE *f = fopen(opt("pts", "").c_str(), "rb");
+        if (!f || fread(in.data(), sizeof(int32_t), in.size(), f) != in.size()) { fprintf(stderr, "pts\n"); return 2; }
+        fclose(f);
+        AdaptiveSparseGrid cg;
+        for (long k = 0; k < np; ++k) {
+            IndexDimension I;
+            for (int d = 0; d < D; ++d) I.replace(d, in[k * D + d]);
+            cg.AddPoint(I);
+        }
+        if (opt("mode", "dirichlet") == "neumann") cg.completeNeumannGrid();
+        else cg.completeDirichletGrid();
+        dump_grid(cg);
     } else if (cmd == "prew2nodal" || cmd == "nodal2prew") {
         // prew2nodal: u = calcNodalByPrew(x); nodal2prew: p = calcPrewByNodal(x)
         std::vector<double> x = read_f64(opt("x", ""), N);

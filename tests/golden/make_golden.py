@@ -12,6 +12,7 @@ reference.
 
     python tests/golden/make_golden.py --bd        # boundary-data right-hand sides -> bd_<name>.npz
     python tests/golden/make_golden.py --pde       # PDE_*::SetUp right-hand sides -> pde_<name>.npz
+    python tests/golden/make_golden.py --complete  # completion of given point sets -> cmp_<name>.npz
 
 prew2nodal / nodal2prew run calcNodalByPrew / calcPrewByNodal on the fixture's
 x (BasisTransformations/BasisTransformations.cpp:486-545,670-706); mass /
@@ -85,6 +86,36 @@ PDE_CASES = [
     ("pde_d3_L3", 3, "level=3", EXPSIN6, SIN2PI),
     ("pde_d4_L2", 4, "level=2", SIN2PI, EXPSIN6),
 ]
+
+
+# a caller's point set completed by the reference (completeDirichletGrid /
+# completeNeumannGrid): name, d, seed, points, max steps from the centre
+# (seed None: the two points of examples_doxygen/gridgeneration_adaptive.cpp)
+COMPLETE_CASES = [
+    ("cmp_d2_example", 2, None, 0, 0),
+    ("cmp_d2_random", 2, 11, 6, 7),
+    ("cmp_d3_random", 3, 12, 5, 6),
+    ("cmp_d4_random", 4, 13, 4, 5),
+]
+
+
+def complete_input(d, seed, npts, steps):
+    """Points reached from the centre by random son steps (deduplicated)."""
+    if seed is None:
+        c = [2] * d
+        bl = [2 * (2 * v) for v in c]  # leftSon(0).leftSon(1).leftSon(0).leftSon(1) in d = 2: (8, 8)
+        tr = [2 * (2 * v + 1) + 1 for v in c]  # the same with rightSon: (11, 11)
+        return np.array([bl, tr], np.int32)
+    rng = np.random.default_rng(seed)
+    pts = []
+    while len(pts) < npts:
+        I = [2] * d
+        for _ in range(int(rng.integers(2, steps + 1))):
+            k = int(rng.integers(0, d))
+            I[k] = 2 * I[k] + int(rng.integers(0, 2))
+        if I not in pts:
+            pts.append(I)
+    return np.array(pts, np.int32)
 
 
 def run(cmd, **kw):
@@ -231,6 +262,24 @@ def make_pde_case(name, d, gridargs, fcoef, gcoef, refsrc):
     print(f"{name}: N={len(out['active'])} NN={len(out['nactive'])} -> {os.path.getsize(path)} bytes")
 
 
+def make_complete_case(name, d, seed, npts, steps, refsrc):
+    run(["make", "-s", "-C", ORACLE, "ref", f"D={d}", f"REFSRC={refsrc}", "-j8"])
+    exe = os.path.join(ORACLE, "_ref", f"d{d}", "ref_harness")
+    pin = complete_input(d, seed, npts, steps)
+    out = {"d": np.int32(d), "in_points": pin}
+    with tempfile.TemporaryDirectory() as tmp:
+        pin.tofile(os.path.join(tmp, "pts.i32"))
+        for mode, prefix in (("dirichlet", ""), ("neumann", "n")):
+            run([exe, "complete", tmp, f"np={len(pin)}", f"pts={tmp}/pts.i32", f"mode={mode}"])
+            meta, arrs = read_meta(os.path.join(tmp, "meta_complete.txt"))
+            got = load_arrays(tmp, arrs, prefix)
+            out[prefix + "points"] = got[prefix + "points"].reshape(-1, d)
+            out[prefix + "active"] = got[prefix + "active"]
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"{name}: {len(pin)} points -> {len(out['active'])} (Dirichlet), {len(out['nactive'])} (Neumann)")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--refsrc", default="/root/reference/library/source")
@@ -238,7 +287,13 @@ def main():
     ap.add_argument("--cmds", default=None, help="comma list: add these commands to existing fixtures")
     ap.add_argument("--bd", action="store_true", help="the boundary-data right-hand-side fixtures")
     ap.add_argument("--pde", action="store_true", help="the PDE right-hand-side (SetUp) fixtures")
+    ap.add_argument("--complete", action="store_true", help="completion of given point sets")
     a = ap.parse_args()
+    if a.complete:
+        for case in COMPLETE_CASES:
+            if not a.only or case[0] == a.only:
+                make_complete_case(*case, refsrc=a.refsrc)
+        return
     if a.pde:
         for case in PDE_CASES:
             if not a.only or case[0] == a.only:

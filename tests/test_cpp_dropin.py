@@ -34,6 +34,23 @@ def test_header_neumann_completion_matches_generator(tmp_path):
         assert np.array_equal(rows[:, 1:], g.points) and np.array_equal(rows[:, 0], g.active)
 
 
+def test_header_adaptive_example_matches_reference(tmp_path):
+    """The reference's adaptive-grid example (two points, completeDirichletGrid)
+    through the C++ drop-in: the grid the compiled reference builds from the
+    same two points (tests/golden/cmp_d2_example.npz), 23 DOFs and 18 hanging
+    nodes."""
+    import numpy as np
+    exe = str(tmp_path / "gridgeneration_adaptive")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "gridgeneration_adaptive.cpp"), lsg.LIB_PATH,
+                    "-Wl,-rpath," + os.path.dirname(lsg.LIB_PATH), "-o", exe], check=True, capture_output=True)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.splitlines()
+    rows = np.array([list(map(int, line.split())) for line in out if not line.startswith("#")], np.int64)
+    z = np.load(os.path.join(ROOT, "tests", "golden", "cmp_d2_example.npz"))
+    assert np.array_equal(rows[:, 1:], z["points"]) and np.array_equal(rows[:, 0], z["active"])
+    assert out[-1] == "# 23 18"
+
+
 def test_dropin_header_compiles_and_links(tmp_path):
     assert os.path.exists(build_example(tmp_path))
 

@@ -156,3 +156,33 @@ def test_neumann_generator_reproduces_reference(path):
     assert np.array_equal(g.active, z["nactive"])
     assert g.boundary_mask().any() and np.all(g.coordinates()[g.points == 0] == 0.0)
     assert np.all(g.coordinates()[g.points == 1] == 1.0)
+
+
+@pytest.mark.parametrize("path", __import__("conftest").GOLDEN_COMPLETE,
+                         ids=lambda p: os.path.basename(p)[:-4])
+def test_completion_of_given_points_matches_reference(path):
+    """completeDirichletGrid / completeNeumannGrid of a caller's point set
+    (lsg_grid_complete): the reference's points, order and hanging flags.
+    cmp_d2_example is the two points of the reference's adaptive-grid example."""
+    z = np.load(path)
+    g = lsg.AdaptiveSparseGrid(z["in_points"])
+    g.completeDirichletGrid()
+    assert np.array_equal(g.points, z["points"]) and np.array_equal(g.active, z["active"])
+    h = lsg.AdaptiveSparseGrid(z["in_points"])
+    h.completeNeumannGrid()
+    assert np.array_equal(h.points, z["npoints"]) and np.array_equal(h.active, z["nactive"])
+
+
+def test_completion_pipeline_equals_generator():
+    """Refinement without completion, then lsg_grid_complete, equals the
+    generator's refinement with completion (pinned to the reference above)."""
+    for d, lv, r, th, tg in [(2, 3, 3, 0.45, "corner"), (3, 2, 3, 0.6, "corner"), (4, 2, 2, 0.3, "plane")]:
+        raw = lsg.AdaptiveSparseGrid.adaptive(d, lv, r, th, tg, complete=False)
+        raw.completeDirichletGrid()
+        ref = lsg.AdaptiveSparseGrid.adaptive(d, lv, r, th, tg)
+        assert np.array_equal(raw.points, ref.points) and np.array_equal(raw.active, ref.active)
+
+
+def test_completion_rejects_bad_input():
+    with pytest.raises(lsg.LsgError):
+        lsg.AdaptiveSparseGrid(np.array([[2, 4], [2, 4]], np.int32)).completeDirichletGrid()  # duplicate
