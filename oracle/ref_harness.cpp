@@ -491,6 +491,60 @@ int main(int argc, char **argv) {
             dump(which == 0 ? "rhs_poisson.f64" : "rhs_helmholtz.f64", rhs);
         }
         g_meta << "NN " << NN << "\n";
+    } else if (cmd == "poissonex") {
+        // The steps of examples_doxygen/poisson_regular.cpp through the
+        // reference's API, for levels 1..levels: u = prod sin(pi x_d), f = d pi^2 u
+        // at the active points; f to prewavelets (calcPrewByNodal), the
+        // right-hand side by the HelmHoltz product, CG::solveHomogen with the
+        // Poisson stencil at eps = 1e-10, the solution back to nodal values
+        // (calcNodalByPrew); the error's maximum, L2 and L2 + H1 norms.
+        int levels = atoi(opt("levels", "5").c_str());
+        std::vector<double> dofs, iters, linf, l2v, h1v;
+        for (int level = 1; level <= levels; ++level) {
+            AdaptiveSparseGrid pg;
+            IndexDimension c;
+            pg.AddRecursiveSonsOfPoint(c, level);
+            MultiLevelAdaptiveSparseGrid pm(&pg);
+            unsigned long PN = pg.getMaximalOccupiedSecondTable();
+            VectorSparseG u(pg), f(pg), rhs(pg), prew(pg), w(pg), err(pg);
+            u = 0.0;
+            f = 0.0;
+            for (unsigned long k = 0; k < PN; ++k) {
+                if (!pg.getActiveTable()[k]) continue;
+                IndexDimension I = pg.getIndexOfTable(k);
+                double s = 1.0;
+                for (int d = 0; d < D; ++d) s *= sin(M_PI * I.coordinate(d));
+                u.setValue(k, s);
+                f.setValue(k, double(D) * M_PI * M_PI * s);
+            }
+            MatrixVectorHomogen mv(pg, pm, true, false);
+            HelmHoltz helm(pg);
+            Poisson pois(pg);
+            prew = 0.0;
+            calcPrewByNodal(prew, f);
+            rhs = 0.0;
+            mv.multiplication(prew, rhs, helm);
+            prew = 0.0;
+            int it = 0;
+            double tp = 0.0;
+            CG::solveHomogen(1e-10, prew, rhs, &it, u, mv, pois, &tp);
+            w = 0.0;
+            calcNodalByPrew(prew, w);
+            err = u - w;
+            L2 l2n(pg, pm);
+            H1 h1n(pg, pm);
+            double l2 = l2n.getValue(err);
+            dofs.push_back(pg.getDOFS());
+            iters.push_back(it);
+            linf.push_back(L_infty(err));
+            l2v.push_back(l2);
+            h1v.push_back(h1n.getValue(err) + l2);
+        }
+        dump("dofs.f64", dofs);
+        dump("iterations.f64", iters);
+        dump("linfty.f64", linf);
+        dump("l2.f64", l2v);
+        dump("h1.f64", h1v);
     } else if (cmd == "complete") {
         // A caller's grid completed by the reference: the points of file `pts`
         // (np x D int32) added with AddPoint in order, then completeDirichletGrid

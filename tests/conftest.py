@@ -12,7 +12,7 @@ if ROOT not in sys.path:
 _ALL = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
 # operator fixtures (matvec, diagonal, CG, transforms) and boundary-data
 # right-hand-side fixtures (bd_*: a grid with boundary points beside the grid)
-GOLDEN = [p for p in _ALL if not os.path.basename(p).startswith(("bd_", "pde_", "cmp_"))]
+GOLDEN = [p for p in _ALL if not os.path.basename(p).startswith(("bd_", "pde_", "cmp_", "ex_"))]
 GOLDEN_BD = [p for p in _ALL if os.path.basename(p).startswith("bd_")]
 # right-hand sides of boundary-data problems (PDE_*::SetUp) and their transforms
 GOLDEN_PDE = [p for p in _ALL if os.path.basename(p).startswith("pde_")]

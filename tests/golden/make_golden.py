@@ -13,6 +13,7 @@ reference.
     python tests/golden/make_golden.py --bd        # boundary-data right-hand sides -> bd_<name>.npz
     python tests/golden/make_golden.py --pde       # PDE_*::SetUp right-hand sides -> pde_<name>.npz
     python tests/golden/make_golden.py --complete  # completion of given point sets -> cmp_<name>.npz
+    python tests/golden/make_golden.py --example   # poisson_regular.cpp's convergence table -> ex_poisson_d3.npz
 
 prew2nodal / nodal2prew run calcNodalByPrew / calcPrewByNodal on the fixture's
 x (BasisTransformations/BasisTransformations.cpp:486-545,670-706); mass /
@@ -280,6 +281,21 @@ def make_complete_case(name, d, seed, npts, steps, refsrc):
     print(f"{name}: {len(pin)} points -> {len(out['active'])} (Dirichlet), {len(out['nactive'])} (Neumann)")
 
 
+def make_poisson_example(refsrc, levels=5):
+    """The convergence table of examples_doxygen/poisson_regular.cpp (d = 3,
+    levels 1..5) from the reference's own API -> ex_poisson_d3.npz."""
+    run(["make", "-s", "-C", ORACLE, "ref", "D=3", f"REFSRC={refsrc}", "-j8"])
+    exe = os.path.join(ORACLE, "_ref", "d3", "ref_harness")
+    with tempfile.TemporaryDirectory() as tmp:
+        run([exe, "poissonex", tmp, f"levels={levels}"])
+        meta, arrs = read_meta(os.path.join(tmp, "meta_poissonex.txt"))
+        out = load_arrays(tmp, arrs, "")
+    out["d"] = np.int32(3)
+    path = os.path.join(HERE, "ex_poisson_d3.npz")
+    np.savez_compressed(path, **out)
+    print(f"ex_poisson_d3: dofs {out['dofs'].tolist()} iterations {out['iterations'].tolist()}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--refsrc", default="/root/reference/library/source")
@@ -288,7 +304,11 @@ def main():
     ap.add_argument("--bd", action="store_true", help="the boundary-data right-hand-side fixtures")
     ap.add_argument("--pde", action="store_true", help="the PDE right-hand-side (SetUp) fixtures")
     ap.add_argument("--complete", action="store_true", help="completion of given point sets")
+    ap.add_argument("--example", action="store_true", help="the Poisson example's convergence table")
     a = ap.parse_args()
+    if a.example:
+        make_poisson_example(a.refsrc)
+        return
     if a.complete:
         for case in COMPLETE_CASES:
             if not a.only or case[0] == a.only:
