@@ -33,7 +33,7 @@ def _rank_main(rank, world, port, out):
 
 def test_time_is_max_over_ranks():
     world = 2
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:  # no fork of a multi-threaded parent
         out = mgr.dict()
         mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
         assert dict(out) == {0: 2.5, 1: 2.5}
