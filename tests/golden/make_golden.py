@@ -61,6 +61,7 @@ CASES = [
     ("d5_L2", 5, "level=2", EXPSIN6, ["tables", "matvec", "diag"]),
     ("d6_L2", 6, "level=2", EXPSIN6, ["tables", "matvec", "poisson", "diag", "cg"]),
     ("d6_L3", 6, "level=3", SINPROD_M, ["matvec", "diag"]),
+    ("d7_L2", 7, "level=2", SINPROD_M, ["tables", "matvec", "poisson", "diag", "mass", "helmholtz", "massdiag"]),
     ("d8_L2", 8, "level=2", EXPSIN6, ["tables", "matvec", "poisson", "prew2nodal", "nodal2prew"]),
     # the CPU-runnable configuration: d = 3, level 7 (7,423 points), a = 1 + 0.5 prod sin(pi x_i)
     ("d3_L7", 3, "level=7", SINPROD, ["matvec", "poisson", "diag", "cg"]),
