@@ -111,7 +111,8 @@ int lsg_matvec_device_noalloc(lsg_operator *op, const void *x, void *y, int32_t 
  * phases; phase_ms[0..3] = mean ms of (nodal transform, P init, prolongation
  * levels, restriction wavefronts incl. the cell operator), phase_ms[4] = whole
  * matvec.  bytes[0..4] = algorithmic bytes of the same phases for this
- * precision (see the design notes); flops = cell-operator flops per matvec. */
+ * precision (every vector, slab and table counted once per kernel that must
+ * touch it); flops = cell-operator flops per matvec. */
 int lsg_matvec_profile(lsg_operator *op, const void *x, void *y, int32_t precision, int32_t iters, double *phase_ms,
                        double *bytes, double *flops);
 
@@ -250,7 +251,7 @@ int lsg_dehierarchize(int32_t d, int64_t n, const int32_t *points, const uint8_t
  * at every point, g at the boundary points of the grid with boundary points
  * (nn points, nn x d 1D indices, its active flags); rhs gets n values (0 at
  * hanging points).  As in the reference, f and g are transformed in place:
- * f to hierarchical coefficients with its interior entries moved out (0), g
+ * f to hierarchical coefficients with its active interior entries moved out (0), g
  * to hierarchical boundary coefficients.  Host arrays; no coefficient needed. */
 #define LSG_PDE_POISSON 0
 #define LSG_PDE_HELMHOLTZ 1
