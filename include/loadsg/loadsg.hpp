@@ -17,6 +17,7 @@
 #pragma once
 #include <algorithm>
 #include <array>
+#include <cmath>
 #include <cstdint>
 #include <map>
 #include <stdexcept>
@@ -152,6 +153,26 @@ struct MidpointDiffusion {
     std::vector<double> params;
     int32_t form = LSG_FORM_STIFFNESS;  // LSG_FORM_MASS: a(x) u v (HelmHoltz for a = 1)
 };
+
+// The reference's constant-coefficient operators (stencils/Stencil.h):
+// Poisson is a = 1 with the stiffness form, HelmHoltz a = 1 with the mass
+// form (Stencil.h:873-919).  The grid argument mirrors their constructors.
+struct Poisson : MidpointDiffusion {
+    template <class Grid>
+    explicit Poisson(const Grid&) : MidpointDiffusion{LSG_COEF_CONST, {1.0}, LSG_FORM_STIFFNESS} {}
+};
+struct HelmHoltz : MidpointDiffusion {
+    template <class Grid>
+    explicit HelmHoltz(const Grid&) : MidpointDiffusion{LSG_COEF_CONST, {1.0}, LSG_FORM_MASS} {}
+};
+
+// L_infty(v) of the reference (applications/norms.h): the largest magnitude
+template <int D>
+inline double L_infty(const VectorSparseG<D>& v) {
+    double m = 0.0;
+    for (int64_t k = 0; k < v.size(); ++k) m = std::max(m, std::fabs(v.getValue(k)));
+    return m;
+}
 
 template <int D>
 class MatrixVectorHomogen {

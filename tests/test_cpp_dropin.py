@@ -51,6 +51,17 @@ def test_header_adaptive_example_matches_reference(tmp_path):
     assert out[-1] == "# 23 18"
 
 
+def test_poisson_example_port_compiles(tmp_path):
+    """The reference's Poisson example written against the drop-in
+    (tests/cpp/poisson_regular_port.cpp) compiles and links; its table is
+    checked on the GPU through the same library calls in tests/test_poisson_example.py."""
+    exe = str(tmp_path / "poisson_regular_port")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "poisson_regular_port.cpp"), lsg.LIB_PATH,
+                    "-Wl,-rpath," + os.path.dirname(lsg.LIB_PATH), "-o", exe], check=True, capture_output=True)
+    assert os.path.exists(exe)
+
+
 def test_dropin_header_compiles_and_links(tmp_path):
     assert os.path.exists(build_example(tmp_path))
 
