@@ -265,8 +265,8 @@ int lsg_pde_boundary_rhs(lsg_operator *op, int32_t kind, int64_t nn, const int32
  * No counterpart in the reference (OpenMP schedule only). */
 typedef struct {
     int32_t cell_threads;    /* threads per cell-operator CTA: 64..256, multiple of 32 */
-    int32_t cell_segment;    /* dim-0 cells per work unit on complete slabs: a power of two, 1..64 */
-    int32_t class_ratio;     /* slab-size ratio that starts a new cell-operator launch: 2..1024 */
+    int32_t cell_space_kb;   /* shared-memory work space per cell-operator CTA in KB: 16..200 */
+    int32_t class_ratio;     /* work-space (slab-size) ratio that starts a new cell-operator launch: 2..1024 */
     int32_t level_threads;   /* threads per restriction-wavefront CTA: 32..512, multiple of 32 */
     int32_t level_cap;       /* shared-memory elements per wavefront ping-pong buffer: 256..65536 */
     int32_t prolong_threads; /* threads per prolongation CTA: 32..1024, multiple of 32 */
@@ -321,6 +321,18 @@ int lsg_plan_export_depths(const lsg_plan *plan, int32_t *depths);
 int lsg_plan_export_sorted_depths(const lsg_plan *plan, int32_t c, int32_t *depth_ids, int32_t *count);
 /* cells of depth T+1 in the grid per depth (CellData, cells/CellStructure.h:23-61) */
 int lsg_plan_export_cell_counts(const lsg_plan *plan, int64_t *counts);
+/* Diagnostic for the CPU tests: applies the level-T cell operator of one dense
+ * slab (depth id t) to u, given per-cell coefficients acell (the slab's cells,
+ * dim 0 fastest), twice on the host: cell by cell as
+ * LocalStiffnessMatrices::applyLocalMatrix does
+ * (localStiffnessMatrices/LocalStiffnessMatrices.cpp:555-582) -> z_cells, and in
+ * the factorised form of the GPU kernel, planned for a work space of wcap
+ * elements and a register dimension of at most na_max nodes -> z_sf.
+ * info (6 entries, may be NULL): mid dims, chunked dims, chunks, a extent,
+ * b extent (0 = none), collapsed dims. */
+int lsg_plan_check_slab_operator(const lsg_plan *plan, int32_t t, int32_t form, int64_t wcap, int32_t na_max,
+                                 const double *acell, const double *u, double *z_cells, double *z_sf,
+                                 int32_t *info);
 /* corners (storage index or -1) of every cell of one depth, 2^d per cell,
  * corner id bit k = right side in dim k; cells ordered by min corner */
 int lsg_plan_export_cells(const lsg_plan *plan, int32_t depth_id, int64_t *corners, int64_t *count);

@@ -79,7 +79,7 @@ class Tuning(ctypes.Structure):
     """Launch parameters of the matvec (lsg_tuning in include/lsg.h)."""
     _fields_ = [
         ("cell_threads", ctypes.c_int32),
-        ("cell_segment", ctypes.c_int32),
+        ("cell_space_kb", ctypes.c_int32),
         ("class_ratio", ctypes.c_int32),
         ("level_threads", ctypes.c_int32),
         ("level_cap", ctypes.c_int32),

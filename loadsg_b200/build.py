@@ -5,6 +5,7 @@
 nvcc compiles the CUDA translation unit and the host planner (OpenMP) and
 links them into one shared library with the static CUDA runtime.
 """
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -15,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "liblsg.so")
 BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["lsg_device.cu", "lsg_batch.cu", "lsg_basis.cu", "lsg_bdrhs.cu", "lsg_mlp.cu", "lsg_plan.cpp", "lsg_grid.cpp", "lsg_gridgen.cpp"]
+SOURCES = ["lsg_device.cu", "lsg_batch.cu", "lsg_basis.cu", "lsg_bdrhs.cu", "lsg_mlp.cu", "lsg_plan.cpp", "lsg_sf.cpp", "lsg_grid.cpp", "lsg_gridgen.cpp"]
 
 
 def nvcc():
@@ -42,21 +43,21 @@ def build(force=False, verbose=False):
     cc = nvcc()
     host = ["-ccbin", "/usr/bin/g++"] if os.path.exists("/usr/bin/g++") else []
     common = host + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp", "-lineinfo"]
-    objs = []
-    for s in SOURCES:
+    def compile_one(s):
         src = os.path.join(CSRC, s)
         obj = os.path.join(BUILD, s + ".o")
         cmd = [cc] + common + ARCH + ["-c", src, "-o", obj]
-        if s.endswith(".cu"):
-            cmd += ["-Xptxas", "-v"] if verbose else []
-        else:
-            cmd += ["-x", "cu"] if False else []
+        if s.endswith(".cu") and verbose:
+            cmd += ["-Xptxas", "-v"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
         if verbose:
             sys.stderr.write(r.stderr)
-        objs.append(obj)
+        return obj
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
     tmp = OUT + ".tmp"
     cmd = [cc] + host + ARCH + ["-shared", "-o", tmp] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"]
     r = subprocess.run(cmd, capture_output=True, text=True)

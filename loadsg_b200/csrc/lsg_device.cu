@@ -14,6 +14,7 @@
 //   k_diag       exact Jacobi diagonal (cg_method.h:544-680)
 //   CG kernels   CG::solveHomogen vector semantics (cg_method.h:759-886)
 #include "lsg_plan.h"
+#include "lsg_sf.h"
 #include "lsg_coef.cuh"
 #include "lsg_internal.h"
 #include "../../include/lsg.h"
@@ -80,6 +81,9 @@ struct DevPlan {
     const lsg::PhaseBItem* b_items;
     const lsg::PhaseBStep* b_steps;
     const int32_t* pts;
+    const int64_t* conv_off;        // per phase-B item: first convert slot (-1: none)
+    const int32_t* conv_items_off;  // per depth: range in conv_items
+    const int32_t* conv_items;      // items whose restrictions end at the depth, in item order
 };
 
 template <typename V>
@@ -560,11 +564,12 @@ __global__ void __launch_bounds__(256, std::is_same<V, float>::value ? 3 : 2) k_
 
 // ----------------------------------------------------------------------------- phase B, wavefront level
 // Per (case, depth) item of one restriction wavefront: z = z_c(T) + gM_c(T),
-// the restriction steps with the gM swap-add, and ConvertToPrewavelet2 into y.
+// the restriction steps with the gM swap-add, and ConvertToPrewavelet2 into
+// the item's own convert slots (summed into y by k_conv_gather).
 // Buffers ping-pong in shared memory when the item's largest vector fits.
 template <int D, typename V>
 __global__ void __launch_bounds__(512) k_level(DevPlan P, const V* __restrict__ zb, V* __restrict__ gm,
-                                               V* __restrict__ scratch, V* __restrict__ y, int32_t item0,
+                                               V* __restrict__ scratch, V* __restrict__ conv, int32_t item0,
                                                int64_t buf_elems) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const lsg::PhaseBItem it = P.b_items[item0 + blockIdx.x];
@@ -616,7 +621,7 @@ __global__ void __launch_bounds__(512) k_level(DevPlan P, const V* __restrict__ 
             if (j == D - 1) {
                 const int32_t* src = P.conv_src + so * 5;
                 const int32_t* code = P.conv_code + so;
-                const int64_t* outmap = P.exa + P.exa_off[tc];
+                V* out = conv + P.conv_off[item0 + blockIdx.x];
                 for (int64_t e = threadIdx.x; e < nout; e += blockDim.x) {
                     int cd = code[e];
                     V acc = V(0);
@@ -626,7 +631,7 @@ __global__ void __launch_bounds__(512) k_level(DevPlan P, const V* __restrict__ 
                         if (i < 0) break;
                         acc += wcode<V>((cd >> (3 * q)) & 7) * A[i];
                     }
-                    atomicAdd(&y[outmap[e]], acc);
+                    out[e] = acc;
                 }
             } else {
                 stage_gather<5, V, V>(P.conv_src + so * 5, P.conv_code + so, nout, A, nullptr, B);
@@ -637,6 +642,25 @@ __global__ void __launch_bounds__(512) k_level(DevPlan P, const V* __restrict__ 
         }
     }
 }
+
+// y at every active point: the sum of its convert contributions over the
+// items whose restrictions end at its depth, in item order (the reference adds
+// the cases' Ax_neu in CasesIterator order, MatrixVectorHomogen.h:740-748).
+template <typename V>
+__global__ void k_conv_gather(DevPlan P, int64_t na, const V* __restrict__ conv, V* __restrict__ y) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= na) return;
+    const int64_t k = P.exa[g];
+    const int t = P.did[k];
+    const int64_t e = g - P.exa_off[t];
+    V acc = V(0);
+    for (int32_t j = P.conv_items_off[t]; j < P.conv_items_off[t + 1]; ++j) acc += conv[P.conv_off[P.conv_items[j]] + e];
+    y[k] = acc;
+}
+
+}  // namespace
+#include "lsg_sf_kernel.cuh"
+namespace {
 
 // ----------------------------------------------------------------------------- coefficient, diag
 // a(x_c) at the midpoint of every cell of one part of the plan (cells
@@ -863,11 +887,6 @@ __global__ void k_install_learned(int64_t n, const uint8_t* __restrict__ act, co
 }
 
 // ----------------------------------------------------------------------------- vector kernels
-template <typename V>
-__global__ void k_zero_active(const int64_t* __restrict__ exa, int64_t na, V* __restrict__ y) {
-    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e < na) y[exa[e]] = V(0);
-}
 
 constexpr int kRedBlocks = 592;  // 4 x 148 SMs
 constexpr int kRedThreads = 256;
@@ -960,7 +979,7 @@ struct DBuf {
     size_t bytes = 0;
     ~DBuf() { if (p) cudaFree(p); }
     int alloc(size_t b, size_t* total) {
-        if (p) { cudaFree(p); p = nullptr; }
+        if (p) { cudaFree(p); p = nullptr; *total -= bytes; }
         bytes = b;
         if (b == 0) return 0;
         cudaError_t e = cudaMalloc(&p, b);
@@ -991,7 +1010,9 @@ struct lsg_operator {
     size_t dev_bytes = 0;
     // tables
     DBuf slabs, did, act, exa_off, exa, cell_key, cell_corner, nodal_stage, nodal_src, nodal_code, nodal_dom, nodal_scr,
-        conv_stage, conv_src, conv_code, conv_dom, prol, restr, a_items, b_items, b_steps, pts, cell_slab_off;
+        conv_stage, conv_src, conv_code, conv_dom, prol, restr, a_items, b_items, b_steps, pts, cell_slab_off,
+        conv_off, conv_items_off, conv_items;
+    int64_t conv_total = 0;  // convert slots of one matvec
     DBuf lam64, lam32;   // Hadamard-basis eigenvalues of the Q1 stiffness (form 0)
     DBuf mu64, mu32;     // ... of the Q1 mass (form 1)
     DBuf one64, one32;   // unit coefficient per cell (constant-coefficient norms)
@@ -1006,7 +1027,7 @@ struct lsg_operator {
     DBuf nbmask;               // same-depth neighbour flags (features)
     // work buffers per precision
     struct Work {
-        DBuf ml, pc, zb, gm, scratch, nscratch;
+        DBuf ml, pc, zb, gm, scratch, nscratch, conv;
     } w64, w32;
     DBuf xbuf64, ybuf64;  // host-call staging
     DBuf diag;            // Jacobi diagonal (FP64)
@@ -1015,43 +1036,81 @@ struct lsg_operator {
     bool have_learned = false;
     int64_t smem_cap64 = 0, smem_cap32 = 0;
     std::vector<int64_t> level_need;  // per phase-B level: largest vector of any item
-    lsg_tuning tune{256, 8, 4, 512, 12288, 256};  // launch parameters (lsg_operator_autotune)
+    lsg_tuning tune{256, 72, 4, 512, 12288, 256};  // launch parameters (lsg_operator_autotune)
     std::shared_ptr<void> basis;      // basis-transform tables (lsg_basis.cu), built on first use
     std::shared_ptr<void> bdrhs;      // boundary right-hand-side tables (lsg_bdrhs.cu), built on first use
-    DBuf cell_order;                  // phase-B items ordered by slab size (k_cells)
-    std::vector<int32_t> cell_class_off;  // size classes in cell_order
-    std::vector<int64_t> cell_class_n;    // largest N_T per class
+    // cell operator launch plan, per precision: the factorised dense-slab
+    // operator k_sf (slab plans, item order, launch classes by work space) and
+    // k_cells for the items of sparse slabs (order, classes by slab size)
+    lsg::SfCoefLayout sf_layout;
+    DBuf coll64, coll32, coll_off, coll_slab, slab_T, slab_cell_off;  // collapsed coefficients
+    struct SfPrec {
+        DBuf plans, order;
+        std::vector<int32_t> class_off;
+        std::vector<int32_t> class_w;
+        std::vector<uint8_t> ok;  // per slab: the plan fits
+        DBuf cell_order;
+        std::vector<int32_t> cell_class_off;
+        std::vector<int64_t> cell_class_n;
+    } sf32, sf64;
 };
 
 namespace {
 
-// k_cells items by slab size, largest first, in size classes: a new class
-// (launch) starts when slabs shrink by tune.class_ratio; shared memory per
-// launch = 2 N_T of the class's largest slab
-int build_cell_classes(lsg_operator* op) {
+// Launch plan of the cell operator.  Dense slabs go to k_sf (planned per
+// precision for a work space of tune.cell_space_kb, FP64 with half the
+// elements), ordered by work space, largest first, in classes: a new class
+// (launch) starts when the work space shrinks by tune.class_ratio.  Items of
+// sparse slabs (and of dense slabs whose plan does not fit) go to k_cells by
+// slab size, with shared memory for 2 N_T of the class's largest slab.
+int build_sf_prec(lsg_operator* op, lsg_operator::SfPrec& S, int64_t wcap, int na_max) {
     const lsg::Plan& p = op->plan;
-    std::vector<int32_t> ord(p.b_items.size());
-    for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int32_t)i;
+    std::vector<lsg::SfSlab> plans = lsg::sf_plan(p, op->sf_layout, wcap, na_max);
+    S.ok.assign(p.nD, 0);
+    for (int t = 0; t < p.nD; ++t) S.ok[t] = plans[t].nm >= 0 && plans[t].nq <= 6;
+    std::vector<int32_t> ord, cord;
+    for (size_t i = 0; i < p.b_items.size(); ++i) (S.ok[p.b_items[i].t] ? ord : cord).push_back((int32_t)i);
     std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) {
-        return p.slabs[p.b_items[a].t].n > p.slabs[p.b_items[b].t].n;
+        return plans[p.b_items[a].t].wtotal > plans[p.b_items[b].t].wtotal;
     });
-    op->cell_class_off.clear();
-    op->cell_class_n.clear();
+    S.class_off.clear();
+    S.class_w.clear();
     int64_t bound = -1;
     for (size_t i = 0; i < ord.size(); ++i) {
-        int64_t n = p.slabs[p.b_items[ord[i]].t].n;
+        int64_t w = std::max(plans[p.b_items[ord[i]].t].wtotal, 1);
+        if (bound < 0 || w * op->tune.class_ratio < bound) {
+            S.class_off.push_back((int32_t)i);
+            S.class_w.push_back((int32_t)w);
+            bound = w;
+        }
+    }
+    S.class_off.push_back((int32_t)ord.size());
+    std::stable_sort(cord.begin(), cord.end(), [&](int32_t a, int32_t b) {
+        return p.slabs[p.b_items[a].t].n > p.slabs[p.b_items[b].t].n;
+    });
+    S.cell_class_off.clear();
+    S.cell_class_n.clear();
+    bound = -1;
+    for (size_t i = 0; i < cord.size(); ++i) {
+        int64_t n = p.slabs[p.b_items[cord[i]].t].n;
         if (bound < 0 || n * op->tune.class_ratio < bound) {
-            op->cell_class_off.push_back((int32_t)i);
-            op->cell_class_n.push_back(n);
+            S.cell_class_off.push_back((int32_t)i);
+            S.cell_class_n.push_back(n);
             bound = n;
         }
     }
-    op->cell_class_off.push_back((int32_t)ord.size());
-    if (op->cell_order.p && op->cell_order.bytes == ord.size() * sizeof(int32_t)) {
-        CUDA_TRY(cudaMemcpy(op->cell_order.p, ord.data(), ord.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-        return 0;
-    }
-    return op->cell_order.upload(ord, &op->dev_bytes) ? LSG_E_CUDA : 0;
+    S.cell_class_off.push_back((int32_t)cord.size());
+    int rc = S.plans.upload(plans, &op->dev_bytes);
+    if (!rc) rc = S.order.upload(ord, &op->dev_bytes);
+    if (!rc) rc = S.cell_order.upload(cord, &op->dev_bytes);
+    return rc ? LSG_E_CUDA : 0;
+}
+
+int build_cell_classes(lsg_operator* op) {
+    const int64_t w32 = (int64_t)op->tune.cell_space_kb * 1024 / 4, w64 = (int64_t)op->tune.cell_space_kb * 1024 / 8;
+    int rc = build_sf_prec(op, op->sf32, w32, 7);
+    if (!rc) rc = build_sf_prec(op, op->sf64, w64, 3);
+    return rc;
 }
 
 int upload_plan(lsg_operator* op) {
@@ -1110,6 +1169,29 @@ int upload_plan(lsg_operator* op) {
     rc |= op->b_steps.upload(p.b_steps, tot);
     rc |= op->pts.upload(p.pts, tot);
     rc |= op->cell_slab_off.upload(cso, tot);
+    {  // private convert slots per item and, per depth, the items that end there
+        std::vector<int64_t> coff(std::max<size_t>(p.b_items.size(), 1), -1);
+        std::vector<std::vector<int32_t>> per(p.nD);
+        int64_t tot_slots = 0;
+        for (size_t i = 0; i < p.b_items.size(); ++i) {
+            int tc = p.b_items[i].t_conv;
+            if (tc < 0) continue;
+            coff[i] = tot_slots;
+            tot_slots += p.exa_off[tc + 1] - p.exa_off[tc];
+            per[tc].push_back((int32_t)i);
+        }
+        std::vector<int32_t> ioff(p.nD + 1, 0), items;
+        for (int t = 0; t < p.nD; ++t) {
+            ioff[t] = (int32_t)items.size();
+            items.insert(items.end(), per[t].begin(), per[t].end());
+        }
+        ioff[p.nD] = (int32_t)items.size();
+        if (items.empty()) items.push_back(0);
+        op->conv_total = tot_slots;
+        rc |= op->conv_off.upload(coff, tot);
+        rc |= op->conv_items_off.upload(ioff, tot);
+        rc |= op->conv_items.upload(items, tot);
+    }
     if (rc) return LSG_E_CUDA;
     // Hadamard-basis eigenvalues of the Q1 element per depth, 1/2^d folded in
     int nc = 1 << d;
@@ -1166,6 +1248,9 @@ int upload_plan(lsg_operator* op) {
     P.b_items = op->b_items.as<lsg::PhaseBItem>();
     P.b_steps = op->b_steps.as<lsg::PhaseBStep>();
     P.pts = op->pts.as<int32_t>();
+    P.conv_off = op->conv_off.as<int64_t>();
+    P.conv_items_off = op->conv_items_off.as<int32_t>();
+    P.conv_items = op->conv_items.as<int32_t>();
     // per-level largest vector of an item (dynamic shared memory of k_level)
     op->level_need.clear();
     for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
@@ -1179,6 +1264,36 @@ int upload_plan(lsg_operator* op) {
             mx = std::max(mx, need);
         }
         op->level_need.push_back(mx);
+    }
+    // collapsed coefficients of the dense slabs (k_sf): per slab its depths,
+    // first cell and collapsed offset; per collapsed cell its slab
+    op->sf_layout = lsg::sf_coef_layout(p);
+    {
+        const int64_t cc = std::max<int64_t>(op->sf_layout.ccount, 1);
+        std::vector<int32_t> cslab(cc, 0);
+        std::vector<int64_t> coff(p.nD + 1, 0), celloff(p.nD);
+        for (int t = 0; t < p.nD; ++t) {
+            celloff[t] = p.slabs[t].cell_off;
+            coff[t] = op->sf_layout.coef_off[t] < 0 ? 0 : op->sf_layout.coef_off[t];
+        }
+        for (int t = 0; t < p.nD; ++t) {
+            int64_t o = op->sf_layout.coef_off[t];
+            if (o < 0) continue;
+            int64_t c = 1;
+            for (int k = 0; k < d; ++k)
+                if (p.slabs[t].T[k] >= 2) c *= ((int64_t)1 << p.slabs[t].T[k]);
+            std::fill(cslab.begin() + o, cslab.begin() + o + c, t);
+        }
+        std::vector<int32_t> sT(p.nD * (size_t)d);
+        for (int t = 0; t < p.nD; ++t)
+            for (int k = 0; k < d; ++k) sT[(size_t)t * d + k] = p.slabs[t].T[k];
+        rc |= op->coll_slab.upload(cslab, tot);
+        rc |= op->coll_off.upload(coff, tot);
+        rc |= op->slab_T.upload(sT, tot);
+        rc |= op->slab_cell_off.upload(celloff, tot);
+        rc |= op->coll64.alloc(cc * sizeof(double), tot);
+        rc |= op->coll32.alloc(cc * sizeof(float), tot);
+        if (rc) return LSG_E_CUDA;
     }
     return build_cell_classes(op);
 }
@@ -1202,33 +1317,58 @@ int ensure_work(lsg_operator* op, lsg_operator::Work& w) {
     rc |= w.gm.alloc(p.gm_total * sizeof(V), tot);
     rc |= w.scratch.alloc(std::max<int64_t>(p.scratch_total, 1) * sizeof(V), tot);
     rc |= w.nscratch.alloc(std::max<int64_t>(p.nodal_scratch, 1) * sizeof(V), tot);
+    rc |= w.conv.alloc(std::max<int64_t>(op->conv_total, 1) * sizeof(V), tot);
     return rc ? LSG_E_CUDA : 0;
 }
 
-template <int D, typename V>
+// Dynamic shared memory above 48 KB needs an opt-in per kernel and device;
+// both precisions are set on the first call for a dimension on a device, so
+// that no attribute call happens later (e.g. inside a stream capture).
+template <int D>
 int set_phaseB_smem() {
-    static bool done = false;
-    if (done) return 0;
-    CUDA_TRY(cudaFuncSetAttribute(k_cells<D, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-    CUDA_TRY(cudaFuncSetAttribute(k_level<D, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-    done = true;
+    static bool done[256] = {};
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return fail(LSG_E_INVALID, "device ordinal out of range");
+    if (done[dev]) return 0;
+    CUDA_TRY(cudaFuncSetAttribute(k_cells<D, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_cells<D, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_level<D, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_level<D, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_sf<float, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_sf<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
+    done[dev] = true;
     return 0;
 }
 
 // Phase B: k_cells per size class, then one k_level per restriction wavefront.
 template <int D, typename V>
-int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* y, const V* acell, const V* lam,
-                  cudaStream_t st) {
+int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* conv, V* y, const V* acell,
+                  const V* lam, cudaStream_t st) {
     const lsg::Plan& p = op->plan;
+    constexpr bool F32 = std::is_same<V, float>::value;
+    const lsg_operator::SfPrec& S = F32 ? op->sf32 : op->sf64;
+    const V* coll = F32 ? (const V*)op->coll32.p : (const V*)op->coll64.p;
+    for (size_t c = 0; c + 1 < S.class_off.size(); ++c) {
+        int32_t b = S.class_off[c], e = S.class_off[c + 1];
+        size_t smem = (size_t)S.class_w[c] * sizeof(V);
+        if (F32)
+            k_sf<float, 7><<<e - b, op->tune.cell_threads, smem, st>>>(
+                op->b_items.as<lsg::PhaseBItem>(), S.plans.as<lsg::SfSlab>(), (const float*)pc, (float*)zb,
+                (const float*)coll, S.order.as<int32_t>(), b, op->unit_coef ? 1 : 0, op->form);
+        else
+            k_sf<double, 3><<<e - b, op->tune.cell_threads, smem, st>>>(
+                op->b_items.as<lsg::PhaseBItem>(), S.plans.as<lsg::SfSlab>(), (const double*)pc, (double*)zb,
+                (const double*)coll, S.order.as<int32_t>(), b, op->unit_coef ? 1 : 0, op->form);
+    }
     const int64_t cap_elems = (200 * 1024) / sizeof(V) - (1 << D);
-    for (size_t c = 0; c + 1 < op->cell_class_off.size(); ++c) {
-        int32_t b = op->cell_class_off[c], e = op->cell_class_off[c + 1];
-        int64_t need = 2 * op->cell_class_n[c];
+    for (size_t c = 0; c + 1 < S.cell_class_off.size(); ++c) {
+        int32_t b = S.cell_class_off[c], e = S.cell_class_off[c + 1];
+        int64_t need = 2 * S.cell_class_n[c];
         int64_t alloc = need <= cap_elems ? need : 0;
         size_t smem = (size_t)((1 << D) + alloc) * sizeof(V);
         k_cells<D, V><<<e - b, op->tune.cell_threads, smem, st>>>(op->dp, pc, zb, acell, lam,
-                                                                  op->cell_order.as<int32_t>(), b, alloc,
-                                                                  op->tune.cell_segment);
+                                                                  S.cell_order.as<int32_t>(), b, alloc, 8);
     }
     // elements per ping-pong buffer (two buffers within the 220 KB opt-in)
     const int64_t lvl_cap = std::min<int64_t>(op->tune.level_cap, (110 * 1024) / sizeof(V));
@@ -1236,8 +1376,11 @@ int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* y,
         int32_t b = p.b_level_off[L], e = p.b_level_off[L + 1];
         if (e <= b) continue;
         int64_t bufn = std::min<int64_t>(op->level_need[L], lvl_cap);
-        k_level<D, V><<<e - b, op->tune.level_threads, 2 * bufn * sizeof(V), st>>>(op->dp, zb, gm, scratch, y, b, bufn);
+        k_level<D, V><<<e - b, op->tune.level_threads, 2 * bufn * sizeof(V), st>>>(op->dp, zb, gm, scratch, conv, b,
+                                                                                    bufn);
     }
+    int64_t na = p.exa_off[p.nD];
+    if (na > 0) k_conv_gather<V><<<nblk(na), 256, 0, st>>>(op->dp, na, conv, y);
     CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -1249,14 +1392,12 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t
     lsg_operator::Work& w = std::is_same<V, double>::value ? op->w64 : op->w32;
     int rc = ensure_work<V>(op, w);
     if (rc) return rc;
-    rc = set_phaseB_smem<D, V>();
+    rc = set_phaseB_smem<D>();
     if (rc) return rc;
     const V* acell = cell_coef<V>(op);
     const V* lam = std::is_same<V, double>::value ? (const V*)(op->form ? op->mu64.p : op->lam64.p)
                                                   : (const V*)(op->form ? op->mu32.p : op->lam32.p);
-    int64_t na = p.exa_off[p.nD];
     if (ev) cudaEventRecord(ev[0], st);
-    if (na > 0) k_zero_active<V><<<nblk(na), 256, 0, st>>>(op->dp.exa, na, y);
     k_nodal<V><<<p.nD, 256, 0, st>>>(op->dp, x, w.ml.as<V>(), w.nscratch.as<V>());
     if (ev) cudaEventRecord(ev[1], st);
     int32_t nb = (int32_t)p.b_items.size();
@@ -1267,7 +1408,8 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t
         if (e > b) k_prolong<V><<<e - b, op->tune.prolong_threads, 0, st>>>(op->dp, w.pc.as<V>(), b);
     }
     if (ev) cudaEventRecord(ev[3], st);
-    rc = phaseB_launch<D, V>(op, w.pc.as<V>(), w.zb.as<V>(), w.gm.as<V>(), w.scratch.as<V>(), y, acell, lam, st);
+    rc = phaseB_launch<D, V>(op, w.pc.as<V>(), w.zb.as<V>(), w.gm.as<V>(), w.scratch.as<V>(), w.conv.as<V>(), y, acell,
+                             lam, st);
     if (rc) return rc;
     if (ev) cudaEventRecord(ev[4], st);
     CUDA_TRY(cudaGetLastError());
@@ -1279,7 +1421,7 @@ int prepare_impl(lsg_operator* op) {
     lsg_operator::Work& w = std::is_same<V, double>::value ? op->w64 : op->w32;
     int rc = ensure_work<V>(op, w);
     if (rc) return rc;
-    return set_phaseB_smem<D, V>();
+    return set_phaseB_smem<D>();
 }
 
 // allocations and function attributes that must not happen during graph capture
@@ -1390,6 +1532,25 @@ int set_part_coefficient(lsg_operator* op, int part, int32_t family, const doubl
                                                 pp, op->acell64.as<double>(), op->acell32.as<float>(),
                                                 op->cell_slab_off.as<int64_t>());
     CUDA_TRY(cudaGetLastError());
+    {  // collapsed coefficients of this part's dense slabs (k_sf)
+        int t_lo = p.inst_t_off[part], t_hi = p.inst_t_off[part + 1];
+        int64_t lo = -1, hi = -1;
+        for (int t = t_lo; t < t_hi; ++t) {
+            int64_t o = op->sf_layout.coef_off[t];
+            if (o < 0) continue;
+            if (lo < 0) lo = o;
+            int64_t c = 1;
+            for (int k = 0; k < p.d; ++k)
+                if (p.slabs[t].T[k] >= 2) c *= ((int64_t)1 << p.slabs[t].T[k]);
+            hi = o + c;
+        }
+        if (lo >= 0 && hi > lo)
+            k_sf_collapse<<<nblk(hi - lo), 256>>>(op->slab_T.as<int32_t>(), p.d, op->slab_cell_off.as<int64_t>(),
+                                                   op->coll_off.as<int64_t>(), op->coll_slab.as<int32_t>(), lo, hi,
+                                                   op->acell64.as<double>(), op->coll64.as<double>(),
+                                                   op->coll32.as<float>());
+        CUDA_TRY(cudaGetLastError());
+    }
     CUDA_TRY(cudaDeviceSynchronize());
     op->part_coef[part] = 1;
     op->have_coef = std::all_of(op->part_coef.begin(), op->part_coef.end(), [](uint8_t v) { return v != 0; });
@@ -1416,7 +1577,8 @@ const lsg::Plan& plan(const lsg_operator* op) { return op->plan; }
 size_t device_bytes(const lsg_operator* op) { return op->dev_bytes; }
 int64_t matvec_launch_count(const lsg_operator* op) {
     const lsg::Plan& p = op->plan;
-    return 3 + (int64_t)(p.a_level_off.size() - 1) + (int64_t)op->cell_class_off.size() - 1 +
+    return 3 + (int64_t)(p.a_level_off.size() - 1) + (int64_t)op->sf32.class_off.size() - 1 +
+           (int64_t)op->sf32.cell_class_off.size() - 1 +
            (int64_t)(p.b_level_off.size() - 1);
 }
 int fail_msg(int code, const char* msg) { return fail(code, msg); }
@@ -1664,6 +1826,36 @@ int lsg_plan_export_sorted_depths(const lsg_plan* p, int32_t c, int32_t* ids, in
 int lsg_plan_export_cell_counts(const lsg_plan* p, int64_t* counts) {
     if (!p || !counts) return fail(LSG_E_INVALID, "null argument");
     for (int t = 0; t < p->plan.nD; ++t) counts[t] = p->plan.slabs[t].ncell;
+    return 0;
+}
+int lsg_plan_check_slab_operator(const lsg_plan* p, int32_t t, int32_t form, int64_t wcap, int32_t na_max,
+                                 const double* acell, const double* u, double* z_cells, double* z_sf, int32_t* info) {
+    if (!p || !acell || !u || !z_cells || !z_sf) return fail(LSG_E_INVALID, "null argument");
+    const lsg::Plan& P = p->plan;
+    if (t < 0 || t >= P.nD) return fail(LSG_E_INVALID, "depth id out of range");
+    if (!P.slabs[t].dense) return fail(LSG_E_INVALID, "the factorised operator covers dense slabs only");
+    if (form != LSG_FORM_STIFFNESS && form != LSG_FORM_MASS) return fail(LSG_E_INVALID, "unknown operator form");
+    lsg::cells_apply_host(P, t, form, acell, u, z_cells);
+    lsg::SfCoefLayout L = lsg::sf_coef_layout(P);
+    std::vector<lsg::SfSlab> sf = lsg::sf_plan(P, L, wcap, na_max);
+    const lsg::SfSlab& D = sf[t];
+    if (D.nm < 0) return fail(LSG_E_INVALID, "the slab's two innermost dimensions do not fit the work space");
+    int64_t cc = 1;
+    for (int k = 0; k < P.d; ++k)
+        if (P.slabs[t].T[k] >= 2) cc *= ((int64_t)1 << P.slabs[t].T[k]);
+    std::vector<double> coef(cc);
+    lsg::sf_collapse_host(P, t, acell, L, coef.data());
+    lsg::sf_apply_host(D, form, coef.data(), u, z_sf);
+    if (info) {
+        int ncol = 0;
+        for (int k = 0; k < P.d; ++k) ncol += P.slabs[t].T[k] == 1;
+        info[0] = D.nm;
+        info[1] = D.nq;
+        info[2] = D.nchunk;
+        info[3] = D.a.T < 0 ? 0 : D.a.n;
+        info[4] = D.b.T < 0 ? 0 : D.b.n;
+        info[5] = ncol;
+    }
     return 0;
 }
 int lsg_plan_export_slab(const lsg_plan* p, int32_t t, int64_t* idx, int64_t* count) {
@@ -2206,8 +2398,7 @@ __global__ void k_pattern(int64_t n, double* x64, float* x32) {
 
 bool tuning_valid(const lsg_tuning& t) {
     auto warps = [](int v, int lo, int hi) { return v >= lo && v <= hi && v % 32 == 0; };
-    return warps(t.cell_threads, 64, 256) && t.cell_segment >= 1 && t.cell_segment <= 64 &&
-           (t.cell_segment & (t.cell_segment - 1)) == 0 && t.class_ratio >= 2 &&
+    return warps(t.cell_threads, 64, 256) && t.cell_space_kb >= 16 && t.cell_space_kb <= 200 && t.class_ratio >= 2 &&
            t.class_ratio <= 1024 && warps(t.level_threads, 32, 512) && t.level_cap >= 256 && t.level_cap <= 65536 &&
            warps(t.prolong_threads, 32, 1024);
 }
@@ -2277,7 +2468,7 @@ extern "C" int lsg_operator_autotune(lsg_operator* op, int32_t precision, int32_
     lsg_tuning cur = start;
     double cur_ms = time_cfg(cur), def_ms = cur_ms;
     const std::vector<std::pair<int32_t lsg_tuning::*, std::vector<int32_t>>> space = {
-        {&lsg_tuning::cell_segment, {4, 8, 16}},      {&lsg_tuning::cell_threads, {128, 256}},
+        {&lsg_tuning::cell_space_kb, {48, 72, 100}},  {&lsg_tuning::cell_threads, {128, 256}},
         {&lsg_tuning::class_ratio, {2, 4, 16}},       {&lsg_tuning::level_threads, {64, 128, 256, 512}},
         {&lsg_tuning::level_cap, {4096, 8192, 12288}}, {&lsg_tuning::prolong_threads, {128, 256, 512}}};
     for (int pass = 0; pass < 2 && !err; ++pass) {
@@ -2351,7 +2542,8 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
     size_t b_gm = align256(p.gm_total * sizeof(V));
     size_t b_sc = align256(std::max<int64_t>(p.scratch_total, 1) * sizeof(V));
     size_t b_ns = align256(std::max<int64_t>(p.nodal_scratch, 1) * sizeof(V));
-    size_t need = b_ml + b_pc + b_zb + b_gm + b_sc + b_ns;
+    size_t b_cv = align256(std::max<int64_t>(op->conv_total, 1) * sizeof(V));
+    size_t need = b_ml + b_pc + b_zb + b_gm + b_sc + b_ns + b_cv;
     if (need > LSG_NOALLOC_SCRATCH_BYTES)
         return fail(LSG_E_INVALID, "lsg_matvec_device_noalloc: this grid needs " + std::to_string(need) +
                                        " bytes of work space, the fixed array holds " +
@@ -2363,17 +2555,16 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
     V* gm = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb);
     V* scratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm);
     V* nscratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm + b_sc);
-    int rc = set_phaseB_smem<D, V>();
+    V* conv = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm + b_sc + b_ns);
+    int rc = set_phaseB_smem<D>();
     if (rc) return rc;
     const V* acell = cell_coef<V>(op);
     const V* lam = std::is_same<V, double>::value ? (const V*)(op->form ? op->mu64.p : op->lam64.p)
                                                   : (const V*)(op->form ? op->mu32.p : op->lam32.p);
     // Every region is written before it is read within one call (nodal slabs by
     // k_nodal, P by k_pinit, gM only where an earlier item of the same call
-    // wrote it, item scratch by its own item), so nothing needs clearing;
-    // y is zeroed at active points as in the allocating path.
-    int64_t na = p.exa_off[p.nD];
-    if (na > 0) k_zero_active<V><<<nblk(na), 256, 0, st>>>(op->dp.exa, na, y);
+    // wrote it, item scratch and convert slots by their own item), so nothing
+    // needs clearing; every active entry of y is written by the final gather.
     k_nodal<V><<<p.nD, 256, 0, st>>>(op->dp, x, ml, nscratch);
     int32_t nb = (int32_t)p.b_items.size();
     if (nb > 0) k_pinit<V><<<nb, 256, 0, st>>>(op->dp, ml, pc, 0);
@@ -2381,7 +2572,7 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
         int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
         if (e > b) k_prolong<V><<<e - b, op->tune.prolong_threads, 0, st>>>(op->dp, pc, b);
     }
-    rc = phaseB_launch<D, V>(op, pc, zb, gm, scratch, y, acell, lam, st);
+    rc = phaseB_launch<D, V>(op, pc, zb, gm, scratch, conv, y, acell, lam, st);
     if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
     return 0;

@@ -65,7 +65,14 @@ CASES = [
     ("d8_L2", 8, "level=2", EXPSIN6, ["tables", "matvec", "poisson", "prew2nodal", "nodal2prew"]),
     # the CPU-runnable configuration: d = 3, level 7 (7,423 points), a = 1 + 0.5 prod sin(pi x_i)
     ("d3_L7", 3, "level=7", SINPROD, ["matvec", "poisson", "diag", "cg"]),
+    # the benchmark's grid family (regular grid refined toward the corner, completed;
+    # hanging nodes) at sizes the compiled reference solves in minutes
+    ("d5_corner", 5, "level=3 refine=2 theta=0.6 target=corner", EXPSIN6, ["tables", "matvec", "diag", "cg"]),
+    ("d6_corner", 6, "level=3 refine=2 theta=0.6 target=corner", EXPSIN6, ["tables", "matvec", "diag", "cg"]),
+    ("d5_corner_L4", 5, "level=4 refine=2 theta=0.6 target=corner", SINPROD_M, ["matvec", "diag"]),
 ]
+# per-cell corner dumps grow as 2^(2d) per cell; fixtures named here keep the counts only
+NO_CELL_DUMP = {"d5_corner", "d6_corner"}
 
 
 # boundary-data right-hand sides: name, d, grid args, boundary-value family (g)
@@ -187,7 +194,7 @@ def make_case(name, d, gridargs, coef, cmds, refsrc):
                     except ValueError:
                         pass
     out["gridargs"] = np.array(gridargs)
-    if d >= 7:  # per-cell corner dumps grow as 2^(2d) per cell; keep the counts only
+    if d >= 7 or name in NO_CELL_DUMP:  # per-cell corner dumps grow as 2^(2d) per cell; keep the counts only
         out.pop("tables_cells", None)
         out.pop("tables_cell_corners", None)
     path = os.path.join(HERE, f"{name}.npz")

@@ -14,9 +14,9 @@ pytestmark = pytest.mark.gpu
 
 SETTINGS = [
     dict(cell_threads=128),
-    dict(cell_segment=1),
-    dict(cell_segment=4, class_ratio=2),
-    dict(cell_segment=64, class_ratio=1024),
+    dict(cell_space_kb=16),                    # small work space: more slabs chunked
+    dict(cell_space_kb=48, class_ratio=2),
+    dict(cell_space_kb=200, class_ratio=1024),
     dict(level_threads=32, level_cap=256),     # most wavefront items spill to global scratch
     dict(level_threads=64, level_cap=65536),
     dict(level_threads=512),
@@ -53,7 +53,7 @@ def test_every_setting_matches_reference(cases, setting):
 
 def test_invalid_settings_are_rejected(cases):
     _, _, m = make(cases[0])
-    for bad in (dict(cell_threads=512), dict(cell_threads=100), dict(cell_segment=0), dict(class_ratio=1),
+    for bad in (dict(cell_threads=512), dict(cell_threads=100), dict(cell_space_kb=8), dict(class_ratio=1),
                 dict(level_threads=1024), dict(level_cap=16), dict(prolong_threads=2048)):
         with pytest.raises(lsg.LsgError):
             m.set_tuning(**bad)
