@@ -4,10 +4,22 @@
 
 One step = one solve of A x = f from x = 0 to ||f - A x|| / ||f|| <= 1e-10
 (FP32 matvec inside FP64 iterative refinement, Jacobi or learned diagonal
-preconditioner), inputs resident in HBM.  The JSON line also carries the plain
-FP64 CG time on the same instance, the matvec GB/s, the roofline of the
-restriction-wavefront kernel (the dominant one), the end-to-end time through
-the C-ABI with host buffers, and the reference's CPU time on a bounded sample.
+preconditioner), inputs resident in HBM.  The default workload is the
+mixed-precision configuration: a d=6 grid of 1,494,847 points (regular level
+8 refined one round toward the corner, completed).  The JSON line also
+carries the plain FP64 CG time on the same instance and the FP32+IR
+solution's distance to it, the matvec times and GB/s, the roofline of the
+cell-operator kernel (the dominant one), the end-to-end time through the C-ABI
+with host buffers, and a same-instance leg: the CPU-runnable configuration
+(d=3 level 7, 7,423 points) solved on the GPU with the right-hand side the
+reference arm solves.
+
+--impl reference runs the reference's own CG::solveHomogen (oracle/_ref, the
+LoAdSG sources compiled in place; the -O3 timing build when present) on that
+CPU-runnable instance on the host cores, measured, never scaled.  The
+mixed-precision workload is out of the reference's reach (fixed hash
+capacities, sgrid/sparseGrid.cc:46 and multilevelSparseGrid.h:21; O(N^2) grid
+completion, GridGeneration.cpp:333-392).
 Multi-GPU runs (torchrun) solve one independent instance per rank (weak
 scaling, no collective on the data path).
 """
@@ -33,7 +45,16 @@ def workload(name, rank):
     """Seeded synthetic instance: (grid, coefficient family, params, f, description)."""
     import loadsg_b200 as lsg
     rng = np.random.default_rng(1000 + rank)
-    if name == "d6_adaptive_corner":
+    if name == "d6_corner_L8":
+        # d=6 grid refined toward the corner (0,...,0): regular level 8, one round
+        # adding the sons of every active point with max_k x_k < 0.6, then the
+        # reference's completion (hanging nodes included): 1,494,847 points
+        g = lsg.AdaptiveSparseGrid.adaptive(6, 8, 1, 0.6, "corner")
+        c = rng.normal(0.0, 0.3, 6)
+        fam, params = lsg.COEF_EXPSIN, list(c)
+        desc = ("d=6 adaptive grid: regular level 8 refined 1 round toward the corner (max_k x_k < 0.6) "
+                "+ completeDirichletGrid; a=exp(sum_k c_k sin(k pi x_k)), c_k~N(0,0.3^2); f~U[-1,1] on active points")
+    elif name == "d6_adaptive_corner":
         # d=6 grid refined toward the corner (0,...,0): regular level 7, then 3
         # rounds adding the sons of every active point with max_k x_k < 0.6*2^(1-r),
         # then the reference's completion (hanging nodes included): 499,107 points
@@ -52,10 +73,22 @@ def workload(name, rank):
         g = lsg.AdaptiveSparseGrid.regular(3, 7)
         fam, params = lsg.COEF_SINPROD, [1.0, 0.5, 1.0, 1.0, 1.0]
         desc = "d=3 regular sparse grid level 7, a=1+0.5 prod sin(pi x_i)"
+        return g, fam, params, config1_rhs(g.n), desc
     else:
         raise SystemExit(f"unknown workload {name}")
     f = rng.uniform(-1.0, 1.0, g.n) * g.active
     return g, fam, params, f, desc
+
+
+# The CPU-runnable configuration, solved by both arms: d=3 regular level 7
+# (AddRecursiveSonsOfPoint(center, 7): 7,423 points, all active), a = 1 + 0.5
+# prod sin(pi x_i), f_k ~ U[-1,1] i.i.d. from seed 0 in storage order.
+CONFIG1 = {"workload": "d3_regular_L7", "d": 3, "level": 7, "n_points": 7423, "coef": "1+0.5 prod sin(pi x_i)",
+           "rhs": "f ~ U[-1,1], seed 0, storage order", "tolerance": 1e-10}
+
+
+def config1_rhs(n):
+    return np.random.default_rng(0).uniform(-1.0, 1.0, n)
 
 
 class ClockSampler:
@@ -121,56 +154,81 @@ def host_cores():
     return max(1, n)
 
 
-def workload_points(name):
-    """Point count of a workload grid (host-side grid generator, no GPU)."""
-    import loadsg_b200 as lsg
-    if name == "d6_adaptive_corner":
-        return lsg.AdaptiveSparseGrid.adaptive(6, 7, 3, 0.6, "corner").n
-    if name.startswith("d6_regular_L"):
-        return lsg.AdaptiveSparseGrid.regular(6, int(name.split("L")[1])).n
-    return lsg.AdaptiveSparseGrid.regular(3, 7).n
+def reference_exe(d):
+    """The reference harness: the -O3 timing build when it runs here, else the
+    golden-vector build (-O2); (path, build name) or (None, reason)."""
+    for sub, name in ((f"fast_d{d}", "-O3 -march=x86-64-v3"), (f"d{d}", "-O2 -march=x86-64-v2")):
+        exe = os.path.join(ROOT, "oracle", "_ref", sub, "ref_harness")
+        if os.path.exists(exe):
+            try:
+                with tempfile.TemporaryDirectory() as tmp:
+                    subprocess.run([exe, "grid", tmp, "level=1"], check=True, capture_output=True, timeout=60)
+                return exe, name
+            except (subprocess.SubprocessError, OSError):
+                continue
+    return None, f"oracle/_ref/(fast_)d{d}/ref_harness missing or not runnable on this host"
 
 
-def cpu_reference_sample(args):
-    """The reference's own CG (oracle/_ref, compiled from the LoAdSG sources) on
-    the largest instance of the workload family it handles in seconds."""
-    d = 6 if args.workload.startswith("d6") else 3
-    exe = os.path.join(ROOT, "oracle", "_ref", f"d{d}", "ref_harness")
-    level = 3 if d == 6 else 5
-    if not os.path.exists(exe):
-        return {"value": None, "unit": "s", "cores": 0, "kind": "reference", "sample": f"{exe} missing"}
+def reference_config1(steps, warmup):
+    """CG::solveHomogen of the reference (applications/cg_method.h:759-886) on the
+    CPU-runnable instance, on the host cores, measured (never scaled).  Its stop
+    rule is r^T D^-1 r <= eps; eps = 1e-20 f^T D^-1 f asks for a relative
+    (preconditioned) residual of 1e-10, with D the reference's own Jacobi
+    diagonal (Preconditioning, cg_method.h:81-754, command "diag").  The true
+    relative residual is recomputed by the harness."""
+    exe, build = reference_exe(3)
+    if exe is None:
+        return {"value": None, "unit": "s", "cores": 0, "kind": "reference", "sample": build}
     cores = host_cores()
-    env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_WAIT_POLICY="PASSIVE")
-    rng = np.random.default_rng(0)
+    common = [f"level={CONFIG1['level']}", "coef=1", "cp=1,0.5,1,1,1"]
+    times, reps = [], []
     with tempfile.TemporaryDirectory() as tmp:
-        subprocess.run([exe, "grid", tmp, f"level={level}"], check=True, capture_output=True, env=env)
+        subprocess.run([exe, "grid", tmp] + common, check=True, capture_output=True,
+                       env=dict(os.environ, OMP_NUM_THREADS="1"))
         n = int([l.split()[1] for l in open(os.path.join(tmp, "meta_grid.txt")) if l.startswith("N ")][0])
-        act = np.fromfile(os.path.join(tmp, "active.u8"), np.uint8)
-        f = rng.uniform(-1, 1, n) * act
+        f = config1_rhs(n)
         f.tofile(os.path.join(tmp, "f.f64"))
-        coef = ["coef=2", "cp=" + ",".join(str(v) for v in rng.normal(0, 0.3, 6))] if d == 6 else \
-               ["coef=1", "cp=1,0.5,1,1,1"]
-        # eps on r^T D^-1 r chosen as 1e-20 * f^T D^-1 f ~ 1e-10 relative residual
-        t0 = time.perf_counter()
-        try:
-            subprocess.run([exe, "cg", tmp, f"level={level}", f"f={tmp}/f.f64", "eps=1e-20"] + coef, check=True,
-                           capture_output=True, env=env, timeout=300)
-        except subprocess.TimeoutExpired:
-            return {"value": None, "unit": "s", "cores": cores, "kind": "reference",
-                    "sample": f"reference CG on d={d} level {level} did not finish within 300 s on {cores} threads"}
-        wall = time.perf_counter() - t0
-        meta = dict(l.split()[:2] for l in open(os.path.join(tmp, "meta_cg.txt")) if len(l.split()) >= 2)
-    secs = float(meta.get("solve_seconds", wall))
-    # scaled to the workload: same iteration count, cost linear in the points
-    # (a lower bound: the reference's iteration count and per-point cost both
-    # grow with the grid)
-    n_work = workload_points(args.workload)
-    return {"value": secs * n_work / n, "unit": "s", "cores": cores, "kind": "reference",
-            "sample": f"reference CG::solveHomogen (Jacobi) on d={d} regular level {level} (N={n}): {secs:.2f} s, "
-                      f"{meta.get('iterations')} iterations, rel.res {meta.get('relres')}; value = that time x "
-                      f"{n_work}/{n} points (linear scaling, a lower bound); the full workload is infeasible for the "
-                      "reference (fixed hash capacities, O(N^2) grid completion)",
-            "sample_seconds": secs, "sample_points": n, "per_dof_us": secs / n * 1e6}
+        # thread count: the reference's matvec is nearly serial and OpenMP can
+        # oversubscribe a container's cores, so one timed matvec per candidate
+        # picks the fastest setting
+        probe = {}
+        for t in sorted({1, 2, 4, cores}):
+            if t > cores:
+                continue
+            env_t = dict(os.environ, OMP_NUM_THREADS=str(t), OMP_WAIT_POLICY="PASSIVE")
+            try:
+                subprocess.run([exe, "matvec", tmp, f"x={tmp}/f.f64"] + common, check=True, capture_output=True,
+                               env=env_t, timeout=60)
+                meta = dict(l.split()[:2] for l in open(os.path.join(tmp, "meta_matvec.txt")) if len(l.split()) >= 2)
+                probe[t] = float(meta["matvec_seconds"])
+            except (subprocess.SubprocessError, KeyError, OSError):
+                continue
+        threads = min(probe, key=probe.get) if probe else 1
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_WAIT_POLICY="PASSIVE")
+        subprocess.run([exe, "diag", tmp] + common, check=True, capture_output=True, env=env, timeout=300)
+        dg = np.fromfile(os.path.join(tmp, "diag.f64"))
+        eps = 1e-20 * float(np.sum(f * f / dg))
+        for k in range(max(0, min(warmup, 1)) + steps):
+            try:
+                subprocess.run([exe, "cg", tmp, f"f={tmp}/f.f64", f"eps={eps!r}"] + common, check=True,
+                               capture_output=True, env=env, timeout=600)
+            except subprocess.TimeoutExpired:
+                return {"value": None, "unit": "s", "cores": cores, "kind": "reference",
+                        "sample": f"reference CG on {CONFIG1['workload']} did not finish within 600 s"}
+            meta = dict(l.split()[:2] for l in open(os.path.join(tmp, "meta_cg.txt")) if len(l.split()) >= 2)
+            if k >= min(warmup, 1):
+                times.append(float(meta["solve_seconds"]))
+                reps.append(meta)
+        x_ref = np.fromfile(os.path.join(tmp, "x.f64"))
+    last = reps[-1]
+    return {"value": float(np.mean(times)), "unit": "s", "cores": threads, "kind": "reference",
+            "build": build, "threads": threads, "host_cores": cores, "matvec_seconds_by_threads": probe,
+            "iterations": int(last["iterations"]),
+            "rel_residual": float(last["relres"]), "precond_seconds": float(last["precond_seconds"]),
+            "eps": eps, "times": times, "n_points": n, "x_norm": float(np.linalg.norm(x_ref)),
+            "sample": (f"the reference's CG::solveHomogen (Jacobi) on {CONFIG1['workload']} ({n} points), "
+                       f"eps = 1e-20 f^T D^-1 f, {threads} thread(s) (fastest of {sorted(probe)} by a timed matvec), "
+                       f"{build}, measured over {len(times)} solve(s)")}
 
 
 def boundary_rhs_leg(lsg, torch, stream, reference=True):
@@ -238,6 +296,54 @@ def boundary_rhs_leg(lsg, torch, stream, reference=True):
                                           "mass_coeff_s": float(meta["coeff_seconds"])}
             except (subprocess.SubprocessError, KeyError, OSError) as e:
                 out["reference_d3_L5"] = {"unavailable": str(e)[:200]}
+    return out
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the cell-operator
+# launches of one FP32 matvec, from an ncu capture of the same workload; not
+# measured in the bench run itself
+TRAFFIC = {}
+TRAFFIC_SOURCE = None
+
+
+def same_instance_leg(lsg, torch, dev, stream, steps, ref=True):
+    """The CPU-runnable configuration solved on the GPU with the right-hand side
+    the reference arm solves (same grid, storage order and coefficient): FP64
+    CG with the Jacobi diagonal (the reference's method) and FP32+IR with it,
+    both to ||f - A x|| / ||f|| <= 1e-10, device time (mean of `steps` after a
+    warm-up) and through host buffers; then the reference itself on the host."""
+    g, fam, params, f_host, desc = workload("d3_regular_L7", 0)
+    prob = lsg.MidpointDiffusion(fam, params)
+    m = lsg.MatrixVectorHomogen(g, prob)
+    f = torch.tensor(f_host, dtype=torch.float64, device=dev)
+    x = torch.zeros_like(f)
+    out = {"config": dict(CONFIG1), "description": desc}
+    xs = {}
+    for name, prec in (("fp64_cg_jacobi", lsg.FP64), ("fp32_ir_jacobi", lsg.FP32)):
+        o = lsg.SolverOpts(1e-10, 1, 3000, 0, prec, 1000, 1e-5, 1)
+        x.zero_()
+        lsg.CG.solve_device(m, f.data_ptr(), x.data_ptr(), o, stream)  # warm-up (diagonal, graphs)
+        secs = []
+        for _ in range(max(1, steps)):
+            x.zero_()
+            r = lsg.CG.solve_device(m, f.data_ptr(), x.data_ptr(), o, stream)
+            secs.append(r["seconds"])
+        xs[name] = x.clone()
+        xh = np.zeros(g.n)
+        t0 = time.perf_counter()
+        rh = lsg.CG.solveHomogen(1e-10, xh, f_host, m, prob, criterion=1, precision=prec, max_iter=3000,
+                                 precond=0, inner_iter=1000, inner_tol=1e-5)
+        host_s = time.perf_counter() - t0
+        out[name] = {"seconds": float(np.mean(secs)), "iterations": r["iterations"],
+                     "rel_residual": r["rel_residual"], "host_buffer_seconds": host_s,
+                     "host_buffer_iterations": rh["iterations"]}
+    out["fp32_ir_vs_fp64_solution_rel_diff"] = float(
+        torch.linalg.norm(xs["fp32_ir_jacobi"] - xs["fp64_cg_jacobi"]) / torch.linalg.norm(xs["fp64_cg_jacobi"]))
+    if ref:
+        res = reference_config1(steps, 1)
+        out["reference"] = res
+        log(f"same instance: reference {res.get('value')} s ({res.get('iterations')} iterations)")
+    log(f"same instance: FP64 {out['fp64_cg_jacobi']['seconds']:.4f} s, FP32+IR {out['fp32_ir_jacobi']['seconds']:.4f} s")
     return out
 
 
@@ -331,10 +437,10 @@ def d8_sweep(lsg, torch, solve_up_to=40000):
         ms64, by64, _ = m.profile(x64.data_ptr(), y64.data_ptr(), lsg.FP64, 2)
         line = {"sweep": "d8_plane", "level": level, "refine": 2, "n_points": g.n, "n_active": g.getDOFS(),
                 "case_cells": int(info["case_cells"]), "device_bytes": int(info["device_bytes"]),
-                "setup_seconds": setup, "fp32_ms": ms32[4], "fp64_ms": ms64[4],
-                "fp32_gbs": by32[4] / (ms32[4] * 1e-3) / 1e9, "fp64_gbs": by64[4] / (ms64[4] * 1e-3) / 1e9,
-                "fp32_hbm_frac": by32[4] / (ms32[4] * 1e-3) / 1e9 / hbm,
-                "cell_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9}
+                "setup_seconds": setup, "fp32_ms": ms32[5], "fp64_ms": ms64[5],
+                "fp32_gbs": by32[5] / (ms32[5] * 1e-3) / 1e9, "fp64_gbs": by64[5] / (ms64[5] * 1e-3) / 1e9,
+                "fp32_hbm_frac": by32[5] / (ms32[5] * 1e-3) / 1e9 / hbm,
+                "cell_op_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9}
         if g.n <= solve_up_to:
             rng = np.random.default_rng(0)
             f = torch.tensor(rng.uniform(-1, 1, g.n) * g.active, device="cuda")
@@ -356,7 +462,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--workload", default="d6_adaptive_corner")
+    ap.add_argument("--workload", default="d6_corner_L8")
     ap.add_argument("--precond", type=int, default=2, help="0 Jacobi, 1 none, 2 learned diagonal")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-bdrhs", action="store_true", help="skip the boundary-data right-hand-side leg")
@@ -365,6 +471,7 @@ def main():
     ap.add_argument("--sweep", action="store_true",
                     help="matvec sweep over d=8 grids refined toward x_1 = 1/2 (one JSON line per grid) instead")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-same-instance", action="store_true", help="skip the CPU-runnable same-instance leg")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -372,13 +479,14 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
+        # the reference's own CPU code only: no part of this repository's library is loaded
         if rank != 0:
             return
-        res = cpu_reference_sample(args)
+        res = reference_config1(args.steps, args.warmup)
         line = {"metric": METRIC, "value": res["value"], "unit": "s", "impl": "reference", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": args.workload}, "cpu_baseline": res,
+                "steps": args.steps, "warmup": min(args.warmup, 1), "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": dict(CONFIG1),
+                "cpu_baseline": res,
                 "e2e": {"value": res["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -479,12 +587,16 @@ def main():
         ev1.record()
         torch.cuda.synchronize()
     step_s = max_over_ranks(ev0.elapsed_time(ev1) / 1e3 / args.steps, dist, dev)
+    x_ir = x.clone()
 
     # plain FP64 CG on the same instance (the comparison the metric names; the
     # reference's CG is always Jacobi-preconditioned), and FP32+IR with Jacobi
     log(f"timed: {step_s:.2f}s per solve")
     rep64 = solve(lsg.FP64, 0, "FP64 CG") or {}
     log(f"FP64 CG: {rep64.get('seconds')}s")
+    # the FP32+IR solution's distance to the FP64 CG solution of the same system
+    sol_err = float(torch.linalg.norm(x_ir - x) / torch.linalg.norm(x)) if rep64 else None
+    log(f"FP32+IR vs FP64 solution: relative difference {sol_err}")
     rep_jac = (solve(lsg.FP32, 0, "FP32+IR Jacobi") or {}) if precond != 0 else reps[-1] if reps else {}
     log(f"FP32+IR Jacobi: {rep_jac.get('seconds')}s")
     # end to end through the C-ABI with host buffers
@@ -501,7 +613,11 @@ def main():
     e2e_s = (time.perf_counter() - te) / args.steps
     log(f"e2e: {e2e_s:.2f}s per solve")
 
-    # matvec bandwidth and the phase-B roofline (CUDA events inside the library)
+    same = None if args.no_same_instance else guarded(
+        lambda: same_instance_leg(lsg, torch, dev, stream, args.steps,
+                                  ref=(not args.no_cpu_baseline and world == 1 and rank == 0)), "same-instance leg")
+
+    # matvec bandwidth and the cell-operator roofline (CUDA events inside the library)
     x32 = torch.randn(g.n, dtype=torch.float32, device=dev)
     y32 = torch.zeros(g.n, dtype=torch.float32, device=dev)
     x64 = x32.double()
@@ -515,11 +631,11 @@ def main():
         hbm, peak_src = float(peaks["hbm_gbs"]), "measured"
     except Exception:
         hbm, peak_src = 6650.0, "fallback"
+    # the cell operator's launches (k_sf, and k_cells for sparse slabs) of one FP32
+    # matvec: algorithmic bytes (slab read, slab written, collapsed coefficients)
+    # over their CUDA-event time
     achieved = by32[3] / (ms32[3] * 1e-3) / 1e9
-    # DRAM bytes of one phase B on this workload, from the ncu capture summarised in
-    # profiles/phaseB_dram_d6_adaptive_corner.md (dram__bytes_read.sum + dram__bytes_write.sum
-    # over the 21 phase-B launches of one FP32 matvec)
-    traffic = 2.23e9 if args.workload == "d6_adaptive_corner" else None
+    traffic = TRAFFIC.get(args.workload)
 
     batch = None if args.no_batch else guarded(lambda: batch_leg(lsg, torch, dev, stream, count=args.batch_grids),
                                                "batch leg")
@@ -532,7 +648,7 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
-    cpu = None if args.no_cpu_baseline or world > 1 else cpu_reference_sample(args)
+    cpu = same.get("reference") if same else None
     last = reps[-1] if reps else {}
     line = {
         "metric": METRIC, "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -544,25 +660,33 @@ def main():
         "iterations": last.get("iterations"), "outer_iterations": last.get("outer_iterations"),
         "rel_residual": last.get("rel_residual"), "failed_solves": failed,
         "fp64_cg": {"seconds": rep64.get("seconds"), "iterations": rep64.get("iterations"),
-                    "rel_residual": rep64.get("rel_residual")},
+                    "rel_residual": rep64.get("rel_residual"), "precond": "jacobi (the reference's method)"},
+        "fp32_ir_vs_fp64_solution_rel_diff": sol_err,
         "speedup_vs_fp64_cg": rep64["seconds"] / step_s if rep64 and step_s > 0 else None,
         "fp32_ir_jacobi": {"seconds": rep_jac.get("seconds"), "iterations": rep_jac.get("iterations"),
                            "rel_residual": rep_jac.get("rel_residual")},
         "preconditioner_setup_ms": {"jacobi_exact_diag": jacobi_ms, "learned": learned_ms},
         "tuning": {"setting": tune_setting, "matvec_ms_fp32": tune_ms, "matvec_ms_fp32_default": tune_default_ms},
-        "matvec": {"fp32_ms": ms32[4], "fp64_ms": ms64[4], "fp32_gbs": by32[4] / (ms32[4] * 1e-3) / 1e9,
-                   "fp64_gbs": by64[4] / (ms64[4] * 1e-3) / 1e9, "phase_ms_fp32": list(ms32[:4]),
-                   "cell_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9,
+        "matvec": {"fp32_ms": ms32[5], "fp64_ms": ms64[5], "fp32_gbs": by32[5] / (ms32[5] * 1e-3) / 1e9,
+                   "fp64_gbs": by64[5] / (ms64[5] * 1e-3) / 1e9,
+                   "phases": ["nodal", "P init", "prolongation", "cell operator", "restriction wavefronts + gather"],
+                   "phase_ms_fp32": list(ms32[:5]), "phase_ms_fp64": list(ms64[:5]),
+                   "phase_bytes_fp32": list(by32[:5]),
+                   "cell_op_gflops_fp32": flops / (ms32[3] * 1e-3) / 1e9,
                    # nominal FP32 rate: 148 SMs x 128 lanes x 2 flops x 1.965 GHz = 74.4 TFLOP/s
-                   "cell_fp32_frac_of_nominal": flops / (ms32[3] * 1e-3) / 74.4e12},
-        "roofline": {"bound": "hbm", "kernel": "phase B: k_cells (cell operator) + k_level (restriction wavefronts)",
+                   "cell_op_fp32_frac_of_nominal": flops / (ms32[3] * 1e-3) / 74.4e12},
+        "roofline": {"bound": "hbm", "kernel": "cell operator (k_sf; k_cells for sparse slabs), FP32",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": peak_src, "traffic": traffic, "traffic_unit": "bytes per phase B (ncu)"},
+                     "peak_source": peak_src, "traffic": traffic,
+                     "traffic_source": TRAFFIC_SOURCE if traffic else None,
+                     "bytes_per_matvec": by32[3], "ms_per_matvec": ms32[3]},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16 * g.n, "d2h_bytes_per_step": 8 * g.n},
         "setup_seconds": setup_s, "plan_seconds": info["plan_seconds"], "device_bytes": info["device_bytes"],
         "clocks": clk.summary(),
         "gpu_launches": int(sum(r["kernel_launches"] for r in reps)),
     }
+    if same is not None:
+        line["same_instance"] = same
     if batch is not None:
         line["batch"] = batch
     if bdrhs is not None:

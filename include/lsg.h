@@ -108,11 +108,12 @@ int lsg_matvec_device(lsg_operator *op, const void *x, void *y, int32_t precisio
 int lsg_matvec_device_noalloc(lsg_operator *op, const void *x, void *y, int32_t precision, void *stream);
 
 /* Times `iters` matvecs on device buffers with CUDA events between the
- * phases; phase_ms[0..3] = mean ms of (nodal transform, P init, prolongation
- * levels, restriction wavefronts incl. the cell operator), phase_ms[4] = whole
- * matvec.  bytes[0..4] = algorithmic bytes of the same phases for this
- * precision (every vector, slab and table counted once per kernel that must
- * touch it); flops = cell-operator flops per matvec. */
+ * phases; phase_ms[0..4] = mean ms of (nodal transform, P init, prolongation
+ * levels, cell operator, restriction wavefronts with the final gather),
+ * phase_ms[5] = whole matvec (6 entries).  bytes[0..5] = algorithmic bytes of
+ * the same phases for this precision (every vector, slab and table counted
+ * once per kernel that must touch it); flops = floating-point operations of
+ * the cell operator per matvec, as its kernels issue them. */
 int lsg_matvec_profile(lsg_operator *op, const void *x, void *y, int32_t precision, int32_t iters, double *phase_ms,
                        double *bytes, double *flops);
 

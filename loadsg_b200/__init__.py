@@ -422,11 +422,11 @@ class MatrixVectorHomogen:
         return _tuning.autotune(self, precision, reps, cache)
 
     def profile(self, x_ptr, y_ptr, precision=FP32, iters=5):
-        """Mean ms per matvec phase (nodal, P init, prolongation, restriction
-        wavefronts with the cell operator, total) plus algorithmic bytes per
-        phase and cell-operator flops."""
-        ms = np.zeros(5)
-        by = np.zeros(5)
+        """Mean ms per matvec phase (nodal, P init, prolongation, cell operator,
+        restriction wavefronts with the final gather, total) plus algorithmic
+        bytes per phase and cell-operator flops."""
+        ms = np.zeros(6)
+        by = np.zeros(6)
         fl = np.zeros(1)
         _check(lib().lsg_matvec_profile(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), precision, iters,
                                         _ptr(ms), _ptr(by), _ptr(fl)))

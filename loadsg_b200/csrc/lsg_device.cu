@@ -5,8 +5,9 @@
 //                MatrixVectorHomogen.cpp:43-74), sum-factorised 3-tap stages
 //   k_pinit      P_c(T) = nodal(T)            ("P += nodal", MVH.h:1649)
 //   k_prolong    one prolongation level       (MVH.h:1655-1670, 444-474)
-//   k_cells      the level-T cell operator (LocalStiffnessMatrices.cpp:555-582)
-//                for every (case, depth) item, applied in the Walsh-Hadamard
+//   k_sf         the level-T cell operator (LocalStiffnessMatrices.cpp:555-582)
+//                of dense slabs, factorised over reduced modes (lsg_sf_kernel.cuh)
+//   k_cells      the same for sparse slabs, per cell in the Walsh-Hadamard
 //                basis where the Q1 element is diagonal
 //   k_level      one restriction wavefront: per (case, depth) item the gM
 //                bookkeeping + restrictions (MVH.h:1672-1735, 485-530)
@@ -81,6 +82,10 @@ struct DevPlan {
     const lsg::PhaseBItem* b_items;
     const lsg::PhaseBStep* b_steps;
     const int32_t* pts;
+    const int64_t* sp_slot_off;     // per phase-B item of a sparse slab: first cell slot (-1: dense)
+    const int64_t* sp_inc_base;     // per sparse slab: start of its per-entry ranges in sp_inc_off
+    const int64_t* sp_inc_off;      // per sparse-slab entry: range of its (cell, corner) slots in sp_inc
+    const int32_t* sp_inc;          // slot ids (cell * 2^d + corner) in cell order
     const int64_t* conv_off;        // per phase-B item: first convert slot (-1: none)
     const int32_t* conv_items_off;  // per depth: range in conv_items
     const int32_t* conv_items;      // items whose restrictions end at the depth, in item order
@@ -205,238 +210,6 @@ __device__ __forceinline__ void wht_group(V* v, int g) {
     }
 }
 
-// Hadamard butterflies over dims 1..D-1 of one dim-0 face: NH values per lane,
-// local dims 1..DL-1 (bit k-1 of the local index), dims DL..D-1 across lanes.
-template <int D, typename V>
-__device__ __forceinline__ void wht_face(V* v, int g) {
-    constexpr int DL = CellCfg<D, V>::DL, NH = CellCfg<D, V>::NH;
-#pragma unroll
-    for (int k = 0; k < DL - 1; ++k)
-#pragma unroll
-        for (int b = 0; b < NH; ++b)
-            if (!(b & (1 << k))) {
-                V p = v[b], q = v[b | (1 << k)];
-                v[b] = p + q;
-                v[b | (1 << k)] = p - q;
-            }
-#pragma unroll
-    for (int k = DL; k < D; ++k) {
-        int m = 1 << (k - DL);
-        V sgn = (g & m) ? V(-1) : V(1);
-#pragma unroll
-        for (int b = 0; b < NH; ++b) {
-            V p = __shfl_xor_sync(0xffffffffu, v[b], m);
-            v[b] = fma(sgn, v[b], p);
-        }
-    }
-}
-
-// z += sum over the slab's cells of a_c H diag(lam) H u_c on a dense slab.
-// Work unit = a segment of at most 8 consecutive cells of one dim-0 column.
-// The Hadamard transform factorises as H = H_0 (x) H_rest; the H_rest
-// transform of a face is shared by the two cells on either side of it, so per
-// cell only the new (right) face is transformed forward, and the left-face
-// outputs of this cell and the right-face outputs of the previous one are
-// summed before one inverse H_rest.  A segment transforms its first left face
-// itself and scatters its last right face; faces on the boundary drop out.
-// Segments (instead of whole columns) keep all lanes busy when dim 0 is long
-// and the other dims short.  All lanes of a warp run the same number of
-// rounds and iterations (the group shuffles need them).
-// FP32 face transform on packed pairs (Blackwell f32x2 add/FMA): value 2q+e of
-// the face is component e of v[q]; local dim 1 (bit 0) pairs the two
-// components, local dims 2..DL-1 pair whole float2s, dims DL..D-1 go across
-// lanes.  Bitwise the same as wht_face<D, float> (p - q is fma(q, -1, p)).
-template <int D>
-__device__ __forceinline__ void wht_face_f2(float2* v, int g) {
-    constexpr int DL = CellCfg<D, float>::DL, NP = CellCfg<D, float>::NH / 2;
-    const float2 neg1 = make_float2(-1.f, -1.f);
-#pragma unroll
-    for (int q = 0; q < NP; ++q) {
-        float a = v[q].x, b = v[q].y;
-        v[q] = make_float2(a + b, a - b);
-    }
-#pragma unroll
-    for (int k = 1; k < DL - 1; ++k)
-#pragma unroll
-        for (int q = 0; q < NP; ++q)
-            if (!(q & (1 << (k - 1)))) {
-                float2 p = v[q], w = v[q | (1 << (k - 1))];
-                v[q] = __fadd2_rn(p, w);
-                v[q | (1 << (k - 1))] = __ffma2_rn(w, neg1, p);
-            }
-#pragma unroll
-    for (int k = DL; k < D; ++k) {
-        int m = 1 << (k - DL);
-        float sg = (g & m) ? -1.f : 1.f;
-        float2 sgn = make_float2(sg, sg);
-#pragma unroll
-        for (int q = 0; q < NP; ++q) {
-            float2 p;
-            p.x = __shfl_xor_sync(0xffffffffu, v[q].x, m);
-            p.y = __shfl_xor_sync(0xffffffffu, v[q].y, m);
-            v[q] = __ffma2_rn(sgn, v[q], p);
-        }
-    }
-}
-
-// z += sum over the slab's cells of a_c H diag(lam) H u_c on a dense slab.
-// Work unit = a segment of `seg` consecutive cells of one dim-0 column (seg and
-// the column length 2^T_0 are powers of two, so every segment is full and the
-// unit decode is shifts and masks).  The Hadamard transform factorises as
-// H = H_0 (x) H_rest; the H_rest transform of a face is shared by the two cells
-// on either side of it, so per cell only the new (right) face is transformed
-// forward, and the left-face outputs of this cell and the right-face outputs
-// of the previous one are summed before one inverse H_rest.  A segment
-// transforms its first left face itself and scatters its last right face;
-// faces on the boundary drop out.  Segments (instead of whole columns) keep
-// all lanes busy when dim 0 is long and the other dims short.  All lanes of a
-// warp run the same number of rounds and iterations (the group shuffles need
-// them); a lane group without a unit works on zeros.
-template <int D, typename V>
-__device__ void cells_dense(const DevSlab& s, const V* __restrict__ u, V* z, const V* __restrict__ ac, const V* lamg,
-                            int32_t segmax) {
-    constexpr int DL = CellCfg<D, V>::DL, G = CellCfg<D, V>::G, NH = CellCfg<D, V>::NH;
-    constexpr bool PACK = std::is_same<V, float>::value && NH >= 4;
-    const int g = threadIdx.x & (G - 1);
-    const int64_t group = threadIdx.x / G, ngroups = blockDim.x / G;
-    const int lc0 = s.T[0];
-    const int32_t c0 = 1 << lc0;  // cells along dim 0
-    const int lseg = min(lc0, 31 - __clz(segmax));
-    const int32_t seg = 1 << lseg;
-    const int64_t units = s.ncell >> lseg;
-    const int64_t rounds = (units + ngroups - 1) / ngroups;
-    V lp[NH], lm[NH];  // eigenvalues for s_0 = + (bit 0 clear) and s_0 = - (bit 0 set)
-#pragma unroll
-    for (int j = 0; j < NH; ++j) { lp[j] = lamg[2 * j]; lm[j] = lamg[2 * j + 1]; }
-    for (int64_t r = 0; r < rounds; ++r) {
-        int64_t unit = r * ngroups + group;
-        bool live = unit < units;
-        int64_t cell0 = live ? unit << lseg : 0;  // linear index of the segment's first cell
-        int32_t m0s = (int32_t)(cell0 & (c0 - 1));
-        int64_t col = cell0 >> lc0;
-        int32_t m[D];
-        int sh = 0;
-#pragma unroll
-        for (int k = 1; k < D; ++k) {
-            m[k] = (int32_t)((col >> sh) & ((1 << s.T[k]) - 1));
-            sh += s.T[k];
-        }
-        int32_t off[NH];
-        bool ok[NH];
-#pragma unroll
-        for (int j = 0; j < NH; ++j) {
-            int32_t o = 0;
-            bool good = live;
-#pragma unroll
-            for (int k = 1; k < D; ++k) {
-                int bit = k < DL ? (j >> (k - 1)) & 1 : (g >> (k - DL)) & 1;
-                int32_t c = m[k] + bit;
-                good = good && c >= 1 && c <= s.ext[k];
-                o += (c - 1) * s.stride[k];
-            }
-            off[j] = o + m0s;  // slab position of face corner j at dim-0 coordinate m0s + 1
-            ok[j] = good;
-        }
-        const V* acol = ac + cell0;
-        if constexpr (PACK) {
-            constexpr int NP = NH / 2;
-            float2 lp2[NP], lm2[NP];
-#pragma unroll
-            for (int q = 0; q < NP; ++q) {
-                lp2[q] = make_float2((float)lp[2 * q], (float)lp[2 * q + 1]);
-                lm2[q] = make_float2((float)lm[2 * q], (float)lm[2 * q + 1]);
-            }
-            float2 lh[NP], cr[NP];
-#pragma unroll
-            for (int q = 0; q < NP; ++q) {
-                lh[q].x = (ok[2 * q] && m0s >= 1) ? u[off[2 * q] - 1] : 0.f;
-                lh[q].y = (ok[2 * q + 1] && m0s >= 1) ? u[off[2 * q + 1] - 1] : 0.f;
-                cr[q] = make_float2(0.f, 0.f);
-            }
-            wht_face_f2<D>(lh, g);
-            const float2 neg1 = make_float2(-1.f, -1.f);
-#pragma unroll 2
-            for (int32_t i = 0; i < seg; ++i) {
-                const int32_t m0 = m0s + i;
-                const bool rin = m0 + 1 < c0;
-                float2 rh[NP];
-#pragma unroll
-                for (int q = 0; q < NP; ++q) {
-                    rh[q].x = (ok[2 * q] && rin) ? u[off[2 * q] + i] : 0.f;
-                    rh[q].y = (ok[2 * q + 1] && rin) ? u[off[2 * q + 1] + i] : 0.f;
-                }
-                wht_face_f2<D>(rh, g);
-                float a = live ? (float)acol[i] : 0.f;
-                float2 a2 = make_float2(a, a);
-                float2 outl[NP];
-#pragma unroll
-                for (int q = 0; q < NP; ++q) {
-                    float2 sp = __fmul2_rn(__fadd2_rn(lh[q], rh[q]), __fmul2_rn(a2, lp2[q]));
-                    float2 sm = __fmul2_rn(__ffma2_rn(rh[q], neg1, lh[q]), __fmul2_rn(a2, lm2[q]));
-                    outl[q] = __fadd2_rn(__fadd2_rn(sp, sm), cr[q]);
-                    lh[q] = rh[q];
-                    cr[q] = __ffma2_rn(sm, neg1, sp);
-                }
-                wht_face_f2<D>(outl, g);
-                if (m0 >= 1) {
-#pragma unroll
-                    for (int q = 0; q < NP; ++q) {
-                        if (ok[2 * q]) atomicAdd((float*)&z[off[2 * q] + i - 1], outl[q].x);
-                        if (ok[2 * q + 1]) atomicAdd((float*)&z[off[2 * q + 1] + i - 1], outl[q].y);
-                    }
-                }
-            }
-            // right face of the segment's last cell, unless it lies on the boundary
-            wht_face_f2<D>(cr, g);
-            if (m0s + seg < c0) {
-#pragma unroll
-                for (int q = 0; q < NP; ++q) {
-                    if (ok[2 * q]) atomicAdd((float*)&z[off[2 * q] + seg - 1], cr[q].x);
-                    if (ok[2 * q + 1]) atomicAdd((float*)&z[off[2 * q + 1] + seg - 1], cr[q].y);
-                }
-            }
-        } else {
-            V lh[NH], cr[NH];  // transformed left face, carried right-face output
-#pragma unroll
-            for (int j = 0; j < NH; ++j) {
-                lh[j] = (ok[j] && m0s >= 1) ? u[off[j] - 1] : V(0);
-                cr[j] = V(0);
-            }
-            wht_face<D, V>(lh, g);
-            for (int32_t i = 0; i < seg; ++i) {
-                const int32_t m0 = m0s + i;
-                const bool rin = m0 + 1 < c0;
-                V rh[NH];
-#pragma unroll
-                for (int j = 0; j < NH; ++j) rh[j] = (ok[j] && rin) ? u[off[j] + i] : V(0);
-                wht_face<D, V>(rh, g);
-                V a = live ? acol[i] : V(0);
-                V outl[NH];
-#pragma unroll
-                for (int j = 0; j < NH; ++j) {
-                    V sp = (lh[j] + rh[j]) * (a * lp[j]);
-                    V sm = (lh[j] - rh[j]) * (a * lm[j]);
-                    outl[j] = sp + sm + cr[j];
-                    lh[j] = rh[j];
-                    cr[j] = sp - sm;
-                }
-                wht_face<D, V>(outl, g);
-                if (m0 >= 1) {
-#pragma unroll
-                    for (int j = 0; j < NH; ++j)
-                        if (ok[j]) atomicAdd(&z[off[j] + i - 1], outl[j]);
-                }
-            }
-            wht_face<D, V>(cr, g);
-            if (m0s + seg < c0) {
-#pragma unroll
-                for (int j = 0; j < NH; ++j)
-                    if (ok[j]) atomicAdd(&z[off[j] + seg - 1], cr[j]);
-            }
-        }
-    }
-}
-
 // FP32 full-cell transform on packed pairs: value 2q+e of the lane's NL
 // corners is component e of v[q]; bit 0 inside pairs, bits 1..DL-1 across
 // pairs, dims DL..D-1 across lanes.  Bitwise the same as wht_group<D, float>.
@@ -473,8 +246,12 @@ __device__ __forceinline__ void wht_group_f2(float2* v, int g) {
     }
 }
 
+// Cell operator of a sparse slab (the cells whose interior corners all exist,
+// cells/CellStructure.h:23-61): every cell's 2^d outputs go to its own slots
+// (cell * 2^d + corner), and each slab entry then sums the slots of its cells
+// in a fixed order (cell, then corner) -- no atomics.
 template <int D, typename V>
-__device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __restrict__ u, V* z,
+__device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __restrict__ u, V* __restrict__ slots,
                              const V* __restrict__ ac, const V* lamg) {
     constexpr int DL = CellCfg<D, V>::DL, G = CellCfg<D, V>::G, NL = CellCfg<D, V>::NL;
     constexpr bool PACK = std::is_same<V, float>::value && NL >= 4;
@@ -485,6 +262,7 @@ __device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __rest
         int64_t ci = r * ngroups + group;
         bool live = ci < s.ncell;
         const int32_t* cp = P.cell_corner + ((s.corner_off + (live ? ci : 0)) << D) + (g << DL);
+        V* out = slots + ((live ? ci : 0) << D) + (g << DL);
         int32_t pos[NL];
 #pragma unroll
         for (int b = 0; b < NL; ++b) pos[b] = live ? cp[b] : -1;
@@ -503,11 +281,12 @@ __device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __rest
             for (int q = 0; q < NP; ++q)
                 v[q] = __fmul2_rn(v[q], __fmul2_rn(a2, make_float2((float)lamg[2 * q], (float)lamg[2 * q + 1])));
             wht_group_f2<D>(v, g);
+            if (live)
 #pragma unroll
-            for (int q = 0; q < NP; ++q) {
-                if (pos[2 * q] >= 0) atomicAdd((float*)&z[pos[2 * q]], v[q].x);
-                if (pos[2 * q + 1] >= 0) atomicAdd((float*)&z[pos[2 * q + 1]], v[q].y);
-            }
+                for (int q = 0; q < NP; ++q) {
+                    out[2 * q] = (V)v[q].x;
+                    out[2 * q + 1] = (V)v[q].y;
+                }
         } else {
             V v[NL];
 #pragma unroll
@@ -516,49 +295,45 @@ __device__ void cells_sparse(const DevPlan& P, const DevSlab& s, const V* __rest
 #pragma unroll
             for (int b = 0; b < NL; ++b) v[b] *= a * lamg[b];
             wht_group<D, V>(v, g);
+            if (live)
 #pragma unroll
-            for (int b = 0; b < NL; ++b)
-                if (pos[b] >= 0) atomicAdd(&z[pos[b]], v[b]);
+                for (int b = 0; b < NL; ++b) out[b] = v[b];
         }
     }
 }
 
-// ----------------------------------------------------------------------------- phase B, cell operator
-// z_c(T) = A_T P_c(T) for every (case, depth) item in one launch (per size
-// class): the cell operator does not depend on the gM chain, so it needs no
-// wavefront ordering.  u and z live in shared memory when 2 N_T fits.
+// ----------------------------------------------------------------------------- phase B, cell operator (sparse slabs)
+// z_c(T) = A_T P_c(T) for the (case, depth) items of sparse slabs, one CTA per
+// item (dense slabs go to k_sf); u lives in shared memory when N_T fits.
 template <int D, typename V>
-__global__ void __launch_bounds__(256, std::is_same<V, float>::value ? 3 : 2) k_cells(DevPlan P, const V* __restrict__ pc, V* __restrict__ zb,
-                                                  const V* __restrict__ acell, const V* __restrict__ lam_all,
-                                                  const int32_t* __restrict__ order, int32_t ord0, int64_t cap,
-                                                  int32_t segmax) {
+__global__ void __launch_bounds__(256) k_cells(DevPlan P, const V* __restrict__ pc, V* __restrict__ zb,
+                                              const V* __restrict__ acell, const V* __restrict__ lam_all,
+                                              const int32_t* __restrict__ order, int32_t ord0, int64_t cap,
+                                              V* __restrict__ slot_buf) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NC = 1 << D;
-    const lsg::PhaseBItem it = P.b_items[order[ord0 + blockIdx.x]];
+    const int32_t ii = order[ord0 + blockIdx.x];
+    const lsg::PhaseBItem it = P.b_items[ii];
     const DevSlab& s = P.slabs[it.t];
     V* lam = reinterpret_cast<V*>(smem_raw);
     for (int b = threadIdx.x; b < NC; b += blockDim.x) lam[b] = lam_all[(int64_t)it.t * NC + b];
     const V* lamg = lam + ((threadIdx.x & (CellCfg<D, V>::G - 1)) << CellCfg<D, V>::DL);
-    const V* u_g = pc + it.p_off;
-    V* z_g = zb + it.p_off;
-    const V* ac = acell + s.cell_off;
-    if (2 * s.n <= cap) {
-        V* u = lam + NC;
-        V* z = u + s.n;
-        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) {
-            u[e] = u_g[e];
-            z[e] = V(0);
-        }
-        __syncthreads();
-        if (s.dense) cells_dense<D, V>(s, u, z, ac, lamg, segmax);
-        else cells_sparse<D, V>(P, s, u, z, ac, lamg);
-        __syncthreads();
-        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) z_g[e] = z[e];
-    } else {
-        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) z_g[e] = V(0);
-        __syncthreads();
-        if (s.dense) cells_dense<D, V>(s, u_g, z_g, ac, lamg, segmax);
-        else cells_sparse<D, V>(P, s, u_g, z_g, ac, lamg);
+    const V* u = pc + it.p_off;
+    if (s.n <= cap) {
+        V* us = lam + NC;
+        for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) us[e] = u[e];
+        u = us;
+    }
+    __syncthreads();
+    V* slots = slot_buf + P.sp_slot_off[ii];
+    cells_sparse<D, V>(P, s, u, slots, acell + s.cell_off, lamg);
+    __syncthreads();
+    const int64_t* inc_off = P.sp_inc_off + P.sp_inc_base[it.t];
+    V* z = zb + it.p_off;
+    for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) {
+        V acc = V(0);
+        for (int64_t j = inc_off[e]; j < inc_off[e + 1]; ++j) acc += slots[P.sp_inc[j]];
+        z[e] = acc;
     }
 }
 
@@ -1011,8 +786,9 @@ struct lsg_operator {
     // tables
     DBuf slabs, did, act, exa_off, exa, cell_key, cell_corner, nodal_stage, nodal_src, nodal_code, nodal_dom, nodal_scr,
         conv_stage, conv_src, conv_code, conv_dom, prol, restr, a_items, b_items, b_steps, pts, cell_slab_off,
-        conv_off, conv_items_off, conv_items;
+        conv_off, conv_items_off, conv_items, sp_slot_off, sp_inc_base, sp_inc_off, sp_inc;
     int64_t conv_total = 0;  // convert slots of one matvec
+    int64_t sp_total = 0;    // cell slots of the sparse-slab items of one matvec
     DBuf lam64, lam32;   // Hadamard-basis eigenvalues of the Q1 stiffness (form 0)
     DBuf mu64, mu32;     // ... of the Q1 mass (form 1)
     DBuf one64, one32;   // unit coefficient per cell (constant-coefficient norms)
@@ -1027,7 +803,7 @@ struct lsg_operator {
     DBuf nbmask;               // same-depth neighbour flags (features)
     // work buffers per precision
     struct Work {
-        DBuf ml, pc, zb, gm, scratch, nscratch, conv;
+        DBuf ml, pc, zb, gm, scratch, nscratch, conv, sp;
     } w64, w32;
     DBuf xbuf64, ybuf64;  // host-call staging
     DBuf diag;            // Jacobi diagonal (FP64)
@@ -1061,13 +837,16 @@ namespace {
 // precision for a work space of tune.cell_space_kb, FP64 with half the
 // elements), ordered by work space, largest first, in classes: a new class
 // (launch) starts when the work space shrinks by tune.class_ratio.  Items of
-// sparse slabs (and of dense slabs whose plan does not fit) go to k_cells by
-// slab size, with shared memory for 2 N_T of the class's largest slab.
+// sparse slabs go to k_cells by slab size, with shared memory for N_T of the
+// class's largest slab.
 int build_sf_prec(lsg_operator* op, lsg_operator::SfPrec& S, int64_t wcap, int na_max) {
     const lsg::Plan& p = op->plan;
     std::vector<lsg::SfSlab> plans = lsg::sf_plan(p, op->sf_layout, wcap, na_max);
     S.ok.assign(p.nD, 0);
-    for (int t = 0; t < p.nD; ++t) S.ok[t] = plans[t].nm >= 0 && plans[t].nq <= 6;
+    for (int t = 0; t < p.nD; ++t) {
+        S.ok[t] = plans[t].nm >= 0;
+        if (p.slabs[t].dense && !S.ok[t]) return fail(LSG_E_INVALID, "no factorised plan fits a dense slab");
+    }
     std::vector<int32_t> ord, cord;
     for (size_t i = 0; i < p.b_items.size(); ++i) (S.ok[p.b_items[i].t] ? ord : cord).push_back((int32_t)i);
     std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) {
@@ -1192,6 +971,43 @@ int upload_plan(lsg_operator* op) {
         rc |= op->conv_items_off.upload(ioff, tot);
         rc |= op->conv_items.upload(items, tot);
     }
+    {  // sparse slabs: per item its cell slots; per entry its (cell, corner) slots in cell order
+        const int nc = 1 << d;
+        std::vector<int64_t> soff(std::max<size_t>(p.b_items.size(), 1), -1), base(p.nD, -1), ioff;
+        std::vector<int32_t> inc;
+        int64_t slots = 0;
+        for (size_t i = 0; i < p.b_items.size(); ++i) {
+            const lsg::Slab& sl = p.slabs[p.b_items[i].t];
+            if (sl.dense) continue;
+            soff[i] = slots;
+            slots += sl.ncell * nc;
+        }
+        for (int t = 0; t < p.nD; ++t) {
+            const lsg::Slab& sl = p.slabs[t];
+            if (sl.dense) continue;
+            base[t] = (int64_t)ioff.size();
+            std::vector<std::vector<int32_t>> per(sl.n);
+            for (int64_t c = 0; c < sl.ncell; ++c)
+                for (int b = 0; b < nc; ++b) {
+                    int32_t at = p.cell_corner[(size_t)(sl.corner_off + c) * nc + b];
+                    if (at >= 0) per[at].push_back((int32_t)(c * nc + b));
+                }
+            int64_t run = (int64_t)inc.size();
+            for (int64_t e = 0; e < sl.n; ++e) {
+                ioff.push_back(run);
+                inc.insert(inc.end(), per[e].begin(), per[e].end());
+                run = (int64_t)inc.size();
+            }
+            ioff.push_back(run);
+        }
+        if (ioff.empty()) ioff.push_back(0);
+        if (inc.empty()) inc.push_back(0);
+        op->sp_total = slots;
+        rc |= op->sp_slot_off.upload(soff, tot);
+        rc |= op->sp_inc_base.upload(base, tot);
+        rc |= op->sp_inc_off.upload(ioff, tot);
+        rc |= op->sp_inc.upload(inc, tot);
+    }
     if (rc) return LSG_E_CUDA;
     // Hadamard-basis eigenvalues of the Q1 element per depth, 1/2^d folded in
     int nc = 1 << d;
@@ -1248,6 +1064,10 @@ int upload_plan(lsg_operator* op) {
     P.b_items = op->b_items.as<lsg::PhaseBItem>();
     P.b_steps = op->b_steps.as<lsg::PhaseBStep>();
     P.pts = op->pts.as<int32_t>();
+    P.sp_slot_off = op->sp_slot_off.as<int64_t>();
+    P.sp_inc_base = op->sp_inc_base.as<int64_t>();
+    P.sp_inc_off = op->sp_inc_off.as<int64_t>();
+    P.sp_inc = op->sp_inc.as<int32_t>();
     P.conv_off = op->conv_off.as<int64_t>();
     P.conv_items_off = op->conv_items_off.as<int32_t>();
     P.conv_items = op->conv_items.as<int32_t>();
@@ -1318,6 +1138,7 @@ int ensure_work(lsg_operator* op, lsg_operator::Work& w) {
     rc |= w.scratch.alloc(std::max<int64_t>(p.scratch_total, 1) * sizeof(V), tot);
     rc |= w.nscratch.alloc(std::max<int64_t>(p.nodal_scratch, 1) * sizeof(V), tot);
     rc |= w.conv.alloc(std::max<int64_t>(op->conv_total, 1) * sizeof(V), tot);
+    rc |= w.sp.alloc(std::max<int64_t>(op->sp_total, 1) * sizeof(V), tot);
     return rc ? LSG_E_CUDA : 0;
 }
 
@@ -1341,10 +1162,11 @@ int set_phaseB_smem() {
     return 0;
 }
 
-// Phase B: k_cells per size class, then one k_level per restriction wavefront.
+// Phase B: the cell operator (k_sf per work-space class, k_cells per sparse
+// size class), then one k_level per restriction wavefront and the gather into y.
 template <int D, typename V>
-int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* conv, V* y, const V* acell,
-                  const V* lam, cudaStream_t st) {
+int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* conv, V* sp, V* y, const V* acell,
+                  const V* lam, cudaStream_t st, cudaEvent_t ev_cells = nullptr) {
     const lsg::Plan& p = op->plan;
     constexpr bool F32 = std::is_same<V, float>::value;
     const lsg_operator::SfPrec& S = F32 ? op->sf32 : op->sf64;
@@ -1364,12 +1186,13 @@ int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* co
     const int64_t cap_elems = (200 * 1024) / sizeof(V) - (1 << D);
     for (size_t c = 0; c + 1 < S.cell_class_off.size(); ++c) {
         int32_t b = S.cell_class_off[c], e = S.cell_class_off[c + 1];
-        int64_t need = 2 * S.cell_class_n[c];
+        int64_t need = S.cell_class_n[c];
         int64_t alloc = need <= cap_elems ? need : 0;
         size_t smem = (size_t)((1 << D) + alloc) * sizeof(V);
         k_cells<D, V><<<e - b, op->tune.cell_threads, smem, st>>>(op->dp, pc, zb, acell, lam,
-                                                                  S.cell_order.as<int32_t>(), b, alloc, 8);
+                                                                  S.cell_order.as<int32_t>(), b, alloc, sp);
     }
+    if (ev_cells) cudaEventRecord(ev_cells, st);
     // elements per ping-pong buffer (two buffers within the 220 KB opt-in)
     const int64_t lvl_cap = std::min<int64_t>(op->tune.level_cap, (110 * 1024) / sizeof(V));
     for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
@@ -1408,10 +1231,10 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t
         if (e > b) k_prolong<V><<<e - b, op->tune.prolong_threads, 0, st>>>(op->dp, w.pc.as<V>(), b);
     }
     if (ev) cudaEventRecord(ev[3], st);
-    rc = phaseB_launch<D, V>(op, w.pc.as<V>(), w.zb.as<V>(), w.gm.as<V>(), w.scratch.as<V>(), w.conv.as<V>(), y, acell,
-                             lam, st);
+    rc = phaseB_launch<D, V>(op, w.pc.as<V>(), w.zb.as<V>(), w.gm.as<V>(), w.scratch.as<V>(), w.conv.as<V>(),
+                             w.sp.as<V>(), y, acell, lam, st, ev ? ev[4] : nullptr);
     if (rc) return rc;
-    if (ev) cudaEventRecord(ev[4], st);
+    if (ev) cudaEventRecord(ev[5], st);
     CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -1685,65 +1508,105 @@ static int64_t matvec_launches(const lsg::Plan& p) {
     return 3 + (int64_t)(p.a_level_off.size() - 1) + (int64_t)(p.b_level_off.size() - 1);
 }
 
-static void phase_bytes(const lsg::Plan& p, double sv, double* b) {
+static void phase_bytes(const lsg_operator* op, double sv, double* b) {
+    const lsg::Plan& p = op->plan;
     int d = p.d;
     double nodal = sv * (double)p.exa_off[p.nD] + sv * (double)p.M;  // x gathered, nodal slabs written
     for (size_t i = 0; i < p.nodal.code.size(); ++i) nodal += 4.0 * (1 + p.nodal.nsrc);  // stage tables
-    double pinit = 0, prol = 0, phb = 0;
+    double pinit = 0, prol = 0, cell = 0, wave = 0;
     for (const auto& it : p.b_items) pinit += 2.0 * sv * p.slabs[it.t].n;
     for (const auto& a : p.a_items) prol += a.n_dst * (3.0 * sv + 8.0) + sv * p.slabs[a.t_src].n;
+    const lsg::SfCoefLayout& L = op->sf_layout;
     for (const auto& it : p.b_items) {
         const lsg::Slab& s = p.slabs[it.t];
-        phb += sv * s.n * (it.gm_prev ? 3.0 : 2.0);            // P read, z written (+ gM read)
-        phb += sv * s.ncell;                                    // cell coefficient
-        if (!s.dense) phb += 4.0 * (1 << d) * s.ncell;          // corner table
+        // cell operator: slab read, slab written, coefficients (collapsed for k_sf)
+        cell += 2.0 * sv * s.n;
+        if (s.dense && L.coef_off[it.t] >= 0) {
+            double c = 1;
+            for (int k = 0; k < d; ++k)
+                if (s.T[k] >= 2) c *= (double)((int64_t)1 << s.T[k]);
+            cell += sv * c;
+        } else {
+            cell += sv * s.ncell + 4.0 * (1 << d) * s.ncell;  // per-cell coefficient, corner table
+        }
+        // wavefronts: z (+ gM) read, restriction tables and vectors, convert stages and slots
+        wave += sv * s.n * (it.gm_prev ? 2.0 : 1.0);
         for (int32_t k = it.step_begin; k < it.step_end; ++k) {
             const lsg::PhaseBStep& st = p.b_steps[k];
-            phb += st.n_dst * (12.0 + sv * (st.gm_prev ? 3.0 : 2.0)) + sv * st.n_src;
+            wave += st.n_dst * (12.0 + sv * (st.gm_prev ? 3.0 : 2.0)) + sv * st.n_src;
         }
         if (it.t_conv >= 0) {
             const int64_t* dom = &p.convert_dom[it.t_conv * (d + 1)];
-            for (int j = 1; j <= d; ++j) phb += dom[j] * (24.0 + sv);
-            phb += sv * dom[d];                                 // y update
+            for (int j = 1; j <= d; ++j) wave += dom[j] * (24.0 + sv);
+            wave += 2.0 * sv * dom[d];                          // slots written, gathered
         }
     }
+    wave += sv * (double)p.exa_off[p.nD];                      // y
     b[0] = nodal;
     b[1] = pinit;
     b[2] = prol;
-    b[3] = phb;
-    b[4] = nodal + pinit + prol + phb;
+    b[3] = cell;
+    b[4] = wave;
+    b[5] = nodal + pinit + prol + cell + wave;
+}
+
+// Floating-point operations of the cell operator as the kernels issue them:
+// k_sf per chunk (gather, mid sweeps, the fused a-b step per pencil plane,
+// transposed sweeps, scatter), k_cells per cell (two Hadamard transforms and
+// the scaling of 2^d corner values).
+static double cell_op_flops(const lsg_operator* op, bool f32) {
+    const lsg::Plan& p = op->plan;
+    const lsg_operator::SfPrec& S = f32 ? op->sf32 : op->sf64;
+    const std::vector<lsg::SfSlab> plans = lsg::sf_plan(p, op->sf_layout, (int64_t)op->tune.cell_space_kb * 1024 / (f32 ? 4 : 8),
+                                                        f32 ? 7 : 3);
+    double fl = 0.0;
+    for (const auto& it : p.b_items) {
+        if (S.ok[it.t]) {
+            const lsg::SfSlab& D = plans[it.t];
+            double ncomb = 1;
+            for (int i = 0; i < D.nq; ++i) ncomb *= 2;
+            double per = 2.0 * D.slice * ncomb;  // gather + scatter
+            for (int k = 0; k < D.nm; ++k) per += D.stage[k + 1] + 1.5 * D.stage[k + 1];  // sweeps, both ways
+            const double na = D.a.n, nb = D.b.n, ma = D.a.T < 0 ? 1 : 2 * na;
+            double row = 2 * (na - 1) + 3 * na;           // E_a and E_a^T of one row
+            double plane = nb * row + (nb - 1) * 9 * ma + 2 * 3 * ma;  // interior and boundary b cells
+            per += D.npl * plane;
+            fl += per * D.nchunk;
+        } else {
+            const int d = p.d, nc = 1 << d;
+            fl += (double)p.slabs[it.t].ncell * ((2.0 * d + 1.0) * nc);
+        }
+    }
+    return fl;
 }
 
 int lsg_matvec_profile(lsg_operator* op, const void* x, void* y, int32_t precision, int32_t iters, double* phase_ms,
                        double* bytes, double* flops) {
     if (!op || !x || !y || !phase_ms || iters < 1) return fail(LSG_E_INVALID, "bad argument");
     if (!op->have_coef) return fail(LSG_E_STATE, "no coefficient set");
-    cudaEvent_t ev[5];
+    cudaEvent_t ev[6];
     for (auto& e : ev) cudaEventCreate(&e);
-    double acc[5] = {0, 0, 0, 0, 0};
+    double acc[6] = {0, 0, 0, 0, 0, 0};
     int rc = 0;
     for (int i = 0; i < iters && !rc; ++i) {
         rc = precision == LSG_FP64 ? matvec_dispatch<double>(op, (const double*)x, (double*)y, nullptr, ev)
                                    : matvec_dispatch<float>(op, (const float*)x, (float*)y, nullptr, ev);
         if (rc) break;
-        cudaEventSynchronize(ev[4]);
+        cudaEventSynchronize(ev[5]);
         float ms;
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < 5; ++k) {
             cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
             acc[k] += ms;
         }
-        cudaEventElapsedTime(&ms, ev[0], ev[4]);
-        acc[4] += ms;
+        cudaEventElapsedTime(&ms, ev[0], ev[5]);
+        acc[5] += ms;
     }
     for (auto& e : ev) cudaEventDestroy(e);
     if (rc) return rc;
-    for (int k = 0; k < 5; ++k) phase_ms[k] = acc[k] / iters;
-    if (bytes) phase_bytes(op->plan, precision == LSG_FP64 ? 8.0 : 4.0, bytes);
-    if (flops) {
-        int64_t cc = 0;
-        for (const auto& it : op->plan.b_items) cc += op->plan.slabs[it.t].ncell;
-        *flops = (double)cc * ((2.0 * op->plan.d + 1.0) * (1 << op->plan.d));
-    }
+    for (int k = 0; k < 6; ++k) phase_ms[k] = acc[k] / iters;
+    const bool f32 = precision != LSG_FP64;
+    if (bytes) phase_bytes(op, f32 ? 4.0 : 8.0, bytes);
+    if (flops) *flops = cell_op_flops(op, f32);
     return 0;
 }
 
@@ -2543,7 +2406,8 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
     size_t b_sc = align256(std::max<int64_t>(p.scratch_total, 1) * sizeof(V));
     size_t b_ns = align256(std::max<int64_t>(p.nodal_scratch, 1) * sizeof(V));
     size_t b_cv = align256(std::max<int64_t>(op->conv_total, 1) * sizeof(V));
-    size_t need = b_ml + b_pc + b_zb + b_gm + b_sc + b_ns + b_cv;
+    size_t b_sp = align256(std::max<int64_t>(op->sp_total, 1) * sizeof(V));
+    size_t need = b_ml + b_pc + b_zb + b_gm + b_sc + b_ns + b_cv + b_sp;
     if (need > LSG_NOALLOC_SCRATCH_BYTES)
         return fail(LSG_E_INVALID, "lsg_matvec_device_noalloc: this grid needs " + std::to_string(need) +
                                        " bytes of work space, the fixed array holds " +
@@ -2556,6 +2420,7 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
     V* scratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm);
     V* nscratch = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm + b_sc);
     V* conv = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm + b_sc + b_ns);
+    V* sp = reinterpret_cast<V*>(base + b_ml + b_pc + b_zb + b_gm + b_sc + b_ns + b_cv);
     int rc = set_phaseB_smem<D>();
     if (rc) return rc;
     const V* acell = cell_coef<V>(op);
@@ -2563,8 +2428,8 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
                                                   : (const V*)(op->form ? op->mu32.p : op->lam32.p);
     // Every region is written before it is read within one call (nodal slabs by
     // k_nodal, P by k_pinit, gM only where an earlier item of the same call
-    // wrote it, item scratch and convert slots by their own item), so nothing
-    // needs clearing; every active entry of y is written by the final gather.
+    // wrote it, item scratch, convert and cell slots by their own item), so
+    // nothing needs clearing; every active entry of y is written by the final gather.
     k_nodal<V><<<p.nD, 256, 0, st>>>(op->dp, x, ml, nscratch);
     int32_t nb = (int32_t)p.b_items.size();
     if (nb > 0) k_pinit<V><<<nb, 256, 0, st>>>(op->dp, ml, pc, 0);
@@ -2572,7 +2437,7 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
         int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
         if (e > b) k_prolong<V><<<e - b, op->tune.prolong_threads, 0, st>>>(op->dp, pc, b);
     }
-    rc = phaseB_launch<D, V>(op, pc, zb, gm, scratch, conv, y, acell, lam, st);
+    rc = phaseB_launch<D, V>(op, pc, zb, gm, scratch, conv, sp, y, acell, lam, st);
     if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
     return 0;

@@ -111,8 +111,8 @@ std::vector<SfSlab> sf_plan(const Plan& p, const SfCoefLayout& L, int64_t wcap, 
             int64_t sl = na * nb, npl = 1;
             for (size_t i = pos; i < rest.size(); ++i) { sl *= rest[i].n; npl *= 2 * rest[i].n; }
             int64_t top = sl << m;
-            int64_t w = m ? top + top / 2 : sl;
-            if (w > wcap || nch > (1 << 24)) continue;
+            int64_t w = m == 0 ? sl : top + top / 2;
+            if (w > wcap || nch > (1 << 28)) continue;
             const double T = 256.0;
             double per = 2.0 * m + 4.0;                                          // stages (syncs)
             per += std::ceil(npl / T) * (double)nb * (double)na * 0.1;          // fused step, rows in series
@@ -155,7 +155,7 @@ std::vector<SfSlab> sf_plan(const Plan& p, const SfCoefLayout& L, int64_t wcap, 
             I *= 2 * D.mid[k].n;
         }
         D.hi_off = D.stage[D.nm];
-        D.wtotal = D.nm > 0 ? D.stage[D.nm] + D.stage[D.nm - 1] : D.stage[0];
+        D.wtotal = D.nm == 0 ? D.stage[0] : D.stage[D.nm] + D.stage[D.nm - 1];
     }
     return out;
 }

@@ -81,7 +81,7 @@ struct SfSlab {
     int32_t stage[kMaxDim + 1] = {};  // stage sizes (elements): stage k has mid dims < k transformed
     SfDiv inner[kMaxDim];     // division by the inner size I_k of mid sweep k
     int32_t hi_off = 0;       // offset of the second ping-pong region (= stage[nm])
-    int32_t wtotal = 0;       // work-space elements (stage[nm] + stage[nm-1], or stage[0])
+    int32_t wtotal = 0;       // work-space elements: stage[0] (nm = 0), else stage[nm] + stage[nm-1]
     int32_t na_max = 0;       // largest a extent this plan was made for
     int32_t pad = 0;
 };

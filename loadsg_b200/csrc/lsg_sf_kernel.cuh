@@ -1,7 +1,7 @@
 // k_sf: the factorised level-T cell operator of a dense slab (see lsg_sf.h for
 // the mathematics and the host emulation in lsg_sf.cpp that the CPU tests
 // check against the cell-by-cell form).  One CTA per (case, slab) item:
-//   chunk loop (reduced modes of the outermost dimensions, one tuple at a time)
+//   chunk loop (reduced modes of the chunked dimensions, one tuple at a time)
 //     gather   W0 = signed sum of <= 2^nq strided blocks of u
 //     sweeps   W(k+1) = E_k W(k) for the mid dimensions (shared memory, ping-pong)
 //     fused    per pencil plane: E_a and E_b, a~ * Lambda, E_b^T and E_a^T in
@@ -15,7 +15,7 @@
 
 namespace lsg_sfk {
 
-constexpr int kMaxComb = 64;  // 2^nq signed blocks of one chunk (nq <= 6)
+constexpr int kMaxComb = 256;  // 2^nq signed blocks of one chunk (nq <= 8)
 
 template <typename V>
 __device__ __forceinline__ V pow2(int e);
@@ -50,83 +50,73 @@ __device__ __forceinline__ void mode_of(int n, int r, int& cell, int& type) {
     type = (r == 0 || r == 2 * n - 1) ? 2 : ((r & 1) ? 0 : 1);
 }
 
-// reduced modes of the register dimension a: BL, P_i, M_i (i < NA-1), BR
-template <typename V, int NA>
-struct Modes {
+// Pairs of values (the P and M mode of one a cell): packed f32x2 arithmetic in
+// FP32 (Blackwell FADD2/FMUL2/FFMA2), two scalar operations in FP64.
+template <typename V>
+struct PairT;
+template <>
+struct PairT<float> { using T = float2; };
+template <>
+struct PairT<double> { using T = double2; };
+
+__device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ double2 padd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 psub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 pmul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+
+// Reduced modes of the register dimension a with NX nodes: BL, the (P_i, M_i)
+// pairs of the interior cells i = 1 .. NX-1, BR.
+template <typename V, int NX>
+struct ModesX {
+    using V2 = typename PairT<V>::T;
     V bl, br;
-    V p[NA - 1], m[NA - 1];
+    V2 pm[NX - 1];
 };
 
-template <typename V, int NA>
-__device__ __forceinline__ void fwd_a(const V* X, int na, bool virt, Modes<V, NA>& F) {
+template <typename V, int NX>
+__device__ __forceinline__ void fwd_x(const V* X, ModesX<V, NX>& F) {
     F.bl = X[0];
-    F.br = V(0);
+    F.br = X[NX - 1];
 #pragma unroll
-    for (int i = 0; i < NA - 1; ++i) {
-        bool ok = !virt && i < na - 1;
-        F.p[i] = ok ? X[i] + X[i + 1] : V(0);
-        F.m[i] = ok ? X[i] - X[i + 1] : V(0);
+    for (int i = 0; i < NX - 1; ++i) F.pm[i] = mk2(X[i] + X[i + 1], X[i] - X[i + 1]);
+}
+
+template <typename V, int NX>
+__device__ __forceinline__ void bwd_x(const ModesX<V, NX>& G, V* Y) {
+    V l = G.bl;
+#pragma unroll
+    for (int j = 0; j < NX - 1; ++j) {
+        Y[j] = l + (G.pm[j].x + G.pm[j].y);
+        l = G.pm[j].x - G.pm[j].y;
     }
-#pragma unroll
-    for (int i = 0; i < NA; ++i)
-        if (!virt && i == na - 1) F.br = X[i];
+    Y[NX - 1] = l + G.br;
 }
 
-template <typename V, int NA>
-__device__ __forceinline__ void bwd_a(const Modes<V, NA>& G, int na, bool virt, V* Y) {
-    if (virt) { Y[0] = G.bl; return; }
-#pragma unroll
-    for (int j = 0; j < NA; ++j) {
-        V l = j == 0 ? G.bl : G.p[j > 0 ? j - 1 : 0] - G.m[j > 0 ? j - 1 : 0];
-        V r = j < NA - 1 ? G.p[j < NA - 1 ? j : 0] + G.m[j < NA - 1 ? j : 0] : V(0);
-        if (j == na - 1) r = G.br;
-        Y[j] = l + r;
-    }
-}
-
-// G = coefficient(cell of each a mode) * Lambda(a type, b type) * F
-template <typename V, int NA>
-__device__ __forceinline__ void scale_a(const Modes<V, NA>& F, const V* c, int na, V lP, V lM, V lB,
-                                        Modes<V, NA>& G) {
-    G.bl = c[0] * lB * F.bl;
-#pragma unroll
-    for (int i = 0; i < NA - 1; ++i) {
-        G.p[i] = c[i + 1] * lP * F.p[i];
-        G.m[i] = c[i + 1] * lM * F.m[i];
-    }
-    V cbr = c[0];
-#pragma unroll
-    for (int i = 1; i <= NA; ++i)
-        if (i == na) cbr = c[i];
-    G.br = cbr * lB * F.br;
-}
-
-template <typename V, int NA>
-__device__ __forceinline__ void add_modes(Modes<V, NA>& A, const Modes<V, NA>& B, V s) {
-    A.bl += s * B.bl;
-    A.br += s * B.br;
-#pragma unroll
-    for (int i = 0; i < NA - 1; ++i) { A.p[i] += s * B.p[i]; A.m[i] += s * B.m[i]; }
-}
-
-// The fused (a, b) step of one pencil plane P (a fastest, rows of na values,
-// nb rows), in place.  (S, M): pair of every other dimension; cf: coefficient
-// of the plane's cell in the other dimensions (a and b cell 0).
-template <typename V, int NA>
+// The fused (a, b) step of one pencil plane P (a fastest, rows of NX values,
+// nb rows), in place, for an a dimension of exactly NX nodes (NX = 1: no a
+// dimension).  (S, M): pair of every other dimension; cf: coefficient of the
+// plane's cell in the other dimensions (a and b cell 0).
+template <typename V, int NX>
 __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M, const V* cf, bool unit, V unit_v,
                                             int form) {
-    const int na = D.a.n, nb = D.b.n;
-    const bool avirt = D.a.T < 0, bvirt = D.b.T < 0;
-    const int csa = D.a.cstride, csb = D.b.cstride;
-    // a factors by a type, folded with (S, M)
+    using V2 = typename PairT<V>::T;
+    const int nb = D.b.n;
+    const bool bvirt = D.b.T < 0;
+    const int64_t csa = D.a.cstride, csb = D.b.cstride;
+    // a factors by a type (P, M, B), folded with (S, M); no a dimension: identity
     V SAt[3], MAt[3];
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
         V kap, mu;
-        fac<V>(D.a.T, t, kap, mu);
+        fac<V>(NX == 1 ? -1 : D.a.T, t, kap, mu);
         SAt[t] = S * mu + M * kap;
         MAt[t] = M * mu;
     }
+    // Lambda(a type, b type) for the b type tb
     auto lam = [&](int tb, V& lP, V& lM, V& lB) {
         V kb, mb;
         fac<V>(D.b.T, tb, kb, mb);
@@ -138,75 +128,112 @@ __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M
             lB = SAt[2] * mb + MAt[2] * kb;
         }
     };
-    auto coefs = [&](int mb_cell, V* c) {
-        const V* q = cf + (int64_t)mb_cell * csb;
+    V X[NX], Y[NX], c[NX + 1];
+    auto coefs = [&](int mb_cell) {
+        const V* q = cf + mb_cell * csb;
 #pragma unroll
-        for (int i = 0; i <= NA; ++i) c[i] = (i <= na && (i == 0 || !avirt)) ? (unit ? unit_v : q[(int64_t)i * csa]) : V(0);
+        for (int i = 0; i <= NX; ++i)
+            if (NX > 1 || i == 0) c[i] = unit ? unit_v : q[i * csa];
     };
-    V X[NA], Y[NA], c[NA + 1];
     auto load = [&](int row) {
 #pragma unroll
-        for (int i = 0; i < NA; ++i) X[i] = i < na ? P[row * na + i] : V(0);
+        for (int i = 0; i < NX; ++i) X[i] = P[row * NX + i];
     };
     auto store = [&](int row) {
 #pragma unroll
-        for (int i = 0; i < NA; ++i)
-            if (i < na) P[row * na + i] = Y[i];
+        for (int i = 0; i < NX; ++i) P[row * NX + i] = Y[i];
     };
-    Modes<V, NA> Fp, Fc, acc;
-    V lP, lM, lB;
-    if (bvirt) {
-        load(0);
-        fwd_a<V, NA>(X, na, avirt, Fc);
-        coefs(0, c);
-        lam(3, lP, lM, lB);  // virtual b: identity factors
-        scale_a<V, NA>(Fc, c, na, lP, lM, lB, acc);
-        bwd_a<V, NA>(acc, na, avirt, Y);
-        store(0);
-        return;
-    }
-    load(0);
-    fwd_a<V, NA>(X, na, avirt, Fp);
-    coefs(0, c);
-    lam(2, lP, lM, lB);
-    scale_a<V, NA>(Fp, c, na, lP, lM, lB, acc);  // left boundary cell of b: row 0 only
-    V pP, pM, pB, mP, mM, mB;  // Lambda(a type, b type) of the interior b cells
-    lam(0, pP, pM, pB);
-    lam(1, mP, mM, mB);
-    for (int jb = 1; jb < nb; ++jb) {
-        load(jb);
-        fwd_a<V, NA>(X, na, avirt, Fc);
-        coefs(jb, c);  // interior b cell jb between rows jb-1 and jb
-        // per a mode: b modes P = Fp + Fc, M = Fp - Fc, scaled; row jb-1 gets
-        // P' + M' (complete), row jb starts with P' - M'
-        auto step = [&](V& ac, V& fp, V f, V cc, V lp, V lm) {
-            V gp = cc * lp * (fp + f), gm = cc * lm * (fp - f);
-            V done = ac + gp + gm;
-            ac = gp - gm;
-            fp = f;
-            return done;
-        };
-        Modes<V, NA> out;
-        out.bl = step(acc.bl, Fp.bl, Fc.bl, c[0], pB, mB);
-#pragma unroll
-        for (int i = 0; i < NA - 1; ++i) {
-            out.p[i] = step(acc.p[i], Fp.p[i], Fc.p[i], c[i + 1], pP, mP);
-            out.m[i] = step(acc.m[i], Fp.m[i], Fc.m[i], c[i + 1], pM, mM);
+    if constexpr (NX == 1) {
+        // one value per row: the b stream alone
+        V lP, lM, lB;
+        if (bvirt) {
+            coefs(0);
+            lam(3, lP, lM, lB);
+            P[0] = c[0] * lB * P[0];
+            return;
         }
-        V cbr = c[0];
+        V pP, pM, pB, mP, mM, mB;
+        lam(0, pP, pM, pB);
+        lam(1, mP, mM, mB);
+        lam(2, lP, lM, lB);
+        V fp = P[0];
+        coefs(0);
+        V acc = c[0] * lB * fp;
+        for (int jb = 1; jb < nb; ++jb) {
+            V f = P[jb];
+            coefs(jb);
+            V gp = c[0] * pB * (fp + f), gm = c[0] * mB * (fp - f);
+            P[jb - 1] = acc + gp + gm;
+            acc = gp - gm;
+            fp = f;
+        }
+        coefs(nb);
+        P[nb - 1] = acc + c[0] * lB * fp;
+    } else {
+        ModesX<V, NX> Fp, Fc, acc;
+        V lP, lM, lB;
+        if (bvirt) {
+            load(0);
+            fwd_x<V, NX>(X, Fc);
+            coefs(0);
+            lam(3, lP, lM, lB);  // virtual b: identity factors
+            acc.bl = c[0] * lB * Fc.bl;
+            acc.br = c[NX] * lB * Fc.br;
 #pragma unroll
-        for (int i = 1; i <= NA; ++i)
-            if (i == na) cbr = c[i];
-        out.br = step(acc.br, Fp.br, Fc.br, cbr, pB, mB);
-        bwd_a<V, NA>(out, na, avirt, Y);
-        store(jb - 1);
+            for (int i = 0; i < NX - 1; ++i) acc.pm[i] = mk2(c[i + 1] * lP * Fc.pm[i].x, c[i + 1] * lM * Fc.pm[i].y);
+            bwd_x<V, NX>(acc, Y);
+            store(0);
+            return;
+        }
+        V pP, pM, pB, mP, mM, mB;  // Lambda of the interior b cells: b type P (p..) and M (m..)
+        lam(0, pP, pM, pB);
+        lam(1, mP, mM, mB);
+        lam(2, lP, lM, lB);        // ... and of the boundary b cells
+        const V2 lp2 = mk2(pP, pM), lm2 = mk2(mP, mM);
+        load(0);
+        fwd_x<V, NX>(X, Fp);
+        coefs(0);  // left boundary b cell: row 0 only
+        acc.bl = c[0] * lB * Fp.bl;
+        acc.br = c[NX] * lB * Fp.br;
+#pragma unroll
+        for (int i = 0; i < NX - 1; ++i) acc.pm[i] = mk2(c[i + 1] * lP * Fp.pm[i].x, c[i + 1] * lM * Fp.pm[i].y);
+        for (int jb = 1; jb < nb; ++jb) {
+            load(jb);
+            fwd_x<V, NX>(X, Fc);
+            coefs(jb);  // interior b cell jb between rows jb-1 and jb
+            // per a mode: b modes P = Fp + Fc, M = Fp - Fc, scaled; row jb-1
+            // gets P' + M' (complete), row jb starts with P' - M'
+            ModesX<V, NX> out;
+            {
+                V gp = c[0] * pB * (Fp.bl + Fc.bl), gm = c[0] * mB * (Fp.bl - Fc.bl);
+                out.bl = acc.bl + gp + gm;
+                acc.bl = gp - gm;
+                gp = c[NX] * pB * (Fp.br + Fc.br);
+                gm = c[NX] * mB * (Fp.br - Fc.br);
+                out.br = acc.br + gp + gm;
+                acc.br = gp - gm;
+            }
+#pragma unroll
+            for (int i = 0; i < NX - 1; ++i) {
+                const V2 cc = mk2(c[i + 1], c[i + 1]);
+                const V2 gp = pmul(pmul(cc, lp2), padd(Fp.pm[i], Fc.pm[i]));
+                const V2 gm = pmul(pmul(cc, lm2), psub(Fp.pm[i], Fc.pm[i]));
+                out.pm[i] = padd(padd(acc.pm[i], gp), gm);
+                acc.pm[i] = psub(gp, gm);
+            }
+            Fp = Fc;
+            bwd_x<V, NX>(out, Y);
+            store(jb - 1);
+        }
+        coefs(nb);  // right boundary b cell: row nb-1 only
+        acc.bl += c[0] * lB * Fp.bl;
+        acc.br += c[NX] * lB * Fp.br;
+#pragma unroll
+        for (int i = 0; i < NX - 1; ++i)
+            acc.pm[i] = padd(acc.pm[i], mk2(c[i + 1] * lP * Fp.pm[i].x, c[i + 1] * lM * Fp.pm[i].y));
+        bwd_x<V, NX>(acc, Y);
+        store(nb - 1);
     }
-    coefs(nb, c);  // right boundary cell of b: row nb-1 only
-    lam(2, lP, lM, lB);
-    scale_a<V, NA>(Fp, c, na, lP, lM, lB, Fc);
-    add_modes<V, NA>(acc, Fc, V(1));
-    bwd_a<V, NA>(acc, na, avirt, Y);
-    store(nb - 1);
 }
 
 }  // namespace lsg_sfk
@@ -214,7 +241,7 @@ __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M
 // One CTA per dense (case, slab) item.  sf: per-slab plans of this precision;
 // coef: collapsed coefficients (or unit: the slab's 2^#collapsed).
 template <typename V, int NA>
-__global__ void __launch_bounds__(256) k_sf(const lsg::PhaseBItem* __restrict__ items, const lsg::SfSlab* __restrict__ sf,
+__global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg::PhaseBItem* __restrict__ items, const lsg::SfSlab* __restrict__ sf,
                                             const V* __restrict__ pc, V* __restrict__ zb, const V* __restrict__ coef,
                                             const int32_t* __restrict__ order, int32_t ord0, int unit, int form) {
     using namespace lsg_sfk;
@@ -288,13 +315,22 @@ __global__ void __launch_bounds__(256) k_sf(const lsg::PhaseBItem* __restrict__ 
             for (int i = nq - 1; i >= 0; --i) x += quot(D.qB[i], x) * (uint32_t)D.qmult[i];
             return (int64_t)x;
         };
-        // gather
-        V* s0 = region(0);
-        for (int e = tid; e < D.slice; e += T) {
-            const int64_t ue = upos((uint32_t)e);
+        // the slice of u for this chunk tuple at stage-0 position e, and its transpose into z
+        auto gath = [&](uint32_t e) {
+            const int64_t ue = upos(e);
             V acc = V(0);
             for (int c = 0; c < ncomb; ++c) acc += s_sgn[c] * u[s_off[c] + ue];
-            s0[e] = acc;
+            return acc;
+        };
+        auto scat = [&](uint32_t e, V v) {
+            const int64_t ue = upos(e);
+            if (nq == 0) z[ue] = v;
+            else
+                for (int c = 0; c < ncomb; ++c) z[s_off[c] + ue] += s_sgn[c] * v;
+        };
+        {  // gather the slice into stage 0
+            V* s0 = region(0);
+            for (int e = tid; e < D.slice; e += T) s0[e] = gath((uint32_t)e);
         }
         __syncthreads();
         // mid sweeps, forward
@@ -338,7 +374,10 @@ __global__ void __launch_bounds__(256) k_sf(const lsg::PhaseBItem* __restrict__ 
                     combine<V>(S, M, x.T, type);
                     cb += (int64_t)cell * x.cstride;
                 }
-                fused_plane<V, NA>(F + (size_t)pl * plane, D, S, M, cf0 + cb, unit != 0, unit_v, form);
+                V* Pp = F + (size_t)pl * plane;
+                if (D.a.T < 0) fused_plane<V, 1>(Pp, D, S, M, cf0 + cb, unit != 0, unit_v, form);
+                else if (NA >= 7 && D.a.n == 7) fused_plane<V, (NA >= 7 ? 7 : 3)>(Pp, D, S, M, cf0 + cb, unit != 0, unit_v, form);
+                else fused_plane<V, 3>(Pp, D, S, M, cf0 + cb, unit != 0, unit_v, form);
             }
             __syncthreads();
         }
@@ -363,14 +402,9 @@ __global__ void __launch_bounds__(256) k_sf(const lsg::PhaseBItem* __restrict__ 
             }
             __syncthreads();
         }
-        // scatter
-        for (int e = tid; e < D.slice; e += T) {
-            V v = s0[e];
-            if (nq == 0) z[e] = v;
-            else {
-                const int64_t ue = upos((uint32_t)e);
-                for (int c = 0; c < ncomb; ++c) z[s_off[c] + ue] += s_sgn[c] * v;
-            }
+        {  // scatter stage 0 into z
+            const V* s0 = region(0);
+            for (int e = tid; e < D.slice; e += T) scat((uint32_t)e, s0[e]);
         }
         __syncthreads();
     }

@@ -326,17 +326,23 @@ int64_t lsgo_num_cells(const lsgo_grid *g, const int32_t *T) {
  * z[p] += K u[q]. */
 static void cells_apply(lsgo_grid *g, int t, int family, const double *params, const double *u, double *z) {
     int d = g->d;
+    const unsigned nc = 1u << d;
     celllist *cl = get_cells(g, t);
+    /* the Q1 entries depend only on the cell widths, equal for all cells of one
+     * depth: one table per call, the same values the plugin returns per cell */
+    double *K = malloc(sizeof(double) * nc * nc);
+    for (unsigned p = 0; p < nc; ++p)
+        for (unsigned q = p; q < nc; ++q) K[p * nc + q] = lsg_q1_entry(g->form, d, cl->h, p, q);
     for (int64_t c = 0; c < cl->nc; ++c) {
         const int64_t *corner = cl->corner + (c << d);
         double a = lsg_coef_eval(family, params, d, cl->xc + c * d);
-        for (unsigned p = 0; p < (1u << d); ++p) {
+        for (unsigned p = 0; p < nc; ++p) {
             int64_t kp = corner[p];
             if (kp < 0) continue;
-            for (unsigned q = p; q < (1u << d); ++q) {
+            for (unsigned q = p; q < nc; ++q) {
                 int64_t kq = corner[q];
                 if (kq < 0) continue;
-                double val = a * lsg_q1_entry(g->form, d, cl->h, p, q);
+                double val = a * K[p * nc + q];
                 if (p == q) z[kq] += val * u[kp];
                 else {
                     z[kq] += val * u[kp];
@@ -345,6 +351,7 @@ static void cells_apply(lsgo_grid *g, int t, int family, const double *params, c
             }
         }
     }
+    free(K);
 }
 
 /* ------------------------------------------------------------ stencils on points */
