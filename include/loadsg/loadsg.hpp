@@ -11,15 +11,31 @@
 //     multiplication(prew, Ax, problem)   MatrixVectorHomogen.h:91-92
 //   CG::solveHomogen              applications/cg_method.h:27-33
 //
-// Differences a caller must know: the grid is frozen when the first
-// MatrixVectorHomogen is built from it (the tables are flattened once); errors
-// throw lsg::Error instead of exit(1).
+//   MultiLevelAdaptiveSparseGrid  sgrid/multilevelSparseGrid.h:13-143 (a handle: the
+//                                 multilevel store lives in the operator's slabs)
+//   calcPrewByNodal / calcNodalByPrew (prew, u)   BasisTransformations/BasisTransformations.h:117,123
+//
+// The reference's own signatures are all here: MatrixVectorHomogen(grid,
+// mgrid, symmetry, mpi_on) (MatrixVectorHomogen.h:72-77), CG::solveHomogen(eps,
+// x, f, &iterations, usol, matrix, stencil, &time) (cg_method.h:27-33), the
+// two-argument transforms (the operator is found through the vector's grid),
+// and L2 / H1 built from (grid, mgrid).  include/loadsg/compat/source/
+// sparseEXPDE.h maps the reference's non-template names (dimension from the
+// DimensionSparseGrid macro, IndexDimension, vector expressions) onto these, so
+// a reference main compiles with the compat directory on the include path.
+//
+// Differences a caller must know: the grid is frozen when the first operator
+// is built from it (the tables are flattened once); errors throw lsg::Error
+// instead of exit(1); the MPI flag of MatrixVectorHomogen must be false (one
+// GPU, no MPI) and the symmetry flag is accepted as given (the operator is
+// symmetric either way).
 #pragma once
 #include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -37,9 +53,30 @@ inline void check(int rc) {
 }
 
 template <int D>
+class MatrixVectorHomogen;
+
+template <int D>
 class AdaptiveSparseGrid {
 public:
     using Index = std::array<int32_t, D>;
+    // the reference's switch between all and only active points in its vector
+    // loops (sgrid/sparseGrid.h:186); vector operations here always cover all
+    // entries, as the reference's expression templates do with the switch off
+    bool WorkOnHangingNodes = false;
+    // AddRecursiveSonsOfPoint(center, level) with the center point given as
+    // indices (the reference's IndexDimension()): every index must be 2.
+    void AddRecursiveSonsOfPoint(const Index& center, int level) {
+        for (int d = 0; d < D; ++d)
+            if (center[d] != 2) throw Error("AddRecursiveSonsOfPoint: only the center point is supported");
+        AddRecursiveSonsOfPoint(level);
+    }
+    // The operator the two-argument transforms and the (grid, mgrid) norms use:
+    // the last MatrixVectorHomogen built on this grid, else one made on first use.
+    MatrixVectorHomogen<D>& op() const;
+    void attach(MatrixVectorHomogen<D>* m) const { attached_ = m; }
+    void detach(MatrixVectorHomogen<D>* m) const {
+        if (attached_ == m) attached_ = nullptr;
+    }
     // AddPoint (sgrid/sparseGrid.cc:482-516): appends in storage order, returns
     // false if the point is already present (it is then marked active).
     bool AddPoint(const Index& I, bool active = true) {
@@ -127,6 +164,21 @@ private:
     std::vector<int32_t> points_;
     std::vector<uint8_t> active_;
     std::map<Index, int64_t> where_;
+    mutable MatrixVectorHomogen<D>* attached_ = nullptr;
+    mutable std::shared_ptr<MatrixVectorHomogen<D>> own_;
+};
+
+// MultiLevelAdaptiveSparseGrid (sgrid/multilevelSparseGrid.h:13-143): the
+// reference's (I, T) store.  The flattened slabs of the operator hold it here,
+// so this is a handle on the grid that keeps the reference's constructor.
+template <int D>
+class MultiLevelAdaptiveSparseGrid {
+public:
+    explicit MultiLevelAdaptiveSparseGrid(AdaptiveSparseGrid<D>* grid) : grid_(grid) {}
+    AdaptiveSparseGrid<D>* getSparseGrid() const { return grid_; }
+
+private:
+    AdaptiveSparseGrid<D>* grid_;
 };
 
 template <int D>
@@ -140,8 +192,30 @@ public:
     const double* getDatatableVector() const { return data_.data(); }
     int64_t size() const { return (int64_t)data_.size(); }
     void operator=(double v) { std::fill(data_.begin(), data_.end(), v); }
+    VectorSparseG& operator=(const VectorSparseG& o) {
+        if (this != &o) {
+            if (o.size() != size()) throw Error("VectorSparseG: vectors of different grids");
+            data_ = o.data_;
+        }
+        return *this;
+    }
+    VectorSparseG(const VectorSparseG&) = default;
+    // element-wise over all entries, like the reference's expression templates (extemp/extempAlg.h)
+    friend VectorSparseG operator+(const VectorSparseG& a, const VectorSparseG& b) { return combine(a, b, 1.0); }
+    friend VectorSparseG operator-(const VectorSparseG& a, const VectorSparseG& b) { return combine(a, b, -1.0); }
+    friend VectorSparseG operator*(double s, const VectorSparseG& a) {
+        VectorSparseG r(*a.grid_);
+        for (int64_t k = 0; k < a.size(); ++k) r.data_[k] = s * a.data_[k];
+        return r;
+    }
 
 private:
+    static VectorSparseG combine(const VectorSparseG& a, const VectorSparseG& b, double sb) {
+        if (a.size() != b.size()) throw Error("VectorSparseG: vectors of different grids");
+        VectorSparseG r(*a.grid_);
+        for (int64_t k = 0; k < a.size(); ++k) r.data_[k] = a.data_[k] + sb * b.data_[k];
+        return r;
+    }
     const AdaptiveSparseGrid<D>* grid_;
     std::vector<double> data_;
 };
@@ -177,10 +251,21 @@ inline double L_infty(const VectorSparseG<D>& v) {
 template <int D>
 class MatrixVectorHomogen {
 public:
-    explicit MatrixVectorHomogen(const AdaptiveSparseGrid<D>& g) {
+    explicit MatrixVectorHomogen(const AdaptiveSparseGrid<D>& g) : grid_(&g) {
         check(lsg_operator_create(D, g.points(), g.getActiveTable(), g.getMaximalOccupiedSecondTable(), &op_));
+        g.attach(this);
     }
-    ~MatrixVectorHomogen() { lsg_operator_destroy(op_); }
+    // The reference's constructor (MatrixVectorHomogen.h:72-77).
+    MatrixVectorHomogen(AdaptiveSparseGrid<D>& g, MultiLevelAdaptiveSparseGrid<D>& mgrid, bool symmetry, bool mpi_on)
+        : MatrixVectorHomogen(g) {
+        (void)symmetry;
+        if (mgrid.getSparseGrid() != &g) throw Error("MatrixVectorHomogen: mgrid was built on another grid");
+        if (mpi_on) throw Error("MatrixVectorHomogen: no MPI distribution (one GPU)");
+    }
+    ~MatrixVectorHomogen() {
+        grid_->detach(this);
+        lsg_operator_destroy(op_);
+    }
     MatrixVectorHomogen(const MatrixVectorHomogen&) = delete;
     MatrixVectorHomogen& operator=(const MatrixVectorHomogen&) = delete;
 
@@ -206,15 +291,36 @@ public:
     }
 
 private:
+    const AdaptiveSparseGrid<D>* grid_;
     lsg_operator* op_ = nullptr;
     bool have_ = false;
     int32_t fam_ = -1, form_ = LSG_FORM_STIFFNESS;
     std::vector<double> par_;
 };
 
+template <int D>
+MatrixVectorHomogen<D>& AdaptiveSparseGrid<D>::op() const {
+    if (attached_) return *attached_;
+    if (!own_) {
+        own_ = std::make_shared<MatrixVectorHomogen<D>>(*this);
+        attached_ = own_.get();
+    }
+    return *own_;
+}
+
 struct CG {
-    // CG::solveHomogen(eps, x, f, &iterations, usol, matrix, stencil, &time):
-    // Jacobi-preconditioned CG with the reference's stopping rule on r^T D^-1 r.
+    // CG::solveHomogen(eps, x, f, &iterations, usol, matrix, stencil, &time)
+    // (applications/cg_method.h:27-33): Jacobi-preconditioned CG with the
+    // reference's stopping rule on r^T D^-1 r.  usol is accepted as the
+    // reference takes it (its error history output is not written); *time
+    // receives the solve's seconds.
+    template <int D>
+    static bool solveHomogen(double eps, VectorSparseG<D>& x, const VectorSparseG<D>& f, int* iterations,
+                             const VectorSparseG<D>& usol, MatrixVectorHomogen<D>& matrix,
+                             const MidpointDiffusion& problem, double* time) {
+        (void)usol;
+        return solveHomogen<D>(eps, x, f, iterations, matrix, problem, time);
+    }
     template <int D>
     static bool solveHomogen(double eps, VectorSparseG<D>& x, const VectorSparseG<D>& f, int* iterations,
                              MatrixVectorHomogen<D>& matrix, const MidpointDiffusion& problem, double* seconds,
@@ -246,6 +352,15 @@ template <int D>
 inline void calcPrewByNodal(VectorSparseG<D>& prew, const VectorSparseG<D>& u, MatrixVectorHomogen<D>& matrix) {
     check(lsg_calc_prew_by_nodal(matrix.handle(), prew.getDatatableVector(), u.getDatatableVector()));
 }
+// The reference's two-argument forms: the operator of the vectors' grid.
+template <int D>
+inline void calcNodalByPrew(const VectorSparseG<D>& prew, VectorSparseG<D>& u) {
+    calcNodalByPrew<D>(prew, u, prew.getSparseGrid()->op());
+}
+template <int D>
+inline void calcPrewByNodal(VectorSparseG<D>& prew, const VectorSparseG<D>& u) {
+    calcPrewByNodal<D>(prew, u, prew.getSparseGrid()->op());
+}
 
 // H1::getValue / L2::getValue (applications/H1_Norm.cpp): the H1 seminorm and
 // the L2 norm of the function with nodal values u.  The reference constructs
@@ -255,6 +370,7 @@ template <int D>
 class H1 {
 public:
     explicit H1(MatrixVectorHomogen<D>& matrix) : m_(matrix) {}
+    H1(AdaptiveSparseGrid<D>& grid, MultiLevelAdaptiveSparseGrid<D>&) : m_(grid.op()) {}
     double getValue(const VectorSparseG<D>& u) {
         double v = 0.0;
         check(lsg_h1_norm(m_.handle(), u.getDatatableVector(), &v));
@@ -268,6 +384,7 @@ template <int D>
 class L2 {
 public:
     explicit L2(MatrixVectorHomogen<D>& matrix) : m_(matrix) {}
+    L2(AdaptiveSparseGrid<D>& grid, MultiLevelAdaptiveSparseGrid<D>&) : m_(grid.op()) {}
     double getValue(const VectorSparseG<D>& u) {
         double v = 0.0;
         check(lsg_l2_norm(m_.handle(), u.getDatatableVector(), &v));

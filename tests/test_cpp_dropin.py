@@ -1,13 +1,42 @@
 """The header-only C++ drop-in (include/loadsg/loadsg.hpp) compiles against
-liblsg.so on the CPU; on a GPU it solves a d=3 problem through the C-ABI."""
+liblsg.so on the CPU; on a GPU it solves through the C-ABI.
+
+The reference's own Poisson example (examples_doxygen/poisson_regular.cpp)
+compiles unchanged against the compatibility header
+include/loadsg/compat/source/sparseEXPDE.h when the reference's sources are at
+hand (LOADSG_REFERENCE = its library/source directory); the binary is kept in
+tests/cpp/_build and its table is checked on the GPU against the table the
+compiled reference printed (tests/golden/ex_poisson_d3.npz), as is the table of
+the repository's own port of that example."""
 import os
 import subprocess
 
+import numpy as np
 import pytest
 
 import loadsg_b200 as lsg
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BUILD = os.path.join(ROOT, "tests", "cpp", "_build")
+REF_MAIN_EXE = os.path.join(BUILD, "poisson_regular_reference")
+GOLDEN_TABLE = os.path.join(ROOT, "tests", "golden", "ex_poisson_d3.npz")
+
+
+def link_args():
+    return [lsg.LIB_PATH, "-Wl,-rpath," + os.path.dirname(lsg.LIB_PATH)]
+
+
+def check_table(rows, ncols):
+    """rows: (level, dofs, linfty, l2, h1, iterations) for levels 1..5 against
+    the reference's table: DOFs exact, iterations within one, errors 1e-4."""
+    z = np.load(GOLDEN_TABLE)
+    rows = np.array(rows[:5], np.float64)
+    assert rows.shape == (5, ncols)
+    assert np.array_equal(rows[:, 0], np.arange(1, 6))
+    assert np.array_equal(rows[:, 1], z["dofs"])
+    assert np.abs(rows[:, 5] - z["iterations"]).max() <= 1
+    for j, key in ((2, "linfty"), (3, "l2"), (4, "h1")):
+        assert np.abs(rows[:, j] / z[key] - 1.0).max() < 1e-4, (key, rows[:, j], z[key])
 
 
 def build_example(tmp_path):
@@ -51,15 +80,35 @@ def test_header_adaptive_example_matches_reference(tmp_path):
     assert out[-1] == "# 23 18"
 
 
-def test_poisson_example_port_compiles(tmp_path):
-    """The reference's Poisson example written against the drop-in
-    (tests/cpp/poisson_regular_port.cpp) compiles and links; its table is
-    checked on the GPU through the same library calls in tests/test_poisson_example.py."""
+def build_port(tmp_path):
     exe = str(tmp_path / "poisson_regular_port")
     subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
-                    os.path.join(ROOT, "tests", "cpp", "poisson_regular_port.cpp"), lsg.LIB_PATH,
-                    "-Wl,-rpath," + os.path.dirname(lsg.LIB_PATH), "-o", exe], check=True, capture_output=True)
-    assert os.path.exists(exe)
+                    os.path.join(ROOT, "tests", "cpp", "poisson_regular_port.cpp")] + link_args() + ["-o", exe],
+                   check=True, capture_output=True)
+    return exe
+
+
+def test_poisson_example_port_compiles(tmp_path):
+    """The reference's Poisson example written against the drop-in
+    (tests/cpp/poisson_regular_port.cpp) compiles and links."""
+    assert os.path.exists(build_port(tmp_path))
+
+
+def test_reference_main_compiles_unchanged():
+    """examples_doxygen/poisson_regular.cpp of the reference, as it is, with
+    only the include path pointing at the compatibility header: it compiles
+    and links against liblsg.so (the binary is kept for the GPU test)."""
+    ref = os.environ.get("LOADSG_REFERENCE")
+    if not ref:
+        pytest.skip("LOADSG_REFERENCE (the reference's library/source directory) not set")
+    src = os.path.join(os.path.dirname(os.path.abspath(ref)), "examples_doxygen", "poisson_regular.cpp")
+    if not os.path.exists(src):
+        pytest.skip(f"{src} not found")
+    os.makedirs(BUILD, exist_ok=True)
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-DDimensionSparseGrid=3", "-I",
+                        os.path.join(ROOT, "include", "loadsg", "compat"), src] + link_args() + ["-o", REF_MAIN_EXE],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
 
 
 def test_dropin_header_compiles_and_links(tmp_path):
@@ -68,7 +117,43 @@ def test_dropin_header_compiles_and_links(tmp_path):
 
 @pytest.mark.gpu
 def test_dropin_solves_on_gpu(tmp_path):
+    """A d=3 level-5 solve through the header: relative residual below 1e-8,
+    transform round trip 1e-10, boundary forms of g = 1 (gradient form 0, root
+    mass 1/8)."""
     exe = build_example(tmp_path)
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "relres" in r.stdout
+    f = dict(kv.split("=") for kv in r.stdout.split() if "=" in kv)
+    assert int(f["N"]) == 351
+    assert 0 < int(f["iterations"]) <= 100
+    assert float(f["relres"]) < 1e-8
+    nums = r.stdout.split()
+    assert float(nums[nums.index("trip") + 1]) < 1e-10
+    assert float(nums[nums.index("mass") + 1]) == 0.125
+
+
+@pytest.mark.gpu
+def test_poisson_port_table_on_gpu(tmp_path):
+    """The port's convergence table (levels 1..5) equals the compiled
+    reference's: DOFs, CG iterations within one, errors to 1e-4."""
+    out = subprocess.run([build_port(tmp_path)], check=True, capture_output=True, text=True).stdout
+    check_table([list(map(float, line.split())) for line in out.splitlines() if line.strip()], 6)
+
+
+@pytest.mark.gpu
+def test_reference_main_on_gpu():
+    """The reference's own poisson_regular.cpp, compiled unchanged against the
+    compatibility header, run on the GPU: its printed table (level, DOFs, L_inf
+    error and ratio, L2 error and ratio, L2+H1 error and ratio, iterations) for
+    levels 1..5 equals the one the compiled reference printed."""
+    if not os.path.exists(REF_MAIN_EXE):
+        pytest.skip("the reference's example was not compiled here (test_reference_main_compiles_unchanged)")
+    r = subprocess.run([REF_MAIN_EXE], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    rows = []
+    for line in r.stdout.splitlines():
+        p = line.split()
+        if len(p) == 9 and p[0].isdigit():
+            v = list(map(float, p))
+            rows.append([v[0], v[1], v[2], v[4], v[6], v[8]])
+    check_table(rows, 6)
