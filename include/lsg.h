@@ -94,9 +94,9 @@ int lsg_matvec_device(lsg_operator *op, const void *x, void *y, int32_t precisio
 
 /* Allocation-free variant of lsg_matvec_device (no counterpart in the
  * reference, which has no device code).  For callers that cannot allocate
- * device memory at call time: code running during CUDA graph capture, hosts
- * whose own allocator owns the whole device, loops that cannot afford the
- * synchronisation of cudaMalloc/cudaFree.  Its work space is one fixed 32 MiB
+ * device memory at call time: hosts whose own allocator owns the whole
+ * device, loops that cannot afford the synchronisation of cudaMalloc/cudaFree.
+ * Its work space is one fixed 32 MiB
  * array compiled into the library (held on every GPU that loads it until the
  * process exits); grids needing more are rejected with LSG_E_INVALID and a
  * message giving both sizes.  It calls no cudaMalloc/cudaFree.  The first call

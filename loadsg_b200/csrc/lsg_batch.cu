@@ -316,9 +316,9 @@ int batch_matvec(lsg_batch* b, const V* x, V* y, cudaStream_t st) {
     return 0;
 }
 
-int64_t batch_matvec_launches(const lsg_batch* b) {
+int64_t batch_matvec_launches(const lsg_batch* b, bool f32) {
     int64_t l = 0;
-    for (auto& g : b->groups) l += lsg_internal::matvec_launch_count(g.op);
+    for (auto& g : b->groups) l += lsg_internal::matvec_launch_count(g.op, f32);
     return l;
 }
 
@@ -454,7 +454,7 @@ struct BSolver {
         }
         if (exec) cudaGraphExecDestroy(exec);
         *ran = it;
-        *launches += (int64_t)it * (batch_matvec_launches(B) + 8);
+        *launches += (int64_t)it * (batch_matvec_launches(B, std::is_same<V, float>::value) + 8);
         return rc;
     }
 };
@@ -530,7 +530,7 @@ int batch_solve(lsg_batch* b, const double* f, double* x, const lsg_solver_opts*
         if (!rc)
             rc = S.loop<double>(x, r, S.g.as<double>(), S.d.as<double>(), S.h.as<double>(), z, crit, eps, maxit, graph, st,
                                 &rounds, &launches);
-        launches += batch_matvec_launches(b) + 12;
+        launches += batch_matvec_launches(b, false) + 12;
         outer_rounds = 1;
     } else {
         const int inner = o->inner_iter > 0 ? o->inner_iter : 1000;
@@ -555,7 +555,7 @@ int batch_solve(lsg_batch* b, const double* f, double* x, const lsg_solver_opts*
                                                      S.rr_prev.as<double>());
             BT_TRY(cudaMemcpyAsync(S.pend_h, S.S.pending, 4, cudaMemcpyDeviceToHost, st));
             BT_TRY(cudaStreamSynchronize(st));
-            launches += batch_matvec_launches(b) + 6;
+            launches += batch_matvec_launches(b, false) + 6;
             if (*S.pend_h == 0) break;
             ++outer_rounds;
             kb_scale_f32<<<b->nchunks, kThreads, 0, st>>>(S.ch(), S.S.scale, r, S.r32.as<float>());

@@ -4,7 +4,7 @@
 //   k_nodal      prewavelet -> nodal values per depth (calcNodal,
 //                MatrixVectorHomogen.cpp:43-74), sum-factorised 3-tap stages
 //   k_pinit      P_c(T) = nodal(T)            ("P += nodal", MVH.h:1649)
-//   k_prolong    one prolongation level       (MVH.h:1655-1670, 444-474)
+//   k_prolong    prolongation chains, one launch per dimension (MVH.h:1655-1670, 444-474)
 //   k_sf         the level-T cell operator (LocalStiffnessMatrices.cpp:555-582)
 //                of dense slabs, factorised over reduced modes (lsg_sf_kernel.cuh)
 //   k_cells      the same for sparse slabs, per cell in the Walsh-Hadamard
@@ -26,8 +26,11 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
+#include <set>
+#include <tuple>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -82,6 +85,8 @@ struct DevPlan {
     const lsg::PhaseBItem* b_items;
     const lsg::PhaseBStep* b_steps;
     const int32_t* pts;
+    const int32_t* a_chain_off;     // per prolongation chain: range in a_chain_items
+    const int32_t* a_chain_items;   // phase-A items, chain by chain, in chain order
     const int64_t* sp_slot_off;     // per phase-B item of a sparse slab: first cell slot (-1: dense)
     const int64_t* sp_inc_base;     // per sparse slab: start of its per-entry ranges in sp_inc_off
     const int64_t* sp_inc_off;      // per sparse-slab entry: range of its (cell, corner) slots in sp_inc
@@ -152,18 +157,26 @@ __global__ void k_pinit(DevPlan P, const V* __restrict__ ml, V* __restrict__ pc,
     for (int64_t e = threadIdx.x; e < s.n; e += blockDim.x) pc[it.p_off + e] = ml[s.off + e];
 }
 
+// One prolongation chain per CTA: the items of one case and dimension k along
+// a line of depths T, T + e_k, T + 2 e_k, ... in that order (each item reads
+// the previous one's output), so a dimension's whole level loop is one launch.
+// Chains of one dimension are independent: they write different slabs.
 template <typename V>
-__global__ void k_prolong(DevPlan P, V* __restrict__ pc, int32_t item0) {
-    const lsg::PhaseAItem it = P.a_items[item0 + blockIdx.x];
-    const int32_t* tab = P.prol + it.tab_off;
-    const V* src = pc + it.src_off;
-    V* dst = pc + it.dst_off;
-    for (int64_t e = threadIdx.x; e < it.n_dst; e += blockDim.x) {
-        int32_t a = tab[2 * e], b = tab[2 * e + 1];
-        V add;
-        if (b == -2) add = src[a];
-        else add = V(0.5) * ((b >= 0 ? src[b] : V(0)) + (a >= 0 ? src[a] : V(0)));
-        dst[e] = dst[e] + add;
+__global__ void k_prolong(DevPlan P, V* __restrict__ pc, int32_t chain0) {
+    const int32_t c = chain0 + blockIdx.x;
+    for (int32_t j = P.a_chain_off[c]; j < P.a_chain_off[c + 1]; ++j) {
+        const lsg::PhaseAItem it = P.a_items[P.a_chain_items[j]];
+        const int32_t* tab = P.prol + it.tab_off;
+        const V* src = pc + it.src_off;
+        V* dst = pc + it.dst_off;
+        for (int64_t e = threadIdx.x; e < it.n_dst; e += blockDim.x) {
+            int32_t a = tab[2 * e], b = tab[2 * e + 1];
+            V add;
+            if (b == -2) add = src[a];
+            else add = V(0.5) * ((b >= 0 ? src[b] : V(0)) + (a >= 0 ? src[a] : V(0)));
+            dst[e] = dst[e] + add;
+        }
+        __syncthreads();
     }
 }
 
@@ -786,7 +799,9 @@ struct lsg_operator {
     // tables
     DBuf slabs, did, act, exa_off, exa, cell_key, cell_corner, nodal_stage, nodal_src, nodal_code, nodal_dom, nodal_scr,
         conv_stage, conv_src, conv_code, conv_dom, prol, restr, a_items, b_items, b_steps, pts, cell_slab_off,
-        conv_off, conv_items_off, conv_items, sp_slot_off, sp_inc_base, sp_inc_off, sp_inc;
+        conv_off, conv_items_off, conv_items, sp_slot_off, sp_inc_base, sp_inc_off, sp_inc, a_chain_off, a_chain_items;
+    std::vector<int32_t> a_dim_chain_off;  // per dimension: its chains [off[k], off[k+1])
+
     int64_t conv_total = 0;  // convert slots of one matvec
     int64_t sp_total = 0;    // cell slots of the sparse-slab items of one matvec
     DBuf lam64, lam32;   // Hadamard-basis eigenvalues of the Q1 stiffness (form 0)
@@ -822,8 +837,8 @@ struct lsg_operator {
     DBuf coll64, coll32, coll_off, coll_slab, slab_T, slab_cell_off;  // collapsed coefficients
     struct SfPrec {
         DBuf plans, order;
-        std::vector<int32_t> class_off;
-        std::vector<int32_t> class_w;
+        std::vector<int32_t> class_off;    // k_sf launches (work-space classes)
+        std::vector<int32_t> class_w;      // dynamic shared memory (bytes) of each launch
         std::vector<uint8_t> ok;  // per slab: the plan fits
         DBuf cell_order;
         std::vector<int32_t> cell_class_off;
@@ -835,10 +850,10 @@ namespace {
 
 // Launch plan of the cell operator.  Dense slabs go to k_sf (planned per
 // precision for a work space of tune.cell_space_kb, FP64 with half the
-// elements), ordered by work space, largest first, in classes: a new class
-// (launch) starts when the work space shrinks by tune.class_ratio.  Items of
-// sparse slabs go to k_cells by slab size, with shared memory for N_T of the
-// class's largest slab.
+// elements) in work-space classes.  Items of sparse slabs go to k_cells by
+// slab size in classes, with shared memory for N_T of the class's largest
+// slab.  A new class (launch) starts when the size shrinks by
+// tune.class_ratio.
 int build_sf_prec(lsg_operator* op, lsg_operator::SfPrec& S, int64_t wcap, int na_max) {
     const lsg::Plan& p = op->plan;
     std::vector<lsg::SfSlab> plans = lsg::sf_plan(p, op->sf_layout, wcap, na_max);
@@ -847,6 +862,9 @@ int build_sf_prec(lsg_operator* op, lsg_operator::SfPrec& S, int64_t wcap, int n
         S.ok[t] = plans[t].nm >= 0;
         if (p.slabs[t].dense && !S.ok[t]) return fail(LSG_E_INVALID, "no factorised plan fits a dense slab");
     }
+    // k_sf: items by work space, largest first, in classes (a new class,
+    // i.e. launch, starts when the work space shrinks by tune.class_ratio);
+    // each launch has thousands of items, which keeps every SM busy
     std::vector<int32_t> ord, cord;
     for (size_t i = 0; i < p.b_items.size(); ++i) (S.ok[p.b_items[i].t] ? ord : cord).push_back((int32_t)i);
     std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) {
@@ -854,13 +872,20 @@ int build_sf_prec(lsg_operator* op, lsg_operator::SfPrec& S, int64_t wcap, int n
     });
     S.class_off.clear();
     S.class_w.clear();
-    int64_t bound = -1;
-    for (size_t i = 0; i < ord.size(); ++i) {
-        int64_t w = std::max(plans[p.b_items[ord[i]].t].wtotal, 1);
-        if (bound < 0 || w * op->tune.class_ratio < bound) {
-            S.class_off.push_back((int32_t)i);
-            S.class_w.push_back((int32_t)w);
-            bound = w;
+    {
+        const size_t vb = (&S == &op->sf32) ? 4 : 8;
+        int64_t bound = -1;
+        for (size_t i = 0; i < ord.size(); ++i) {
+            const lsg::SfSlab& D = plans[p.b_items[ord[i]].t];
+            int64_t w = std::max(D.wtotal, 1);
+            int64_t bytes = (int64_t)lsg::sf_smem_bytes(D, vb);
+            if (bound < 0 || w * op->tune.class_ratio < bound) {
+                S.class_off.push_back((int32_t)i);
+                S.class_w.push_back((int32_t)bytes);
+                bound = w;
+            } else {
+                S.class_w.back() = std::max<int32_t>(S.class_w.back(), (int32_t)bytes);
+            }
         }
     }
     S.class_off.push_back((int32_t)ord.size());
@@ -869,7 +894,7 @@ int build_sf_prec(lsg_operator* op, lsg_operator::SfPrec& S, int64_t wcap, int n
     });
     S.cell_class_off.clear();
     S.cell_class_n.clear();
-    bound = -1;
+    int64_t bound = -1;
     for (size_t i = 0; i < cord.size(); ++i) {
         int64_t n = p.slabs[p.b_items[cord[i]].t].n;
         if (bound < 0 || n * op->tune.class_ratio < bound) {
@@ -971,6 +996,36 @@ int upload_plan(lsg_operator* op) {
         rc |= op->conv_items_off.upload(ioff, tot);
         rc |= op->conv_items.upload(items, tot);
     }
+    {  // prolongation chains: per dimension, items linked source -> target within a case
+        std::map<std::tuple<int, int, int>, int32_t> by_src;  // (case, source depth, dim) -> item
+        std::set<std::tuple<int, int, int>> targets;
+        for (size_t i = 0; i < p.a_items.size(); ++i) {
+            const lsg::PhaseAItem& a = p.a_items[i];
+            by_src[std::make_tuple(a.c, a.t_src, a.dim)] = (int32_t)i;
+            targets.insert(std::make_tuple(a.c, a.t_dst, a.dim));
+        }
+        std::vector<int32_t> coff, citems;
+        op->a_dim_chain_off.assign(d + 1, 0);
+        for (int k = 0; k < d; ++k) {
+            op->a_dim_chain_off[k] = (int32_t)coff.size();
+            for (size_t i = 0; i < p.a_items.size(); ++i) {  // chain heads: not the target of another item
+                const lsg::PhaseAItem& a = p.a_items[i];
+                if (a.dim != k || targets.count(std::make_tuple(a.c, a.t_src, a.dim))) continue;
+                coff.push_back((int32_t)citems.size());
+                for (int32_t cur = (int32_t)i;;) {
+                    citems.push_back(cur);
+                    auto nx = by_src.find(std::make_tuple(a.c, p.a_items[cur].t_dst, k));
+                    if (nx == by_src.end()) break;
+                    cur = nx->second;
+                }
+            }
+        }
+        op->a_dim_chain_off[d] = (int32_t)coff.size();
+        coff.push_back((int32_t)citems.size());
+        if (citems.empty()) citems.push_back(0);
+        rc |= op->a_chain_off.upload(coff, tot);
+        rc |= op->a_chain_items.upload(citems, tot);
+    }
     {  // sparse slabs: per item its cell slots; per entry its (cell, corner) slots in cell order
         const int nc = 1 << d;
         std::vector<int64_t> soff(std::max<size_t>(p.b_items.size(), 1), -1), base(p.nD, -1), ioff;
@@ -1064,6 +1119,8 @@ int upload_plan(lsg_operator* op) {
     P.b_items = op->b_items.as<lsg::PhaseBItem>();
     P.b_steps = op->b_steps.as<lsg::PhaseBStep>();
     P.pts = op->pts.as<int32_t>();
+    P.a_chain_off = op->a_chain_off.as<int32_t>();
+    P.a_chain_items = op->a_chain_items.as<int32_t>();
     P.sp_slot_off = op->sp_slot_off.as<int64_t>();
     P.sp_inc_base = op->sp_inc_base.as<int64_t>();
     P.sp_inc_off = op->sp_inc_off.as<int64_t>();
@@ -1162,8 +1219,8 @@ int set_phaseB_smem() {
     return 0;
 }
 
-// Phase B: the cell operator (k_sf per work-space class, k_cells per sparse
-// size class), then one k_level per restriction wavefront and the gather into y.
+// Phase B: the cell operator (k_cells per sparse size class, k_sf per
+// work-space class), one k_level per restriction wavefront, the gather into y.
 template <int D, typename V>
 int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* conv, V* sp, V* y, const V* acell,
                   const V* lam, cudaStream_t st, cudaEvent_t ev_cells = nullptr) {
@@ -1171,18 +1228,7 @@ int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* co
     constexpr bool F32 = std::is_same<V, float>::value;
     const lsg_operator::SfPrec& S = F32 ? op->sf32 : op->sf64;
     const V* coll = F32 ? (const V*)op->coll32.p : (const V*)op->coll64.p;
-    for (size_t c = 0; c + 1 < S.class_off.size(); ++c) {
-        int32_t b = S.class_off[c], e = S.class_off[c + 1];
-        size_t smem = (size_t)S.class_w[c] * sizeof(V);
-        if (F32)
-            k_sf<float, 7><<<e - b, op->tune.cell_threads, smem, st>>>(
-                op->b_items.as<lsg::PhaseBItem>(), S.plans.as<lsg::SfSlab>(), (const float*)pc, (float*)zb,
-                (const float*)coll, S.order.as<int32_t>(), b, op->unit_coef ? 1 : 0, op->form);
-        else
-            k_sf<double, 3><<<e - b, op->tune.cell_threads, smem, st>>>(
-                op->b_items.as<lsg::PhaseBItem>(), S.plans.as<lsg::SfSlab>(), (const double*)pc, (double*)zb,
-                (const double*)coll, S.order.as<int32_t>(), b, op->unit_coef ? 1 : 0, op->form);
-    }
+    // the cell operator: sparse slabs (few, small), then k_sf per work-space class
     const int64_t cap_elems = (200 * 1024) / sizeof(V) - (1 << D);
     for (size_t c = 0; c + 1 < S.cell_class_off.size(); ++c) {
         int32_t b = S.cell_class_off[c], e = S.cell_class_off[c + 1];
@@ -1192,15 +1238,26 @@ int phaseB_launch(lsg_operator* op, const V* pc, V* zb, V* gm, V* scratch, V* co
         k_cells<D, V><<<e - b, op->tune.cell_threads, smem, st>>>(op->dp, pc, zb, acell, lam,
                                                                   S.cell_order.as<int32_t>(), b, alloc, sp);
     }
+    for (size_t c = 0; c + 1 < S.class_off.size(); ++c) {
+        int32_t b = S.class_off[c], e = S.class_off[c + 1];
+        size_t smem = (size_t)S.class_w[c];
+        if (F32)
+            k_sf<float, 7><<<e - b, op->tune.cell_threads, smem, st>>>(
+                op->b_items.as<lsg::PhaseBItem>(), S.plans.as<lsg::SfSlab>(), (const float*)pc, (float*)zb,
+                (const float*)coll, S.order.as<int32_t>(), b, op->unit_coef ? 1 : 0, op->form);
+        else
+            k_sf<double, 3><<<e - b, op->tune.cell_threads, smem, st>>>(
+                op->b_items.as<lsg::PhaseBItem>(), S.plans.as<lsg::SfSlab>(), (const double*)pc, (double*)zb,
+                (const double*)coll, S.order.as<int32_t>(), b, op->unit_coef ? 1 : 0, op->form);
+    }
     if (ev_cells) cudaEventRecord(ev_cells, st);
-    // elements per ping-pong buffer (two buffers within the 220 KB opt-in)
+    // restriction wavefronts, then every active entry of y from the convert slots
     const int64_t lvl_cap = std::min<int64_t>(op->tune.level_cap, (110 * 1024) / sizeof(V));
     for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) {
         int32_t b = p.b_level_off[L], e = p.b_level_off[L + 1];
         if (e <= b) continue;
         int64_t bufn = std::min<int64_t>(op->level_need[L], lvl_cap);
-        k_level<D, V><<<e - b, op->tune.level_threads, 2 * bufn * sizeof(V), st>>>(op->dp, zb, gm, scratch, conv, b,
-                                                                                    bufn);
+        k_level<D, V><<<e - b, op->tune.level_threads, 2 * bufn * sizeof(V), st>>>(op->dp, zb, gm, scratch, conv, b, bufn);
     }
     int64_t na = p.exa_off[p.nD];
     if (na > 0) k_conv_gather<V><<<nblk(na), 256, 0, st>>>(op->dp, na, conv, y);
@@ -1226,8 +1283,8 @@ int matvec_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, cudaEvent_t
     int32_t nb = (int32_t)p.b_items.size();
     if (nb > 0) k_pinit<V><<<nb, 256, 0, st>>>(op->dp, w.ml.as<V>(), w.pc.as<V>(), 0);
     if (ev) cudaEventRecord(ev[2], st);
-    for (size_t L = 0; L + 1 < p.a_level_off.size(); ++L) {
-        int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
+    for (int k = 0; k < p.d; ++k) {
+        int32_t b = op->a_dim_chain_off[k], e = op->a_dim_chain_off[k + 1];
         if (e > b) k_prolong<V><<<e - b, op->tune.prolong_threads, 0, st>>>(op->dp, w.pc.as<V>(), b);
     }
     if (ev) cudaEventRecord(ev[3], st);
@@ -1398,11 +1455,16 @@ int jacobi_diag(lsg_operator* op, cudaStream_t st, const double** diag) {
 bool has_coefficient(const lsg_operator* op) { return op->have_coef; }
 const lsg::Plan& plan(const lsg_operator* op) { return op->plan; }
 size_t device_bytes(const lsg_operator* op) { return op->dev_bytes; }
-int64_t matvec_launch_count(const lsg_operator* op) {
+int64_t matvec_launch_count(const lsg_operator* op, bool f32) {
     const lsg::Plan& p = op->plan;
-    return 3 + (int64_t)(p.a_level_off.size() - 1) + (int64_t)op->sf32.class_off.size() - 1 +
-           (int64_t)op->sf32.cell_class_off.size() - 1 +
-           (int64_t)(p.b_level_off.size() - 1);
+    const lsg_operator::SfPrec& S = f32 ? op->sf32 : op->sf64;
+    int64_t prol = 0;
+    for (int k = 0; k < p.d; ++k) prol += op->a_dim_chain_off[k + 1] > op->a_dim_chain_off[k];
+    int64_t lv = 0;
+    for (size_t L = 0; L + 1 < p.b_level_off.size(); ++L) lv += p.b_level_off[L + 1] > p.b_level_off[L];
+    // nodal, P init, prolongation, cell operator (k_sf classes, k_cells classes), wavefronts, gather
+    return 2 + prol + (int64_t)S.class_off.size() - 1 + (int64_t)S.cell_class_off.size() - 1 + lv +
+           (p.exa_off[p.nD] > 0 ? 1 : 0);
 }
 int fail_msg(int code, const char* msg) { return fail(code, msg); }
 
@@ -1502,11 +1564,11 @@ int lsg_matvec_device(lsg_operator* op, const void* x, void* y, int32_t precisio
     return fail(LSG_E_INVALID, "precision must be LSG_FP64 or LSG_FP32");
 }
 
+// Kernel launches of one matvec in the given precision.
+static int64_t matvec_launches(const lsg_operator* op, bool f32) { return lsg_internal::matvec_launch_count(op, f32); }
+
 // Algorithmic bytes per phase of one matvec (value size sv): every array the
 // phase must touch, counted once per item that touches it.
-static int64_t matvec_launches(const lsg::Plan& p) {
-    return 3 + (int64_t)(p.a_level_off.size() - 1) + (int64_t)(p.b_level_off.size() - 1);
-}
 
 static void phase_bytes(const lsg_operator* op, double sv, double* b) {
     const lsg::Plan& p = op->plan;
@@ -1997,7 +2059,7 @@ int cg_loop(Solver& S, V* x, V* r, V* g, V* d, V* h, const V* z, double eps, int
     }
     if (exec) cudaGraphExecDestroy(exec);
     *its = it;
-    *launches += (int64_t)it * (matvec_launches(S.op->plan) + 9 + (want_rr ? 2 : 0));
+    *launches += (int64_t)it * (matvec_launches(S.op, std::is_same<V, float>::value) + 9 + (want_rr ? 2 : 0));
     return rc;
 }
 
@@ -2159,7 +2221,7 @@ int solve_device(lsg_operator* op, const double* f, double* x, const lsg_solver_
             const double istep = inner_step_tol(itol, std::sqrt(eps * eps * ff / rr), slow_steps ? 0.1 : 0.5);
             rc = cg_loop<float>(S, e32, r32, S.g32.as<float>(), d32, h32, z32, 0.0, 1, istep * istep, inner,
                                 o->use_graph != 0, st, &its, &lrr, &R.kernel_launches, kInnerStallWindow);
-            R.kernel_launches += matvec_launches(op->plan) + 12;
+            R.kernel_launches += matvec_launches(op, true) + 12;
             if (rc) break;
             total += its;
             if (!std::isfinite(lrr) || !std::isfinite(S.pin.h[3])) {
@@ -2362,11 +2424,10 @@ extern "C" int lsg_operator_autotune(lsg_operator* op, int32_t precision, int32_
 }
 
 // ============================================================================= allocation-free matvec
-// Some callers cannot allocate device memory when they need a product: code
-// running while a CUDA graph is being captured (cudaMalloc is not permitted
-// during capture), host applications whose own allocator owns every byte of
-// the device and forbids foreign allocations, and latency-critical loops that
-// cannot afford the implicit synchronisation of cudaMalloc/cudaFree.  For them
+// Some callers cannot allocate device memory when they need a product: host
+// applications whose own allocator owns every byte of the device and forbids
+// foreign allocations, and latency-critical loops that cannot afford the
+// implicit synchronisation of cudaMalloc/cudaFree.  For them
 // lsg_matvec_device_noalloc takes its work space from one fixed array that is
 // part of the library image on every GPU that loads it.
 #define LSG_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
@@ -2433,8 +2494,8 @@ int matvec_noalloc_impl(lsg_operator* op, const V* x, V* y, cudaStream_t st, uns
     k_nodal<V><<<p.nD, 256, 0, st>>>(op->dp, x, ml, nscratch);
     int32_t nb = (int32_t)p.b_items.size();
     if (nb > 0) k_pinit<V><<<nb, 256, 0, st>>>(op->dp, ml, pc, 0);
-    for (size_t L = 0; L + 1 < p.a_level_off.size(); ++L) {
-        int32_t b = p.a_level_off[L], e = p.a_level_off[L + 1];
+    for (int k = 0; k < p.d; ++k) {
+        int32_t b = op->a_dim_chain_off[k], e = op->a_dim_chain_off[k + 1];
         if (e > b) k_prolong<V><<<e - b, op->tune.prolong_threads, 0, st>>>(op->dp, pc, b);
     }
     rc = phaseB_launch<D, V>(op, pc, zb, gm, scratch, conv, sp, y, acell, lam, st);

@@ -26,7 +26,7 @@ int jacobi_diag(lsg_operator* op, cudaStream_t st, const double** diag);
 bool has_coefficient(const lsg_operator* op);
 const lsg::Plan& plan(const lsg_operator* op);
 size_t device_bytes(const lsg_operator* op);
-int64_t matvec_launch_count(const lsg_operator* op);
+int64_t matvec_launch_count(const lsg_operator* op, bool f32);
 int fail_msg(int code, const char* msg);
 int autotune(lsg_operator* op, int32_t precision, int32_t reps);
 // y = A x with coefficient 1 in form 0 (stiffness) or 1 (mass), FP64

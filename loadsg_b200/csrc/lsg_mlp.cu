@@ -3,10 +3,14 @@
 // trained on the GPU by the kernels below (forward, backward, Adam).
 //
 // Work is organised in tiles of 64 rows: a CTA keeps the tile's inputs and all
-// hidden activations in shared memory, computes each layer as a small
-// row-tile x weight product, and in the backward pass forms the weight
-// gradients of the tile as activation^T x delta products, adding them to the
-// global gradient with one atomic per parameter per tile.
+// hidden activations in shared memory.  The three hidden layers run on the
+// tensor cores: mma.sync m16n8k16 with BF16 A (the layer input, rounded to
+// BF16) and BF16 B (the weights), FP32 accumulation, bias and ReLU in FP32; each
+// of the CTA's 8 warps owns a 16 x 32 block of the 64 x 64 layer output.  The
+// output layer (64 -> 1) and the backward pass run on the CUDA cores with the
+// same rounded activations; the backward pass forms the weight gradients of
+// the tile as activation^T x delta products, adding them to the global
+// gradient with one atomic per parameter per tile.
 //
 // Parameter layout (FP32 master copy, flat):
 //   W1[64][F] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64] b4[1]
@@ -52,7 +56,11 @@ struct Layout {
 __device__ __forceinline__ float softplus(float o) { return o > 20.f ? o : log1pf(expf(o)); }
 __device__ __forceinline__ float sigmoidf_(float o) { return 1.f / (1.f + expf(-o)); }
 
+constexpr int LDH = H + 8;  // BF16 row stride of 64-wide operands (conflict-free fragment loads)
+__host__ __device__ inline int ldx(int F) { return ((F + 15) / 16) * 16 + 8; }  // layer-1 input stride
+
 // shared-memory tile of the network's weights (BF16 values widened to FP32)
+// and, for the tensor cores, BF16 copies of the weights and layer inputs
 struct Smem {
     float* W1;  // H*F
     float* W2;  // H*H
@@ -64,6 +72,12 @@ struct Smem {
     float* A2;
     float* A3;
     float* o;   // TR
+    __nv_bfloat16* W1b;  // H x ldx(F), zero padded
+    __nv_bfloat16* W2b;  // H x LDH
+    __nv_bfloat16* W3b;
+    __nv_bfloat16* Xb;   // TR x ldx(F), zero padded
+    __nv_bfloat16* A1b;  // TR x LDH
+    __nv_bfloat16* A2b;
 };
 
 __device__ Smem carve(float* base, int F) {
@@ -78,18 +92,35 @@ __device__ Smem carve(float* base, int F) {
     s.A2 = s.A1 + TR * H;
     s.A3 = s.A2 + TR * H;
     s.o = s.A3 + TR * H;
+    s.W1b = reinterpret_cast<__nv_bfloat16*>(s.o + TR);
+    s.W2b = s.W1b + H * ldx(F);
+    s.W3b = s.W2b + H * LDH;
+    s.Xb = s.W3b + H * LDH;
+    s.A1b = s.Xb + TR * ldx(F);
+    s.A2b = s.A1b + TR * LDH;
     return s;
 }
 
-size_t smem_bytes(int F) { return sizeof(float) * ((size_t)H * F + 2 * H * H + H + 3 * H + 1 + TR * F + 3 * TR * H + TR); }
+size_t smem_bytes(int F) {
+    return sizeof(float) * ((size_t)H * F + 2 * H * H + H + 3 * H + 1 + TR * F + 3 * TR * H + TR) +
+           sizeof(__nv_bfloat16) * ((size_t)(H + TR) * ldx(F) + (size_t)(2 * H + 2 * TR) * LDH);
+}
 
 __device__ void load_weights(const __nv_bfloat16* wb, const float* p, Smem& s, int F) {
     Layout L(F);
+    const int lx = ldx(F);
     for (int i = threadIdx.x; i < H * F; i += blockDim.x) s.W1[i] = __bfloat162float(wb[L.w1 + i]);
+    for (int i = threadIdx.x; i < H * lx; i += blockDim.x) {
+        int o = i / lx, k = i % lx;
+        s.W1b[i] = k < F ? wb[L.w1 + o * F + k] : __float2bfloat16_rn(0.f);
+    }
     for (int i = threadIdx.x; i < H * H; i += blockDim.x) {
         s.W2[i] = __bfloat162float(wb[L.w2 + i]);
         s.W3[i] = __bfloat162float(wb[L.w3 + i]);
+        s.W2b[(i / H) * LDH + i % H] = wb[L.w2 + i];
+        s.W3b[(i / H) * LDH + i % H] = wb[L.w3 + i];
     }
+    for (int i = threadIdx.x; i < TR * lx; i += blockDim.x) s.Xb[i] = __float2bfloat16_rn(0.f);  // K padding
     for (int i = threadIdx.x; i < H; i += blockDim.x) {
         s.W4[i] = __bfloat162float(wb[L.w4 + i]);
         s.b[i] = p[L.b1 + i];
@@ -99,29 +130,75 @@ __device__ void load_weights(const __nv_bfloat16* wb, const float* p, Smem& s, i
     if (threadIdx.x == 0) s.b[3 * H] = p[L.b4];
 }
 
-// A[r][o] = relu(b[o] + sum_i W[o][i] In[r][i]) for r < TR, o < H
-__device__ void layer(const float* In, int nin, const float* W, const float* bias, float* A) {
-    for (int e = threadIdx.x; e < TR * H; e += blockDim.x) {
-        int r = e / H, o = e % H;
-        float acc = bias[o];
-        const float* in = In + r * nin;
-        const float* w = W + o * nin;
-        for (int i = 0; i < nin; ++i) acc = fmaf(w[i], in[i], acc);
-        A[e] = acc > 0.f ? acc : 0.f;
+// D += A * B for one m16n8k16 tile: A 16 x 16 BF16 (row), B 16 x 8 BF16 (col), D FP32
+__device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// One hidden layer on the tensor cores: A[r][o] = relu(b[o] + sum_k W[o][k] In[r][k])
+// for r < TR, o < H, K a multiple of 16 (In, W BF16 with row strides ldi, ldw).
+// Warp w computes rows 16 (w & 3) .. +15 and columns 32 (w >> 2) .. +31.
+// Af receives the result (rounded to BF16 when Ab is given, the next layer's
+// input, so that Af holds exactly what that layer reads); Ab its BF16 copy.
+__device__ void layer_tc(const __nv_bfloat16* In, int ldi, int K, const __nv_bfloat16* W, int ldw, const float* bias,
+                         float* Af, __nv_bfloat16* Ab) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int r0 = (warp & 3) * 16, c0 = (warp >> 2) * 32;
+    float acc[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[j][q] = 0.f;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        uint32_t a[4];
+        a[0] = *reinterpret_cast<const uint32_t*>(In + (r0 + g) * ldi + k0 + 2 * t);
+        a[1] = *reinterpret_cast<const uint32_t*>(In + (r0 + g + 8) * ldi + k0 + 2 * t);
+        a[2] = *reinterpret_cast<const uint32_t*>(In + (r0 + g) * ldi + k0 + 2 * t + 8);
+        a[3] = *reinterpret_cast<const uint32_t*>(In + (r0 + g + 8) * ldi + k0 + 2 * t + 8);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = c0 + 8 * j + g;
+            uint32_t b[2];
+            b[0] = *reinterpret_cast<const uint32_t*>(W + n * ldw + k0 + 2 * t);
+            b[1] = *reinterpret_cast<const uint32_t*>(W + n * ldw + k0 + 2 * t + 8);
+            mma_bf16(acc[j], a, b);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int col = c0 + 8 * j + 2 * t;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = r0 + g + (q >= 2 ? 8 : 0), c = col + (q & 1);
+            float v = acc[j][q] + bias[c];
+            v = v > 0.f ? v : 0.f;
+            if (Ab) {
+                __nv_bfloat16 vb = __float2bfloat16_rn(v);
+                Ab[r * LDH + c] = vb;
+                v = __bfloat162float(vb);
+            }
+            Af[r * H + c] = v;
+        }
     }
 }
 
 __device__ void forward_tile(const float* __restrict__ X, int64_t row0, int64_t rows, Smem& s, int F) {
+    const int lx = ldx(F);
     for (int e = threadIdx.x; e < TR * F; e += blockDim.x) {
         int64_t r = row0 + e / F;
-        s.X[e] = r < rows ? X[r * F + e % F] : 0.f;
+        __nv_bfloat16 vb = __float2bfloat16_rn(r < rows ? X[r * F + e % F] : 0.f);
+        s.Xb[(e / F) * lx + e % F] = vb;
+        s.X[e] = __bfloat162float(vb);  // the layer-1 input as the tensor cores see it
     }
     __syncthreads();
-    layer(s.X, F, s.W1, s.b, s.A1);
+    layer_tc(s.Xb, lx, ((F + 15) / 16) * 16, s.W1b, lx, s.b, s.A1, s.A1b);
     __syncthreads();
-    layer(s.A1, H, s.W2, s.b + H, s.A2);
+    layer_tc(s.A1b, LDH, H, s.W2b, LDH, s.b + H, s.A2, s.A2b);
     __syncthreads();
-    layer(s.A2, H, s.W3, s.b + 2 * H, s.A3);
+    layer_tc(s.A2b, LDH, H, s.W3b, LDH, s.b + 2 * H, s.A3, nullptr);
     __syncthreads();
     for (int r = threadIdx.x; r < TR; r += blockDim.x) {
         float acc = s.b[3 * H];

@@ -42,11 +42,18 @@
 // output is written by one thread per stage, and the chunk loop adds into z in
 // a fixed order.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <string>
 #include <vector>
 
 #include "lsg_plan.h"
+
+#ifdef __CUDACC__
+#define LSG_SF_HD __host__ __device__
+#else
+#define LSG_SF_HD
+#endif
 
 namespace lsg {
 
@@ -85,6 +92,15 @@ struct SfSlab {
     int32_t na_max = 0;       // largest a extent this plan was made for
     int32_t pad = 0;
 };
+
+// Dynamic shared memory of the k_sf CTA of one slab: the work space, then the
+// chunk's 2^nq signed blocks (int64 offsets, then signs of the value size).
+inline LSG_SF_HD size_t sf_comb_offset(const SfSlab& D, size_t value_bytes) {
+    return ((size_t)(D.wtotal > 0 ? D.wtotal : 1) * value_bytes + 15) & ~(size_t)15;
+}
+inline LSG_SF_HD size_t sf_smem_bytes(const SfSlab& D, size_t value_bytes) {
+    return sf_comb_offset(D, value_bytes) + ((size_t)1 << D.nq) * (8 + value_bytes);
+}
 
 // Collapsed-coefficient layout of every dense slab: for slab t, the cells of its
 // non-collapsed dimensions (extents n_k + 1, dim 0 fastest) from coef_off[t];

@@ -15,7 +15,6 @@
 
 namespace lsg_sfk {
 
-constexpr int kMaxComb = 256;  // 2^nq signed blocks of one chunk (nq <= 8)
 
 template <typename V>
 __device__ __forceinline__ V pow2(int e);
@@ -199,8 +198,8 @@ __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M
         for (int i = 0; i < NX - 1; ++i) acc.pm[i] = mk2(c[i + 1] * lP * Fp.pm[i].x, c[i + 1] * lM * Fp.pm[i].y);
         for (int jb = 1; jb < nb; ++jb) {
             load(jb);
-            fwd_x<V, NX>(X, Fc);
-            coefs(jb);  // interior b cell jb between rows jb-1 and jb
+            coefs(jb);
+            fwd_x<V, NX>(X, Fc);  // interior b cell jb between rows jb-1 and jb
             // per a mode: b modes P = Fp + Fc, M = Fp - Fc, scaled; row jb-1
             // gets P' + M' (complete), row jb starts with P' - M'
             ModesX<V, NX> out;
@@ -225,7 +224,7 @@ __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M
             bwd_x<V, NX>(out, Y);
             store(jb - 1);
         }
-        coefs(nb);  // right boundary b cell: row nb-1 only
+        coefs(nb);  // right boundary b cell nb: row nb-1 only
         acc.bl += c[0] * lB * Fp.bl;
         acc.br += c[NX] * lB * Fp.br;
 #pragma unroll
@@ -247,8 +246,6 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
     using namespace lsg_sfk;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(16) unsigned char draw[sizeof(lsg::SfSlab)];
-    __shared__ int64_t s_off[kMaxComb];
-    __shared__ V s_sgn[kMaxComb];
     __shared__ int s_ncomb;
     __shared__ V s_cS, s_cM;
     __shared__ int64_t s_cbase;
@@ -266,6 +263,9 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
     const V unit_v = V(D.unit_sum);
     V* Wl = reinterpret_cast<V*>(smem_raw);
     V* Wh = Wl + D.hi_off;
+    // the chunk's signed blocks (2^nq of them) after the work space
+    int64_t* s_off = reinterpret_cast<int64_t*>(smem_raw + lsg::sf_comb_offset(D, sizeof(V)));
+    V* s_sgn = reinterpret_cast<V*>(s_off + (1 << D.nq));
     const int nm = D.nm, nq = D.nq;
     auto region = [&](int k) { return ((nm - k) & 1) ? Wh : Wl; };
     const int tid = threadIdx.x, T = blockDim.x;
@@ -330,6 +330,7 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
         };
         {  // gather the slice into stage 0
             V* s0 = region(0);
+#pragma unroll 4
             for (int e = tid; e < D.slice; e += T) s0[e] = gath((uint32_t)e);
         }
         __syncthreads();
@@ -404,6 +405,7 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
         }
         {  // scatter stage 0 into z
             const V* s0 = region(0);
+#pragma unroll 4
             for (int e = tid; e < D.slice; e += T) scat((uint32_t)e, s0[e]);
         }
         __syncthreads();

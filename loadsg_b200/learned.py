@@ -170,8 +170,20 @@ def expsin_problem(d, seed, sigma=0.3):
     return MidpointDiffusion(COEF_EXPSIN, rng.normal(0.0, sigma, d))
 
 
+_GRIDS = {}
+
+
+def corner_grid(d, level, refine):
+    """The corner-refined grid of an instance; instances differ only in their
+    coefficient, so one grid per (d, level, refine) serves them all."""
+    key = (d, level, refine)
+    if key not in _GRIDS:
+        _GRIDS[key] = AdaptiveSparseGrid.adaptive(d, level, refine, 0.6, "corner")
+    return _GRIDS[key]
+
+
 def make_instance(d, level, refine, seed, family="lognormal"):
-    g = AdaptiveSparseGrid.adaptive(d, level, refine, 0.6, "corner")
+    g = corner_grid(d, level, refine)
     prob = lognormal_problem(d, seed) if family == "lognormal" else expsin_problem(d, seed)
     return g, prob, MatrixVectorHomogen(g, prob)
 

@@ -3,8 +3,10 @@
 Same layout and loss as loadsg_b200/csrc/lsg_mlp.cu: W1[64][F] b1 W2[64][64] b2
 W3[64][64] b3 W4[64] b4, ReLU hidden layers, loss mean_r (log softplus(o_r) -
 y_r)^2.  Weights are rounded to BF16 (round to nearest even) as the CUDA
-forward/backward passes use them; biases stay FP32.  Used to check the CUDA
-gradients."""
+forward/backward passes use them, and so are the inputs of the three hidden
+layers (the tensor cores multiply BF16 by BF16: the features X and the
+activations a1, a2); biases, a3 and the output layer stay in floating point.
+Used to check the CUDA forward pass and gradients."""
 import numpy as np
 
 H = 64
@@ -39,9 +41,9 @@ def unpack(p, F):
 def forward(p, X):
     F = X.shape[1]
     W1, b1, W2, b2, W3, b3, W4, b4 = unpack(p, F)
-    X = X.astype(np.float64)
-    a1 = np.maximum(X @ W1.T + b1, 0)
-    a2 = np.maximum(a1 @ W2.T + b2, 0)
+    X = bf16_round(X).astype(np.float64)
+    a1 = bf16_round(np.maximum(X @ W1.T + b1, 0)).astype(np.float64)
+    a2 = bf16_round(np.maximum(a1 @ W2.T + b2, 0)).astype(np.float64)
     a3 = np.maximum(a2 @ W3.T + b3, 0)
     return a3 @ W4 + b4, (X, a1, a2, a3)
 

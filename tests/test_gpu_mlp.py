@@ -24,11 +24,18 @@ def test_forward_and_gradient_match_fp64_reference():
     Yd = torch.tensor(Y, device="cuda")
     o = net.forward(Xd).cpu().numpy()
     o_ref, _ = mlp_ref.forward(p, X)
-    assert np.abs(o - o_ref).max() <= 1e-4 * (1 + np.abs(o_ref).max())
+    # The hidden layers multiply BF16 by BF16 on the tensor cores with FP32
+    # accumulation; the reference rounds at the same points but accumulates in
+    # FP64, so an activation whose FP32 and FP64 values straddle a BF16 rounding
+    # boundary differs by one BF16 unit (2^-8 relative): BF16-level tolerances.
+    assert np.abs(o - o_ref).max() <= 3e-3 * (1 + np.abs(o_ref).max())
     loss, g = net.gradient(Xd, Yd)
     loss_ref, g_ref = mlp_ref.loss_and_grad(p, X, Y)
-    assert abs(loss - loss_ref) <= 1e-4 * abs(loss_ref)
-    assert np.abs(g - g_ref).max() <= 1e-3 * np.abs(g_ref).max()
+    assert abs(loss - loss_ref) <= 3e-3 * abs(loss_ref)
+    assert np.abs(g - g_ref).max() <= 1e-2 * np.abs(g_ref).max()
+    # and far below what an FP32-activation forward would leave: the rounding
+    # points are the reference's
+    assert np.median(np.abs(o - o_ref)) <= 1e-3 * (1 + np.abs(o_ref).max())
 
 
 def test_training_reduces_loss():
