@@ -330,7 +330,6 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
         };
         {  // gather the slice into stage 0
             V* s0 = region(0);
-#pragma unroll 4
             for (int e = tid; e < D.slice; e += T) s0[e] = gath((uint32_t)e);
         }
         __syncthreads();
@@ -405,7 +404,6 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
         }
         {  // scatter stage 0 into z
             const V* s0 = region(0);
-#pragma unroll 4
             for (int e = tid; e < D.slice; e += T) scat((uint32_t)e, s0[e]);
         }
         __syncthreads();

@@ -117,14 +117,15 @@ def test_dropin_header_compiles_and_links(tmp_path):
 
 @pytest.mark.gpu
 def test_dropin_solves_on_gpu(tmp_path):
-    """A d=3 level-5 solve through the header: relative residual below 1e-8,
+    """A d=3 level-5 solve (1,023 points, the reference's level numbering as in
+    its Poisson example's table) through the header: relative residual below 1e-8,
     transform round trip 1e-10, boundary forms of g = 1 (gradient form 0, root
     mass 1/8)."""
     exe = build_example(tmp_path)
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     f = dict(kv.split("=") for kv in r.stdout.split() if "=" in kv)
-    assert int(f["N"]) == 351
+    assert int(f["N"]) == 1023
     assert 0 < int(f["iterations"]) <= 100
     assert float(f["relres"]) < 1e-8
     nums = r.stdout.split()

@@ -44,11 +44,16 @@ def test_single_process_value_passes_through():
 
 
 def test_each_rank_solves_its_own_instance():
-    g0, fam0, p0, f0, _ = bench.workload("d3_regular_L7", 0)
-    g1, fam1, p1, f1, _ = bench.workload("d3_regular_L7", 1)
+    # the seeded synthetic workloads (the d = 3 level-7 case is the reference's
+    # fixed instance, the same on every rank, and is not one of them)
+    g0, fam0, p0, f0, _ = bench.workload("d6_regular_L3", 0)
+    g1, fam1, p1, f1, _ = bench.workload("d6_regular_L3", 1)
     assert g0.n == g1.n and fam0 == fam1  # same size per GPU: weak scaling
     assert not np.array_equal(f0, f1)     # independent right-hand sides
     assert not np.any(f0[g0.active == 0])
+    ga, _, _, fa, _ = bench.workload("d3_regular_L7", 0)
+    gb, _, _, fb, _ = bench.workload("d3_regular_L7", 1)
+    assert ga.n == 7423 and np.array_equal(fa, fb)
 
 
 def test_reference_arm_runs_on_rank_zero_only():
