@@ -93,13 +93,14 @@ struct SfSlab {
     int32_t pad = 0;
 };
 
-// Dynamic shared memory of the k_sf CTA of one slab: the work space, then the
-// chunk's 2^nq signed blocks (int64 offsets, then signs of the value size).
+// Dynamic shared memory of the k_sf CTA of one slab: the work space, then two
+// buffers (this chunk's and the next one's) of the chunk's 2^nq signed blocks:
+// int64 offsets of both buffers, then signs of the value size of both.
 inline LSG_SF_HD size_t sf_comb_offset(const SfSlab& D, size_t value_bytes) {
     return ((size_t)(D.wtotal > 0 ? D.wtotal : 1) * value_bytes + 15) & ~(size_t)15;
 }
 inline LSG_SF_HD size_t sf_smem_bytes(const SfSlab& D, size_t value_bytes) {
-    return sf_comb_offset(D, value_bytes) + ((size_t)1 << D.nq) * (8 + value_bytes);
+    return sf_comb_offset(D, value_bytes) + 2 * ((size_t)1 << D.nq) * (8 + value_bytes);
 }
 
 // Collapsed-coefficient layout of every dense slab: for slab t, the cells of its

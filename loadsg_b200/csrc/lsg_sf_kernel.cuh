@@ -15,6 +15,9 @@
 
 namespace lsg_sfk {
 
+// elements per thread in flight in the gather and scatter of a chunk
+constexpr int kGS = 4;
+
 
 template <typename V>
 __device__ __forceinline__ V pow2(int e);
@@ -246,9 +249,9 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
     using namespace lsg_sfk;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(16) unsigned char draw[sizeof(lsg::SfSlab)];
-    __shared__ int s_ncomb;
-    __shared__ V s_cS, s_cM;
-    __shared__ int64_t s_cbase;
+    __shared__ int s_ncomb[2];
+    __shared__ V s_cS[2], s_cM[2];
+    __shared__ int64_t s_cbase[2];
     const lsg::PhaseBItem it = items[order[ord0 + blockIdx.x]];
     {
         const int* src = reinterpret_cast<const int*>(sf + it.t);
@@ -263,74 +266,94 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
     const V unit_v = V(D.unit_sum);
     V* Wl = reinterpret_cast<V*>(smem_raw);
     V* Wh = Wl + D.hi_off;
-    // the chunk's signed blocks (2^nq of them) after the work space
-    int64_t* s_off = reinterpret_cast<int64_t*>(smem_raw + lsg::sf_comb_offset(D, sizeof(V)));
-    V* s_sgn = reinterpret_cast<V*>(s_off + (1 << D.nq));
     const int nm = D.nm, nq = D.nq;
+    // the signed blocks (2^nq of them) of this chunk and the next one, after the
+    // work space: offsets of buffer 0 and 1, then signs of buffer 0 and 1
+    const int ncmax = 1 << nq;
+    int64_t* s_off0 = reinterpret_cast<int64_t*>(smem_raw + lsg::sf_comb_offset(D, sizeof(V)));
+    V* s_sgn0 = reinterpret_cast<V*>(s_off0 + 2 * ncmax);
     auto region = [&](int k) { return ((nm - k) & 1) ? Wh : Wl; };
     const int tid = threadIdx.x, T = blockDim.x;
+    // chunk tuple -> signed blocks, (S, M) and coefficient offset, into buffer bf
+    // (one thread)
+    auto combos = [&](int ch, int bf) {
+        int64_t* so = s_off0 + bf * ncmax;
+        V* sg = s_sgn0 + bf * ncmax;
+        V cS = V(D.S0), cM = V(D.M0);
+        int64_t cbase = 0;
+        int ncomb = 1;
+        so[0] = 0;
+        sg[0] = V(1);
+        int rem = ch;
+        for (int i = 0; i < nq; ++i) {
+            const lsg::SfDim& x = D.q[i];
+            int r = rem % (2 * x.n);
+            rem /= 2 * x.n;
+            int cell, type;
+            mode_of(x.n, r, cell, type);
+            combine<V>(cS, cM, x.T, type);
+            cbase += (int64_t)cell * x.cstride;
+            if (type == 2) {
+                int j = r == 0 ? 1 : x.n;
+                for (int c = 0; c < ncomb; ++c) so[c] += (int64_t)(j - 1) * x.pstride;
+            } else {
+                V sv = type == 0 ? V(1) : V(-1);
+                for (int c = 0; c < ncomb; ++c) {
+                    so[ncomb + c] = so[c] + (int64_t)cell * x.pstride;  // node cell + 1
+                    sg[ncomb + c] = sg[c] * sv;
+                    so[c] += (int64_t)(cell - 1) * x.pstride;           // node cell
+                }
+                ncomb *= 2;
+            }
+        }
+        s_ncomb[bf] = ncomb;
+        s_cS[bf] = cS;
+        s_cM[bf] = cM;
+        s_cbase[bf] = cbase;
+    };
     if (nq > 0) {
         int64_t N = D.slice;
         for (int i = 0; i < nq; ++i) N *= D.q[i].n;
         for (int64_t e = tid; e < N; e += T) z[e] = V(0);
     }
+    if (tid == T - 1) combos(0, 0);
+    __syncthreads();
     for (int ch = 0; ch < D.nchunk; ++ch) {
-        if (tid == 0) {  // chunk tuple -> signed blocks, (S, M) and coefficient offset
-            V cS = V(D.S0), cM = V(D.M0);
-            int64_t cbase = 0;
-            int ncomb = 1;
-            s_off[0] = 0;
-            s_sgn[0] = V(1);
-            int rem = ch;
-            for (int i = 0; i < nq; ++i) {
-                const lsg::SfDim& x = D.q[i];
-                int r = rem % (2 * x.n);
-                rem /= 2 * x.n;
-                int cell, type;
-                mode_of(x.n, r, cell, type);
-                combine<V>(cS, cM, x.T, type);
-                cbase += (int64_t)cell * x.cstride;
-                if (type == 2) {
-                    int j = r == 0 ? 1 : x.n;
-                    for (int c = 0; c < ncomb; ++c) s_off[c] += (int64_t)(j - 1) * x.pstride;
-                } else {
-                    V sg = type == 0 ? V(1) : V(-1);
-                    for (int c = 0; c < ncomb; ++c) {
-                        s_off[ncomb + c] = s_off[c] + (int64_t)cell * x.pstride;  // node cell + 1
-                        s_sgn[ncomb + c] = s_sgn[c] * sg;
-                        s_off[c] += (int64_t)(cell - 1) * x.pstride;              // node cell
-                    }
-                    ncomb *= 2;
-                }
-            }
-            s_ncomb = ncomb;
-            s_cS = cS;
-            s_cM = cM;
-            s_cbase = cbase;
-        }
-        __syncthreads();
-        const int ncomb = s_ncomb;
+        const int bf = ch & 1;
+        const int ncomb = s_ncomb[bf];
+        const int64_t* s_off = s_off0 + bf * ncmax;
+        const V* s_sgn = s_sgn0 + bf * ncmax;
         // slice position -> u position: insert the chunked dimensions, outer to inner
         auto upos = [&](uint32_t x) {
             for (int i = nq - 1; i >= 0; --i) x += quot(D.qB[i], x) * (uint32_t)D.qmult[i];
             return (int64_t)x;
         };
-        // the slice of u for this chunk tuple at stage-0 position e, and its transpose into z
-        auto gath = [&](uint32_t e) {
-            const int64_t ue = upos(e);
-            V acc = V(0);
-            for (int c = 0; c < ncomb; ++c) acc += s_sgn[c] * u[s_off[c] + ue];
-            return acc;
-        };
-        auto scat = [&](uint32_t e, V v) {
-            const int64_t ue = upos(e);
-            if (nq == 0) z[ue] = v;
-            else
-                for (int c = 0; c < ncomb; ++c) z[s_off[c] + ue] += s_sgn[c] * v;
-        };
-        {  // gather the slice into stage 0
+        // gather the slice of u for this chunk tuple into stage 0: kGS elements
+        // per thread, all their loads issued before the sums
+        {
             V* s0 = region(0);
-            for (int e = tid; e < D.slice; e += T) s0[e] = gath((uint32_t)e);
+            for (int e0 = tid; e0 < D.slice; e0 += kGS * T) {
+                int64_t ue[kGS];
+                V acc[kGS];
+#pragma unroll
+                for (int k = 0; k < kGS; ++k) {
+                    const int e = e0 + k * T;
+                    ue[k] = e < D.slice ? upos((uint32_t)e) : -1;
+                    acc[k] = V(0);
+                }
+                for (int c = 0; c < ncomb; ++c) {
+                    const V sg = s_sgn[c];
+                    const V* uc = u + s_off[c];
+                    V x[kGS];
+#pragma unroll
+                    for (int k = 0; k < kGS; ++k) x[k] = ue[k] >= 0 ? uc[ue[k]] : V(0);
+#pragma unroll
+                    for (int k = 0; k < kGS; ++k) acc[k] += sg * x[k];
+                }
+#pragma unroll
+                for (int k = 0; k < kGS; ++k)
+                    if (ue[k] >= 0) s0[e0 + k * T] = acc[k];
+            }
         }
         __syncthreads();
         // mid sweeps, forward
@@ -361,8 +384,8 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
             V* F = region(nm);
             const int plane = D.a.n * D.b.n;
             for (int pl = tid; pl < D.npl; pl += T) {
-                V S = s_cS, M = s_cM;
-                int64_t cb = s_cbase;
+                V S = s_cS[bf], M = s_cM[bf];
+                int64_t cb = s_cbase[bf];
                 uint32_t r = (uint32_t)pl;
                 for (int k = 0; k < nm; ++k) {
                     const lsg::SfDim& x = D.mid[k];
@@ -402,10 +425,40 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
             }
             __syncthreads();
         }
-        {  // scatter stage 0 into z
+        // scatter stage 0 into z (its transpose of the gather), kGS elements per
+        // thread: per signed block all loads of z before the stores
+        {
             const V* s0 = region(0);
-            for (int e = tid; e < D.slice; e += T) scat((uint32_t)e, s0[e]);
+            for (int e0 = tid; e0 < D.slice; e0 += kGS * T) {
+                int64_t ue[kGS];
+                V v[kGS];
+#pragma unroll
+                for (int k = 0; k < kGS; ++k) {
+                    const int e = e0 + k * T;
+                    ue[k] = e < D.slice ? upos((uint32_t)e) : -1;
+                    v[k] = ue[k] >= 0 ? s0[e] : V(0);
+                }
+                if (nq == 0) {
+#pragma unroll
+                    for (int k = 0; k < kGS; ++k)
+                        if (ue[k] >= 0) z[ue[k]] = v[k];
+                } else {
+                    for (int c = 0; c < ncomb; ++c) {
+                        const V sg = s_sgn[c];
+                        V* zc = z + s_off[c];
+                        V old[kGS];
+#pragma unroll
+                        for (int k = 0; k < kGS; ++k) old[k] = ue[k] >= 0 ? zc[ue[k]] : V(0);
+#pragma unroll
+                        for (int k = 0; k < kGS; ++k)
+                            if (ue[k] >= 0) zc[ue[k]] = old[k] + sg * v[k];
+                    }
+                }
+            }
         }
+        // the next chunk's signed blocks into the other buffer (its last reader,
+        // chunk ch - 1, finished before the previous barrier)
+        if (tid == T - 1 && ch + 1 < D.nchunk) combos(ch + 1, bf ^ 1);
         __syncthreads();
     }
 }
