@@ -840,6 +840,7 @@ struct lsg_operator {
         std::vector<int32_t> class_off;    // k_sf launches (work-space classes)
         std::vector<int32_t> class_w;      // dynamic shared memory (bytes) of each launch
         std::vector<uint8_t> ok;  // per slab: the plan fits
+        DBuf cstr;                // per (slab, dim): coefficient stride in this precision's order
         DBuf cell_order;
         std::vector<int32_t> cell_class_off;
         std::vector<int64_t> cell_class_n;
@@ -904,17 +905,50 @@ int build_sf_prec(lsg_operator* op, lsg_operator::SfPrec& S, int64_t wcap, int n
         }
     }
     S.cell_class_off.push_back((int32_t)cord.size());
+    std::vector<int32_t> cstr((size_t)p.nD * p.d, 0);
+    for (int t = 0; t < p.nD; ++t)
+        if (S.ok[t]) lsg::sf_cell_strides(p, t, plans[t], cstr.data() + (size_t)t * p.d);
     int rc = S.plans.upload(plans, &op->dev_bytes);
+    if (!rc) rc = S.cstr.upload(cstr, &op->dev_bytes);
     if (!rc) rc = S.order.upload(ord, &op->dev_bytes);
     if (!rc) rc = S.cell_order.upload(cord, &op->dev_bytes);
     return rc ? LSG_E_CUDA : 0;
+}
+
+// Collapsed coefficients of one part's dense slabs (k_sf), in the order of the
+// current FP64 and FP32 plans.
+cudaError_t collapse_part(lsg_operator* op, int part) {
+    const lsg::Plan& p = op->plan;
+    int t_lo = p.inst_t_off[part], t_hi = p.inst_t_off[part + 1];
+    int64_t lo = -1, hi = -1;
+    for (int t = t_lo; t < t_hi; ++t) {
+        int64_t o = op->sf_layout.coef_off[t];
+        if (o < 0) continue;
+        if (lo < 0) lo = o;
+        int64_t c = 1;
+        for (int k = 0; k < p.d; ++k)
+            if (p.slabs[t].T[k] >= 2) c *= ((int64_t)1 << p.slabs[t].T[k]);
+        hi = o + c;
+    }
+    if (lo >= 0 && hi > lo)
+        k_sf_collapse<<<nblk(hi - lo), 256>>>(op->slab_T.as<int32_t>(), p.d, op->slab_cell_off.as<int64_t>(),
+                                               op->coll_off.as<int64_t>(), op->coll_slab.as<int32_t>(), lo, hi,
+                                               op->acell64.as<double>(), op->sf64.cstr.as<int32_t>(),
+                                               op->sf32.cstr.as<int32_t>(), op->coll64.as<double>(),
+                                               op->coll32.as<float>());
+    return cudaGetLastError();
 }
 
 int build_cell_classes(lsg_operator* op) {
     const int64_t w32 = (int64_t)op->tune.cell_space_kb * 1024 / 4, w64 = (int64_t)op->tune.cell_space_kb * 1024 / 8;
     int rc = build_sf_prec(op, op->sf32, w32, 7);
     if (!rc) rc = build_sf_prec(op, op->sf64, w64, 3);
-    return rc;
+    if (rc) return rc;
+    // new plans order the collapsed coefficients differently: redo the parts
+    // whose coefficients are set
+    for (size_t part = 0; part < op->part_coef.size(); ++part)
+        if (op->part_coef[part]) CUDA_TRY(collapse_part(op, (int)part));
+    return 0;
 }
 
 int upload_plan(lsg_operator* op) {
@@ -1412,25 +1446,7 @@ int set_part_coefficient(lsg_operator* op, int part, int32_t family, const doubl
                                                 pp, op->acell64.as<double>(), op->acell32.as<float>(),
                                                 op->cell_slab_off.as<int64_t>());
     CUDA_TRY(cudaGetLastError());
-    {  // collapsed coefficients of this part's dense slabs (k_sf)
-        int t_lo = p.inst_t_off[part], t_hi = p.inst_t_off[part + 1];
-        int64_t lo = -1, hi = -1;
-        for (int t = t_lo; t < t_hi; ++t) {
-            int64_t o = op->sf_layout.coef_off[t];
-            if (o < 0) continue;
-            if (lo < 0) lo = o;
-            int64_t c = 1;
-            for (int k = 0; k < p.d; ++k)
-                if (p.slabs[t].T[k] >= 2) c *= ((int64_t)1 << p.slabs[t].T[k]);
-            hi = o + c;
-        }
-        if (lo >= 0 && hi > lo)
-            k_sf_collapse<<<nblk(hi - lo), 256>>>(op->slab_T.as<int32_t>(), p.d, op->slab_cell_off.as<int64_t>(),
-                                                   op->coll_off.as<int64_t>(), op->coll_slab.as<int32_t>(), lo, hi,
-                                                   op->acell64.as<double>(), op->coll64.as<double>(),
-                                                   op->coll32.as<float>());
-        CUDA_TRY(cudaGetLastError());
-    }
+    CUDA_TRY(collapse_part(op, part));
     CUDA_TRY(cudaDeviceSynchronize());
     op->part_coef[part] = 1;
     op->have_coef = std::all_of(op->part_coef.begin(), op->part_coef.end(), [](uint8_t v) { return v != 0; });
@@ -1769,7 +1785,7 @@ int lsg_plan_check_slab_operator(const lsg_plan* p, int32_t t, int32_t form, int
     for (int k = 0; k < P.d; ++k)
         if (P.slabs[t].T[k] >= 2) cc *= ((int64_t)1 << P.slabs[t].T[k]);
     std::vector<double> coef(cc);
-    lsg::sf_collapse_host(P, t, acell, L, coef.data());
+    lsg::sf_collapse_host(P, t, D, acell, coef.data());
     lsg::sf_apply_host(D, form, coef.data(), u, z_sf);
     if (info) {
         int ncol = 0;

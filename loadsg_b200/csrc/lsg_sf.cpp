@@ -58,9 +58,10 @@ std::vector<SfSlab> sf_plan(const Plan& p, const SfCoefLayout& L, int64_t wcap, 
         D.na_max = na_max;
         if (!s.dense) { D.nm = D.nq = -1; continue; }
         D.coef_off = L.coef_off[t];
-        // non-collapsed dimensions, inner to outer, with their strides
+        // non-collapsed dimensions, inner to outer, with their position strides
+        // (coefficient strides are set once the roles are known)
         std::vector<SfDim> nc;
-        int64_t pst = 1, cst = 1;
+        int64_t pst = 1;
         double S = 0.0, M = 1.0, unit = 1.0;
         for (int k = 0; k < d; ++k) {
             int32_t n = (1 << s.T[k]) - 1;
@@ -76,12 +77,10 @@ std::vector<SfSlab> sf_plan(const Plan& p, const SfCoefLayout& L, int64_t wcap, 
             SfDim x;
             x.n = n;
             x.pstride = (int32_t)pst;
-            x.cstride = (int32_t)cst;
             x.T = s.T[k];
             x.div2n = sf_div((uint32_t)(2 * n));
             nc.push_back(x);
             pst *= n;
-            cst *= (n + 1);
         }
         D.S0 = S;
         D.M0 = M;
@@ -156,15 +155,41 @@ std::vector<SfSlab> sf_plan(const Plan& p, const SfCoefLayout& L, int64_t wcap, 
         }
         D.hi_off = D.stage[D.nm];
         D.wtotal = D.nm == 0 ? D.stage[0] : D.stage[D.nm] + D.stage[D.nm - 1];
+        // coefficient order of the slab: mid dimensions fastest, then a, b and
+        // the chunked dimensions (n + 1 cells each)
+        int32_t cs = 1;
+        for (int i = 0; i < D.nm; ++i) { D.mid[i].cstride = cs; cs *= D.mid[i].n + 1; }
+        if (D.a.T >= 0) { D.a.cstride = cs; cs *= D.a.n + 1; } else D.a.cstride = 0;
+        if (D.b.T >= 0) { D.b.cstride = cs; cs *= D.b.n + 1; } else D.b.cstride = 0;
+        for (int i = 0; i < D.nq; ++i) { D.q[i].cstride = cs; cs *= D.q[i].n + 1; }
     }
     return out;
 }
 
-void sf_collapse_host(const Plan& p, int t, const double* acell, const SfCoefLayout& L, double* coef) {
+void sf_cell_strides(const Plan& p, int t, const SfSlab& D, int32_t* by_dim) {
+    const Slab& s = p.slabs[t];
+    int64_t pst = 1;
+    for (int k = 0; k < p.d; ++k) {
+        by_dim[k] = 0;
+        const int32_t n = (1 << s.T[k]) - 1;
+        if (n == 1) continue;  // collapsed
+        auto match = [&](const SfDim& x) {
+            if (x.T >= 0 && x.pstride == pst) by_dim[k] = x.cstride;
+        };
+        match(D.a);
+        match(D.b);
+        for (int i = 0; i < D.nm; ++i) match(D.mid[i]);
+        for (int i = 0; i < D.nq; ++i) match(D.q[i]);
+        pst *= n;
+    }
+}
+
+void sf_collapse_host(const Plan& p, int t, const SfSlab& D, const double* acell, double* coef) {
     const Slab& s = p.slabs[t];
     const int d = p.d;
-    (void)L;
     int64_t cstr[kMaxDim], ext[kMaxDim];
+    int32_t ostr[kMaxDim];
+    sf_cell_strides(p, t, D, ostr);
     int64_t st = 1;
     for (int k = 0; k < d; ++k) { cstr[k] = st; ext[k] = (int64_t)1 << s.T[k]; st *= ext[k]; }
     std::vector<int> ncd, cd;
@@ -172,8 +197,13 @@ void sf_collapse_host(const Plan& p, int t, const double* acell, const SfCoefLay
     int64_t cnt = 1;
     for (int k : ncd) cnt *= ext[k];
     for (int64_t c = 0; c < cnt; ++c) {
-        int64_t r = c, base = 0;
-        for (int k : ncd) { base += (r % ext[k]) * cstr[k]; r /= ext[k]; }
+        int64_t r = c, base = 0, pos = 0;
+        for (int k : ncd) {
+            const int64_t ck = r % ext[k];
+            base += ck * cstr[k];
+            pos += ck * ostr[k];
+            r /= ext[k];
+        }
         double acc = 0.0;
         for (int b = 0; b < (1 << cd.size()); ++b) {  // collapsed cells in binary order
             int64_t key = base;
@@ -181,7 +211,7 @@ void sf_collapse_host(const Plan& p, int t, const double* acell, const SfCoefLay
                 if ((b >> i) & 1) key += cstr[cd[i]];
             acc += acell[key];
         }
-        coef[c] = acc;
+        coef[pos] = acc;
     }
 }
 

@@ -67,7 +67,7 @@ SfDiv sf_div(uint32_t d);
 struct SfDim {
     int32_t n = 1;        // interior nodes (1 for a virtual dimension)
     int32_t pstride = 0;  // slab-position stride
-    int32_t cstride = 0;  // stride in the slab's collapsed-coefficient array
+    int32_t cstride = 0;  // stride in the slab's collapsed-coefficient array (plan order)
     int32_t T = 0;        // depth (h = 2^-T); a virtual dimension has T = -1
     SfDiv div2n;          // division by 2n (decode of reduced-mode indices)
 };
@@ -104,8 +104,12 @@ inline LSG_SF_HD size_t sf_smem_bytes(const SfSlab& D, size_t value_bytes) {
 }
 
 // Collapsed-coefficient layout of every dense slab: for slab t, the cells of its
-// non-collapsed dimensions (extents n_k + 1, dim 0 fastest) from coef_off[t];
-// ccount = total.  Sparse slabs get no entries.
+// non-collapsed dimensions (extents n_k + 1) from coef_off[t]; ccount = total.
+// Sparse slabs get no entries.  The order of the dimensions inside a slab's
+// block is its plan's (sf_plan): the mid dimensions fastest (inner to outer),
+// then a, b and the chunked dimensions, so that the threads of a warp, which
+// take consecutive mid modes in the fused step, read neighbouring coefficients.
+// The FP32 and FP64 plans differ, and so do their coefficient arrays' orders.
 struct SfCoefLayout {
     std::vector<int64_t> coef_off;  // per slab
     int64_t ccount = 0;
@@ -118,7 +122,10 @@ std::vector<SfSlab> sf_plan(const Plan& p, const SfCoefLayout& L, int64_t wcap, 
 
 // Host emulation (tests): collapsed coefficients of one slab from per-cell
 // coefficients (slab cell order), and the factorised apply z = A_T u.
-void sf_collapse_host(const Plan& p, int t, const double* acell_slab, const SfCoefLayout& L, double* coef);
+// Coefficient stride of every slab dimension k in plan D's order (0 for a
+// collapsed dimension): by_dim[0 .. d-1].
+void sf_cell_strides(const Plan& p, int t, const SfSlab& D, int32_t* by_dim);
+void sf_collapse_host(const Plan& p, int t, const SfSlab& D, const double* acell_slab, double* coef);
 void sf_apply_host(const SfSlab& D, int form, const double* coef, const double* u, double* z);
 // Direct cell-by-cell apply of the same operator (corner pairs of every cell
 // with both corners in the slab), the reference's LocalStiffnessMatrices form.

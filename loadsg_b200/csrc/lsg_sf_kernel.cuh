@@ -465,23 +465,32 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
 
 // Collapsed coefficients of every dense slab: per non-collapsed cell the sum of
 // a over the collapsed dimensions' cells in binary order (FP64, rounded once
-// for FP32), for the collapsed cells [lo, hi); coll_slab: slab of each
-// collapsed cell, coll_off: first collapsed cell of each slab.
+// for FP32), for the collapsed cells [lo, hi) enumerated in slab-dimension
+// order; coll_slab: slab of each collapsed cell, coll_off: first collapsed cell
+// of each slab; str64 / str32: per (slab, dim) the coefficient stride of the
+// FP64 / FP32 plan, which place the value in that plan's order.
 __global__ void k_sf_collapse(const int32_t* __restrict__ slab_T, int d, const int64_t* __restrict__ cell_off,
                               const int64_t* __restrict__ coll_off, const int32_t* __restrict__ coll_slab, int64_t lo,
-                              int64_t hi, const double* __restrict__ acell, double* __restrict__ c64,
-                              float* __restrict__ c32) {
+                              int64_t hi, const double* __restrict__ acell, const int32_t* __restrict__ str64,
+                              const int32_t* __restrict__ str32, double* __restrict__ c64, float* __restrict__ c32) {
     int64_t gi = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (gi >= hi) return;
     const int t = coll_slab[gi];
     const int32_t* T = slab_T + (size_t)t * d;
-    int64_t r = gi - coll_off[t], base = 0, st = 1;
+    const int32_t* s64 = str64 + (size_t)t * d;
+    const int32_t* s32 = str32 + (size_t)t * d;
+    int64_t r = gi - coll_off[t], base = 0, st = 1, p64 = 0, p32 = 0;
     int ncd = 0;
     int64_t cstr[lsg::kMaxDim];
     for (int k = 0; k < d; ++k) {
         int64_t ext = (int64_t)1 << T[k];
-        if (T[k] >= 2) { base += (r % ext) * st; r /= ext; }
-        else cstr[ncd++] = st;
+        if (T[k] >= 2) {
+            const int64_t ck = r % ext;
+            base += ck * st;
+            p64 += ck * s64[k];
+            p32 += ck * s32[k];
+            r /= ext;
+        } else cstr[ncd++] = st;
         st *= ext;
     }
     const double* a = acell + cell_off[t];
@@ -492,6 +501,6 @@ __global__ void k_sf_collapse(const int32_t* __restrict__ slab_T, int d, const i
             if ((b >> i) & 1) key += cstr[i];
         acc += a[key];
     }
-    c64[gi] = acc;
-    c32[gi] = (float)acc;
+    c64[coll_off[t] + p64] = acc;
+    c32[coll_off[t] + p32] = (float)acc;
 }
