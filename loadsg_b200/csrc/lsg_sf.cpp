@@ -155,6 +155,16 @@ std::vector<SfSlab> sf_plan(const Plan& p, const SfCoefLayout& L, int64_t wcap, 
         }
         D.hi_off = D.stage[D.nm];
         D.wtotal = D.nm == 0 ? D.stage[0] : D.stage[D.nm] + D.stage[D.nm - 1];
+        // b segments of the fused step: as many as fill the CTA's 256 threads,
+        // each of at least two b cells; the two parts of every row between
+        // segments go to the idle ping-pong region (nm >= 1 only)
+        D.nseg = 1;
+        if (D.nm >= 1 && D.b.T >= 0 && D.a.n < 7) {  // the 7-node a path has no registers to spare
+            const int64_t cells = (int64_t)D.b.n + 1;
+            while ((int64_t)D.npl * D.nseg * 2 <= 256 && D.nseg * 2 * 2 <= cells &&
+                   (int64_t)D.npl * (D.nseg * 2 - 1) * 2 * D.a.n <= D.stage[D.nm - 1])
+                D.nseg *= 2;
+        }
         // coefficient order of the slab: mid dimensions fastest, then a, b and
         // the chunked dimensions (n + 1 cells each)
         int32_t cs = 1;

@@ -35,7 +35,10 @@
 //   * the remaining "mid" dimensions are swept through shared memory, one
 //     dimension per stage, ping-ponging between two regions;
 //   * the two innermost remaining dimensions (a, held in registers, and b,
-//     streamed) are transformed, scaled and transformed back in one pass.
+//     streamed) are transformed, scaled and transformed back in one pass; when
+//     a chunk has few planes, each plane's b cells are split into nseg
+//     segments on as many threads, and the row shared by two segments is the
+//     sum of their two partial rows, added in segment order after a barrier.
 // Stage layouts keep the slab's dimension order without the chunked
 // dimensions (a fastest); slice position e maps to u by inserting each chunked
 // dimension (fast division by the slice extent below it).  No atomics: every
@@ -90,7 +93,7 @@ struct SfSlab {
     int32_t hi_off = 0;       // offset of the second ping-pong region (= stage[nm])
     int32_t wtotal = 0;       // work-space elements: stage[0] (nm = 0), else stage[nm] + stage[nm-1]
     int32_t na_max = 0;       // largest a extent this plan was made for
-    int32_t pad = 0;
+    int32_t nseg = 1;         // b segments per plane in the fused step (power of two; FP64 kernel)
 };
 
 // Dynamic shared memory of the k_sf CTA of one slab: the work space, then two

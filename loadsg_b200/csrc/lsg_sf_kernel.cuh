@@ -100,11 +100,16 @@ __device__ __forceinline__ void bwd_x(const ModesX<V, NX>& G, V* Y) {
 
 // The fused (a, b) step of one pencil plane P (a fastest, rows of NX values,
 // nb rows), in place, for an a dimension of exactly NX nodes (NX = 1: no a
-// dimension).  (S, M): pair of every other dimension; cf: coefficient of the
-// plane's cell in the other dimensions (a and b cell 0).
+// dimension), over the b cells [c0, c1) of the cells 0 .. nb (cell 0 and nb:
+// the boundary cells; cell c: rows c - 1 and c).  (S, M): pair of every other
+// dimension; cf: coefficient of the plane's cell in the other dimensions (a and
+// b cell 0).  Rows with both cells in the range are written in place.  With
+// c0 > 0, row c0 - 1 gets only cell c0's part: it goes to bnd[-NX .. -1] (value
+// space); with c1 <= nb, row c1 - 1 gets only cell c1 - 1's part: it goes to
+// bnd[0 .. NX-1].  The whole plane (c0 = 0, c1 = nb + 1) has neither.
 template <typename V, int NX>
 __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M, const V* cf, bool unit, V unit_v,
-                                            int form) {
+                                            int form, int c0, int c1, V* bnd) {
     using V2 = typename PairT<V>::T;
     const int nb = D.b.n;
     const bool bvirt = D.b.T < 0;
@@ -145,6 +150,7 @@ __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M
 #pragma unroll
         for (int i = 0; i < NX; ++i) P[row * NX + i] = Y[i];
     };
+    const int ce = c1 < nb ? c1 : nb;  // interior cells [cs, ce)
     if constexpr (NX == 1) {
         // one value per row: the b stream alone
         V lP, lM, lB;
@@ -158,23 +164,40 @@ __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M
         lam(0, pP, pM, pB);
         lam(1, mP, mM, mB);
         lam(2, lP, lM, lB);
-        V fp = P[0];
-        coefs(0);
-        V acc = c[0] * lB * fp;
-        for (int jb = 1; jb < nb; ++jb) {
+        V fp, acc;
+        int cs;
+        if (c0 == 0) {  // left boundary cell: row 0 only
+            fp = P[0];
+            coefs(0);
+            acc = c[0] * lB * fp;
+            cs = 1;
+        } else {        // row c0 - 1: this segment's part starts empty
+            fp = P[c0 - 1];
+            acc = V(0);
+            cs = c0;
+        }
+        auto cell = [&](int jb) {
             V f = P[jb];
             coefs(jb);
             V gp = c[0] * pB * (fp + f), gm = c[0] * mB * (fp - f);
-            P[jb - 1] = acc + gp + gm;
+            V o = acc + gp + gm;
             acc = gp - gm;
             fp = f;
+            return o;
+        };
+        if (c0 > 0) bnd[-1] = cell(cs++);
+        for (int jb = cs; jb < ce; ++jb) P[jb - 1] = cell(jb);
+        if (c1 > nb) {  // right boundary cell nb: row nb-1 only
+            coefs(nb);
+            P[nb - 1] = acc + c[0] * lB * fp;
+        } else {
+            bnd[0] = acc;
         }
-        coefs(nb);
-        P[nb - 1] = acc + c[0] * lB * fp;
     } else {
-        ModesX<V, NX> Fp, Fc, acc;
+        ModesX<V, NX> Fp, acc;
         V lP, lM, lB;
         if (bvirt) {
+            ModesX<V, NX> Fc;
             load(0);
             fwd_x<V, NX>(X, Fc);
             coefs(0);
@@ -192,20 +215,14 @@ __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M
         lam(1, mP, mM, mB);
         lam(2, lP, lM, lB);        // ... and of the boundary b cells
         const V2 lp2 = mk2(pP, pM), lm2 = mk2(mP, mM);
-        load(0);
-        fwd_x<V, NX>(X, Fp);
-        coefs(0);  // left boundary b cell: row 0 only
-        acc.bl = c[0] * lB * Fp.bl;
-        acc.br = c[NX] * lB * Fp.br;
-#pragma unroll
-        for (int i = 0; i < NX - 1; ++i) acc.pm[i] = mk2(c[i + 1] * lP * Fp.pm[i].x, c[i + 1] * lM * Fp.pm[i].y);
-        for (int jb = 1; jb < nb; ++jb) {
+        // interior b cell jb between rows jb-1 and jb: per a mode, b modes
+        // P = Fp + Fc, M = Fp - Fc, scaled; row jb-1 gets P' + M' (complete, into
+        // Y), row jb starts with P' - M'
+        auto cell = [&](int jb) {
             load(jb);
             coefs(jb);
-            fwd_x<V, NX>(X, Fc);  // interior b cell jb between rows jb-1 and jb
-            // per a mode: b modes P = Fp + Fc, M = Fp - Fc, scaled; row jb-1
-            // gets P' + M' (complete), row jb starts with P' - M'
-            ModesX<V, NX> out;
+            ModesX<V, NX> Fc, out;
+            fwd_x<V, NX>(X, Fc);
             {
                 V gp = c[0] * pB * (Fp.bl + Fc.bl), gm = c[0] * mB * (Fp.bl - Fc.bl);
                 out.bl = acc.bl + gp + gm;
@@ -225,16 +242,47 @@ __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M
             }
             Fp = Fc;
             bwd_x<V, NX>(out, Y);
+        };
+        int cs;
+        if (c0 == 0) {
+            load(0);
+            fwd_x<V, NX>(X, Fp);
+            coefs(0);  // left boundary b cell: row 0 only
+            acc.bl = c[0] * lB * Fp.bl;
+            acc.br = c[NX] * lB * Fp.br;
+#pragma unroll
+            for (int i = 0; i < NX - 1; ++i) acc.pm[i] = mk2(c[i + 1] * lP * Fp.pm[i].x, c[i + 1] * lM * Fp.pm[i].y);
+            cs = 1;
+        } else {  // row c0 - 1: this segment's part starts empty and goes to bnd[-NX ..]
+            load(c0 - 1);
+            fwd_x<V, NX>(X, Fp);
+            acc.bl = V(0);
+            acc.br = V(0);
+#pragma unroll
+            for (int i = 0; i < NX - 1; ++i) acc.pm[i] = mk2(V(0), V(0));
+            cell(c0);
+#pragma unroll
+            for (int i = 0; i < NX; ++i) bnd[i - NX] = Y[i];
+            cs = c0 + 1;
+        }
+        for (int jb = cs; jb < ce; ++jb) {
+            cell(jb);
             store(jb - 1);
         }
-        coefs(nb);  // right boundary b cell nb: row nb-1 only
-        acc.bl += c[0] * lB * Fp.bl;
-        acc.br += c[NX] * lB * Fp.br;
+        if (c1 > nb) {
+            coefs(nb);  // right boundary b cell nb: row nb-1 only
+            acc.bl += c[0] * lB * Fp.bl;
+            acc.br += c[NX] * lB * Fp.br;
 #pragma unroll
-        for (int i = 0; i < NX - 1; ++i)
-            acc.pm[i] = padd(acc.pm[i], mk2(c[i + 1] * lP * Fp.pm[i].x, c[i + 1] * lM * Fp.pm[i].y));
-        bwd_x<V, NX>(acc, Y);
-        store(nb - 1);
+            for (int i = 0; i < NX - 1; ++i)
+                acc.pm[i] = padd(acc.pm[i], mk2(c[i + 1] * lP * Fp.pm[i].x, c[i + 1] * lM * Fp.pm[i].y));
+            bwd_x<V, NX>(acc, Y);
+            store(nb - 1);
+        } else {
+            bwd_x<V, NX>(acc, Y);
+#pragma unroll
+            for (int i = 0; i < NX; ++i) bnd[i] = Y[i];
+        }
     }
 }
 
@@ -369,7 +417,23 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
                 V* out = dst + i + (size_t)I * 2 * n * o;
                 V xp = in[0];
                 out[0] = xp;
-                for (int j = 1; j < n; ++j) {
+                int j = 1;
+                if constexpr (sizeof(V) == 8) {  // FP64: four loads in flight before the stores
+                    for (; j + 3 < n; j += 4) {
+                        const V x0 = in[(size_t)j * I], x1 = in[(size_t)(j + 1) * I];
+                        const V x2 = in[(size_t)(j + 2) * I], x3 = in[(size_t)(j + 3) * I];
+                        out[(size_t)(2 * j - 1) * I] = xp + x0;
+                        out[(size_t)(2 * j) * I] = xp - x0;
+                        out[(size_t)(2 * j + 1) * I] = x0 + x1;
+                        out[(size_t)(2 * j + 2) * I] = x0 - x1;
+                        out[(size_t)(2 * j + 3) * I] = x1 + x2;
+                        out[(size_t)(2 * j + 4) * I] = x1 - x2;
+                        out[(size_t)(2 * j + 5) * I] = x2 + x3;
+                        out[(size_t)(2 * j + 6) * I] = x2 - x3;
+                        xp = x3;
+                    }
+                }
+                for (; j < n; ++j) {
                     V x = in[(size_t)j * I];
                     out[(size_t)(2 * j - 1) * I] = xp + x;
                     out[(size_t)(2 * j) * I] = xp - x;
@@ -379,11 +443,20 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
             }
             __syncthreads();
         }
-        // fused (a, b) step on every pencil plane
+        // fused (a, b) step on every pencil plane; with G > 1 segments per
+        // plane, each row between two segments is completed after a barrier
+        // from the two parts the segments left in the idle ping-pong region:
+        // the left segment's, then the right segment's
         {
             V* F = region(nm);
-            const int plane = D.a.n * D.b.n;
-            for (int pl = tid; pl < D.npl; pl += T) {
+            const int plane = D.a.n * D.b.n, na = D.a.n;
+            // FP64 only: the FP32 kernel (80 registers for three CTAs per SM) has none to spare
+            const int G = (sizeof(V) == 8 && D.nseg > 1 && D.npl * D.nseg <= T) ? D.nseg : 1;
+            const int lg = 31 - __clz(G);
+            const int L = (D.b.n + 1) >> lg;  // b cells per segment (nb + 1 = 2^T_b when G > 1)
+            V* Wr = region(nm > 0 ? nm - 1 : 0);  // per boundary row: [left part | right part]
+            for (int w = tid; w < D.npl * G; w += T) {
+                const int pl = w >> lg, sg = w & (G - 1);
                 V S = s_cS[bf], M = s_cM[bf];
                 int64_t cb = s_cbase[bf];
                 uint32_t r = (uint32_t)pl;
@@ -398,11 +471,25 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
                     cb += (int64_t)cell * x.cstride;
                 }
                 V* Pp = F + (size_t)pl * plane;
-                if (D.a.T < 0) fused_plane<V, 1>(Pp, D, S, M, cf0 + cb, unit != 0, unit_v, form);
-                else if (NA >= 7 && D.a.n == 7) fused_plane<V, (NA >= 7 ? 7 : 3)>(Pp, D, S, M, cf0 + cb, unit != 0, unit_v, form);
-                else fused_plane<V, 3>(Pp, D, S, M, cf0 + cb, unit != 0, unit_v, form);
+                const int c0 = sg * L, c1 = G == 1 ? D.b.n + 1 : c0 + L;
+                // boundary row sg (after this segment): [this segment's part | the next one's]
+                V* bnd = Wr + (size_t)2 * na * ((size_t)pl * (G - 1) + sg);
+                if (D.a.T < 0) fused_plane<V, 1>(Pp, D, S, M, cf0 + cb, unit != 0, unit_v, form, c0, c1, bnd);
+                else if (NA >= 7 && D.a.n == 7)  // never segmented (register budget)
+                    fused_plane<V, (NA >= 7 ? 7 : 3)>(Pp, D, S, M, cf0 + cb, unit != 0, unit_v, form, 0, D.b.n + 1, bnd);
+                else fused_plane<V, 3>(Pp, D, S, M, cf0 + cb, unit != 0, unit_v, form, c0, c1, bnd);
             }
             __syncthreads();
+            if (G > 1) {
+                const int nbr = D.npl * (G - 1) * na;  // boundary-row values
+                for (int e = tid; e < nbr; e += T) {
+                    const int i = e % na, rowid = e / na;             // rowid = pl * (G - 1) + (sg - 1)
+                    const int pl = rowid / (G - 1), sg = rowid - pl * (G - 1) + 1;
+                    const V* part = Wr + (size_t)2 * na * rowid;
+                    F[(size_t)pl * plane + (size_t)(sg * L - 1) * na + i] = part[i] + part[na + i];
+                }
+                __syncthreads();
+            }
         }
         // mid sweeps, transposed
         for (int k = nm - 1; k >= 0; --k) {
@@ -416,7 +503,23 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
                 const V* in = src + i + (size_t)I * 2 * n * o;
                 V* out = dst + i + (size_t)I * n * o;
                 V l = in[0];
-                for (int j = 1; j < n; ++j) {
+                int j = 1;
+                if constexpr (sizeof(V) == 8) {  // FP64: eight loads in flight before the stores
+                    for (; j + 3 < n; j += 4) {
+                        V pp[4], mm[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            pp[u] = in[(size_t)(2 * (j + u) - 1) * I];
+                            mm[u] = in[(size_t)(2 * (j + u)) * I];
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            out[(size_t)(j + u - 1) * I] = l + (pp[u] + mm[u]);
+                            l = pp[u] - mm[u];
+                        }
+                    }
+                }
+                for (; j < n; ++j) {
                     V pp = in[(size_t)(2 * j - 1) * I], mm = in[(size_t)(2 * j) * I];
                     out[(size_t)(j - 1) * I] = l + (pp + mm);
                     l = pp - mm;
