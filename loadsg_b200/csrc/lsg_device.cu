@@ -827,7 +827,7 @@ struct lsg_operator {
     bool have_learned = false;
     int64_t smem_cap64 = 0, smem_cap32 = 0;
     std::vector<int64_t> level_need;  // per phase-B level: largest vector of any item
-    lsg_tuning tune{256, 72, 4, 512, 12288, 256};  // launch parameters (lsg_operator_autotune)
+    lsg_tuning tune{256, 72, 4, 512, 4096, 256};  // launch parameters (lsg_operator_autotune)
     std::shared_ptr<void> basis;      // basis-transform tables (lsg_basis.cu), built on first use
     std::shared_ptr<void> bdrhs;      // boundary right-hand-side tables (lsg_bdrhs.cu), built on first use
     // cell operator launch plan, per precision: the factorised dense-slab
@@ -2411,7 +2411,7 @@ extern "C" int lsg_operator_autotune(lsg_operator* op, int32_t precision, int32_
     const std::vector<std::pair<int32_t lsg_tuning::*, std::vector<int32_t>>> space = {
         {&lsg_tuning::cell_space_kb, {48, 72, 100}},  {&lsg_tuning::cell_threads, {128, 256}},
         {&lsg_tuning::class_ratio, {2, 4, 16}},       {&lsg_tuning::level_threads, {64, 128, 256, 512}},
-        {&lsg_tuning::level_cap, {4096, 8192, 12288}}, {&lsg_tuning::prolong_threads, {128, 256, 512}}};
+        {&lsg_tuning::level_cap, {2048, 4096, 8192, 12288}}, {&lsg_tuning::prolong_threads, {128, 256, 512}}};
     for (int pass = 0; pass < 2 && !err; ++pass) {
         bool moved = false;
         for (const auto& dim : space) {
