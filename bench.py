@@ -326,51 +326,88 @@ def log(msg):
     print(f"[bench {time.perf_counter() - _T0:8.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
-def batch_leg(lsg, torch, dev, stream, count=48, seed=7):
-    """Many uneven grids solved in one batch against the same grids solved one
-    after another: d ~ U{4,5,6}, regular level ~ U{3..6} (129 to 40,193
-    points), a = 1 + 0.9 prod sin(pi m_i x_i) with m_i ~ U{1..3}, f ~ U[-1,1];
-    FP32+IR with Jacobi to relative residual 1e-10."""
+# device bytes per grid point of a batch operator (FP64 and FP32 buffers of the
+# per-case slabs and the tables), by dimension: sizes the groups of the batch leg
+BATCH_BYTES_PER_POINT = {4: 2000, 5: 3200, 6: 5000}
+
+
+def batch_leg(lsg, torch, dev, stream, count=48, seed=7, levels=(3, 6), mem_gb=100.0, compare_every=1):
+    """Many uneven grids solved in batches against grids solved one after
+    another: d ~ U{4,5,6}, regular level ~ U{levels}, a = 1 + 0.9 prod
+    sin(pi m_i x_i) with m_i ~ U{1..3}, f ~ U[-1,1]; FP32+IR with Jacobi to
+    relative residual 1e-10.  Grids go into consecutive groups of at most
+    mem_gb estimated device memory; each group is one batch (one CUDA graph
+    per batched iteration).  The one-at-a-time comparison takes every
+    compare_every-th grid, solved alone and as one batch."""
     rng = np.random.default_rng(seed)
     grids, probs, fs = [], [], []
+    t0 = time.perf_counter()
     for _ in range(count):
         d = int(rng.integers(4, 7))
-        level = int(rng.integers(3, 7))
+        level = int(rng.integers(levels[0], levels[1] + 1))
         g = lsg.AdaptiveSparseGrid.regular(d, level)
         grids.append(g)
         probs.append(lsg.MidpointDiffusion(lsg.COEF_SINPROD, [1.0, 0.9] + list(rng.integers(1, 4, d).astype(float))))
         fs.append(rng.uniform(-1, 1, g.n) * g.active)
-    t0 = time.perf_counter()
-    b = lsg.Batch(grids, probs)
-    setup = time.perf_counter() - t0
-    log(f"batch: {count} grids, {b.size} points, created in {setup:.1f}s")
-    b.autotune(lsg.FP32, reps=2)
-    log("batch: autotuned")
-    f = torch.tensor(b.gather(fs), dtype=torch.float64, device=dev)
-    x = torch.zeros_like(f)
+    log(f"batch: {count} grids, {sum(g.n for g in grids)} points generated in {time.perf_counter() - t0:.1f}s")
     o = lsg.SolverOpts(1e-10, 1, 3000, 0, lsg.FP32, 1000, 1e-5, 1)
-    b.solve_device(f.data_ptr(), x.data_ptr(), o, stream)  # warm-up
-    x.zero_()
-    reps, tot = b.solve_device(f.data_ptr(), x.data_ptr(), o, stream)
-    log(f"batch: solved in {tot['seconds']:.3f}s ({tot['iterations']} batched iterations)")
-    # the same grids one at a time
+    warm = lsg.SolverOpts(1e-10, 1, 4, 0, lsg.FP32, 4, 1e-5, 1)  # builds and captures the iteration graphs
+
+    def solve_batch(idx):
+        t0 = time.perf_counter()
+        b = lsg.Batch([grids[i] for i in idx], [probs[i] for i in idx])
+        setup = time.perf_counter() - t0
+        b.autotune(lsg.FP32, reps=2)
+        f = torch.tensor(b.gather([fs[i] for i in idx]), dtype=torch.float64, device=dev)
+        x = torch.zeros_like(f)
+        b.solve_device(f.data_ptr(), x.data_ptr(), warm, stream)
+        x.zero_()
+        reps, tot = b.solve_device(f.data_ptr(), x.data_ptr(), o, stream)
+        out = {"grids": len(idx), "points": int(b.size), "seconds": tot["seconds"], "iterations": tot["iterations"],
+               "max_rel_residual": tot["rel_residual"], "converged": bool(tot["converged"]),
+               "kernel_launches": int(tot["kernel_launches"]), "setup_seconds": setup}
+        del b
+        return out
+
+    groups, cur, cur_b = [], [], 0.0
+    for i, g in enumerate(grids):
+        est = BATCH_BYTES_PER_POINT[g.d] * g.n / 1e9
+        if cur and cur_b + est > mem_gb:
+            groups.append(cur)
+            cur, cur_b = [], 0.0
+        cur.append(i)
+        cur_b += est
+    groups.append(cur)
+    parts = []
+    for gi, idx in enumerate(groups):
+        r = solve_batch(idx)
+        parts.append(r)
+        log(f"batch group {gi}: {r['grids']} grids, {r['points']} points, solved in {r['seconds']:.3f}s "
+            f"({r['iterations']} batched iterations, converged {r['converged']})")
+    total = sum(r["seconds"] for r in parts)
+    sub = list(range(0, count, compare_every))
+    sub_batched = total if compare_every == 1 else solve_batch(sub)["seconds"]
     seq = 0.0
-    seq_its = []
-    for g, p, fi in zip(grids, probs, fs):
-        m = lsg.MatrixVectorHomogen(g, p)
-        fd = torch.tensor(fi, dtype=torch.float64, device=dev)
+    for i in sub:
+        m = lsg.MatrixVectorHomogen(grids[i], probs[i])
+        fd = torch.tensor(fs[i], dtype=torch.float64, device=dev)
         xd = torch.zeros_like(fd)
-        lsg.CG.solve_device(m, fd.data_ptr(), xd.data_ptr(), o, stream)  # warm-up
+        lsg.CG.solve_device(m, fd.data_ptr(), xd.data_ptr(), warm, stream)
         xd.zero_()
         r = lsg.CG.solve_device(m, fd.data_ptr(), xd.data_ptr(), o, stream)
         seq += r["seconds"]
-        seq_its.append(r["iterations"])
-    log(f"batch: one at a time {seq:.3f}s")
-    return {"grids": count, "points": int(b.size), "description": batch_leg.__doc__.split(":", 1)[1].strip(),
-            "seconds": tot["seconds"], "batched_iterations": tot["iterations"],
-            "max_rel_residual": tot["rel_residual"], "all_converged": bool(tot["converged"]),
-            "one_at_a_time_seconds": seq, "speedup": seq / tot["seconds"] if tot["seconds"] > 0 else None,
-            "setup_seconds": setup, "kernel_launches": int(tot["kernel_launches"])}
+        del m
+    log(f"batch: {len(sub)} grids one at a time {seq:.3f}s, as one batch {sub_batched:.3f}s")
+    return {"grids": count, "points": int(sum(g.n for g in grids)), "levels": list(levels),
+            "description": batch_leg.__doc__.split(":", 1)[1].strip(),
+            "groups": len(parts), "group_mem_gb": mem_gb, "seconds": total,
+            "batched_iterations": max(r["iterations"] for r in parts),
+            "max_rel_residual": max(r["max_rel_residual"] for r in parts),
+            "all_converged": all(r["converged"] for r in parts),
+            "kernel_launches": sum(r["kernel_launches"] for r in parts),
+            "setup_seconds": sum(r["setup_seconds"] for r in parts), "group_results": parts,
+            "compare_grids": len(sub), "compare_batched_seconds": sub_batched, "one_at_a_time_seconds": seq,
+            "speedup": seq / sub_batched if sub_batched > 0 else None}
 
 
 def d8_sweep(lsg, torch, solve_up_to=40000):
@@ -428,6 +465,10 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-bdrhs", action="store_true", help="skip the boundary-data right-hand-side leg")
     ap.add_argument("--batch-grids", type=int, default=48, help="grids in the batch leg")
+    ap.add_argument("--batch-levels", default="3,6", help="regular levels of the batch grids: lo,hi")
+    ap.add_argument("--batch-mem-gb", type=float, default=100.0, help="estimated device memory per batch")
+    ap.add_argument("--batch-compare-every", type=int, default=1,
+                    help="one-at-a-time comparison on every k-th grid (solved alone and as one batch)")
     ap.add_argument("--batch-only", action="store_true", help="run only the batch leg (one JSON line)")
     ap.add_argument("--sweep", action="store_true",
                     help="matvec sweep over d=8 grids refined toward x_1 = 1/2 (one JSON line per grid) instead")
@@ -462,7 +503,9 @@ def main():
         return
     if args.batch_only:
         dev = torch.device("cuda", local)
-        b = batch_leg(lsg, torch, dev, torch.cuda.current_stream().cuda_stream, count=args.batch_grids)
+        b = batch_leg(lsg, torch, dev, torch.cuda.current_stream().cuda_stream, count=args.batch_grids,
+                      levels=tuple(int(v) for v in args.batch_levels.split(",")), mem_gb=args.batch_mem_gb,
+                      compare_every=args.batch_compare_every)
         if rank == 0:
             print(json.dumps({"batch": b}))
         return

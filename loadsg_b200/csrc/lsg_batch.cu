@@ -632,11 +632,14 @@ int lsg_batch_create(int32_t count, const int32_t* dims, const int32_t* const* p
     std::unique_ptr<lsg_batch> b(new lsg_batch());
     b->count = count;
     std::vector<lsg::Plan> plans(count);
-    for (int i = 0; i < count; ++i) {
+    for (int i = 0; i < count; ++i)
         if (!points[i] || !active[i]) return fail_msg(LSG_E_INVALID, "null grid in batch");
-        if (!lsg::build_plan(dims[i], n[i], points[i], active[i], plans[i]))
-            return fail_msg(LSG_E_INVALID, ("grid " + std::to_string(i) + ": " + plans[i].error).c_str());
-    }
+    // the grids' plans are independent host work: one grid per thread
+    std::vector<uint8_t> ok(count, 0);
+#pragma omp parallel for schedule(dynamic, 1) if (count > 1)
+    for (int i = 0; i < count; ++i) ok[i] = lsg::build_plan(dims[i], n[i], points[i], active[i], plans[i]) ? 1 : 0;
+    for (int i = 0; i < count; ++i)
+        if (!ok[i]) return fail_msg(LSG_E_INVALID, ("grid " + std::to_string(i) + ": " + plans[i].error).c_str());
     b->grid_group.assign(count, -1);
     b->grid_part.assign(count, -1);
     b->off.assign(count, 0);
