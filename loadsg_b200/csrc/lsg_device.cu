@@ -827,7 +827,7 @@ struct lsg_operator {
     bool have_learned = false;
     int64_t smem_cap64 = 0, smem_cap32 = 0;
     std::vector<int64_t> level_need;  // per phase-B level: largest vector of any item
-    lsg_tuning tune{256, 72, 4, 512, 4096, 256};  // launch parameters (lsg_operator_autotune)
+    lsg_tuning tune{256, 72, 4, 256, 2048, 256};  // launch parameters (lsg_operator_autotune)
     std::shared_ptr<void> basis;      // basis-transform tables (lsg_basis.cu), built on first use
     std::shared_ptr<void> bdrhs;      // boundary right-hand-side tables (lsg_bdrhs.cu), built on first use
     // cell operator launch plan, per precision: the factorised dense-slab
