@@ -10,8 +10,10 @@
 //       overlap, refill :12-200)
 // Points are kept in insertion (storage) order; the iteration orders of the
 // reference are kept as well, so the result is the reference's grid, storage
-// order included.  Stage (e) pairs points through their supports with a
-// per-depth index instead of testing all point pairs.
+// order included.  Stage (e) tests the reference's point pairs (depth-group
+// pairs whose componentwise maximum is a depth of the grid, then every active
+// pair with overlapping supports), which is quadratic in the grid size: it runs
+// on grids of at most LSG_PAIRWISE_MAX points.
 #include "../../include/lsg.h"
 
 #include <algorithm>
