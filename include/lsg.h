@@ -260,9 +260,11 @@ int lsg_pde_boundary_rhs(lsg_operator *op, int32_t kind, int64_t nn, const int32
                          double *f, double *g, double *rhs);
 
 /* ---- launch parameters of the matvec and the autotuner that picks them.
- * The defaults suit large d=5/6 grids; lsg_operator_autotune times matvecs of
- * this operator over a candidate set per parameter (coordinate descent, two
- * passes, best of `reps` timings per setting) and keeps the fastest setting.
+ * The defaults (256, 72, 4, 256, 2048, 256) suit large d=5/6 grids;
+ * lsg_operator_autotune times matvecs of this operator over a candidate set
+ * per parameter (coordinate descent, two passes, best of `reps` timings per
+ * setting) and keeps the fastest setting.  Changing cell_space_kb re-plans the
+ * dense slabs (and re-orders their collapsed coefficients).
  * No counterpart in the reference (OpenMP schedule only). */
 typedef struct {
     int32_t cell_threads;    /* threads per cell-operator CTA: 64..256, multiple of 32 */

@@ -56,7 +56,6 @@ struct Buf {
         if (e != cudaSuccess) return fail_msg(LSG_E_CUDA, (std::string("cudaMalloc: ") + cudaGetErrorString(e)).c_str());
         return 0;
     }
-    int zero(cudaStream_t st) { return bytes ? (int)cudaMemsetAsync(p, 0, bytes, st) : 0; }
     template <typename T>
     T* as() const { return static_cast<T*>(p); }
 };

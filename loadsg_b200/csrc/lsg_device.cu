@@ -196,7 +196,6 @@ struct CellCfg {
     static constexpr int DL = D <= KDL ? D : KDL;
     static constexpr int G = 1 << (D - DL);
     static constexpr int NL = 1 << DL;
-    static constexpr int NH = NL / 2;  // corners per dim-0 face held by one lane
 };
 
 template <int D, typename V>

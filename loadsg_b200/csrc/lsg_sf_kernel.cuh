@@ -194,7 +194,7 @@ __device__ __forceinline__ void fused_plane(V* P, const lsg::SfSlab& D, V S, V M
             bnd[0] = acc;
         }
     } else {
-        ModesX<V, NX> Fp, acc;
+        ModesX<V, NX> Fp{}, acc{};
         V lP, lM, lB;
         if (bvirt) {
             ModesX<V, NX> Fc;
@@ -481,10 +481,11 @@ __global__ void __launch_bounds__(256, (sizeof(V) == 4 ? 3 : 2)) k_sf(const lsg:
             }
             __syncthreads();
             if (G > 1) {
-                const int nbr = D.npl * (G - 1) * na;  // boundary-row values
+                const int g1 = G - 1 > 0 ? G - 1 : 1;  // boundary rows per plane
+                const int nbr = D.npl * g1 * na;       // boundary-row values
                 for (int e = tid; e < nbr; e += T) {
-                    const int i = e % na, rowid = e / na;             // rowid = pl * (G - 1) + (sg - 1)
-                    const int pl = rowid / (G - 1), sg = rowid - pl * (G - 1) + 1;
+                    const int i = e % na, rowid = e / na;  // rowid = pl * (G - 1) + (sg - 1)
+                    const int pl = rowid / g1, sg = rowid - pl * g1 + 1;
                     const V* part = Wr + (size_t)2 * na * rowid;
                     F[(size_t)pl * plane + (size_t)(sg * L - 1) * na + i] = part[i] + part[na + i];
                 }
