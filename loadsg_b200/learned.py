@@ -15,6 +15,7 @@ diagonal inside the library.
     python -m loadsg_b200.learned train --out loadsg_b200/weights/diag_mlp_d5.npz
 """
 import argparse
+import json
 import ctypes
 import os
 import time
@@ -261,6 +262,17 @@ def report(weights, d, level, refine, family, seeds, log=print):
             res[name] = (rep["iterations"], time.perf_counter() - t0, rep["rel_residual"], rep["fell_back"])
         rows.append(res)
         log(res)
+    if rows:  # summary over the held-out instances
+        summ = {"instances": len(rows), "n": rows[0]["n"], "d": d, "level": level, "refine": refine, "family": family}
+        for name in ("none", "jacobi", "learned"):
+            its = np.array([r[name][0] for r in rows], dtype=float)
+            secs = np.array([r[name][1] for r in rows], dtype=float)
+            summ[name] = {"iterations_mean": float(its.mean()), "iterations_min": int(its.min()),
+                          "iterations_max": int(its.max()), "seconds_mean": float(secs.mean()),
+                          "fell_back": int(sum(r[name][3] for r in rows))}
+        lj = np.array([r["learned"][0] - r["jacobi"][0] for r in rows])
+        summ["learned_minus_jacobi_iterations"] = {"mean": float(lj.mean()), "min": int(lj.min()), "max": int(lj.max())}
+        log(json.dumps({"summary": summ}))
     return rows
 
 
@@ -282,7 +294,11 @@ def main():
         train(out=a.out, d=a.d, level=levels, refine=a.refine, epochs=a.epochs, n_train=a.n_train, n_val=a.n_val,
               family=a.family)
     else:
-        report(a.out, a.d, int(a.level.split(",")[-1]), a.refine, a.family, [int(x) for x in a.seeds.split(",")])
+        seeds = []
+        for part in a.seeds.split(","):  # "10000,10001" or a range "10000-10199"
+            lo, _, hi = part.partition("-")
+            seeds += list(range(int(lo), int(hi) + 1)) if hi else [int(lo)]
+        report(a.out, a.d, int(a.level.split(",")[-1]), a.refine, a.family, seeds)
 
 
 if __name__ == "__main__":
