@@ -81,7 +81,11 @@ def test_cg_reference_criterion(golden):
 
 def test_cg_iterations_match_oracle(golden):
     """Reference stopping rule at its default eps = 1e-10: same iteration count
-    as the CPU restatement of CG::solveHomogen."""
+    as the CPU restatement of CG::solveHomogen, and then the same solution to
+    relative error 1e-10.  The rule r^T D^-1 r <= 1e-10 stops early, at a
+    relative residual of order 1e-5, so where a delta sits at the threshold
+    rounding can move the stop by one iteration; the solutions then differ by
+    that one CG step (1e-6)."""
     if "cg_x" not in golden:
         pytest.skip("no CG vector")
     g, m, prob = op_for(golden)
@@ -90,7 +94,7 @@ def test_cg_iterations_match_oracle(golden):
     o = oracle.OracleGrid(golden["points"], golden["active"])
     xo, it = o.cg(int(golden["coef_family"]), golden["coef_params"], golden["f"], 1e-10)
     assert abs(rep["iterations"] - it) <= 1
-    assert rel(x, xo) < 1e-6
+    assert rel(x, xo) < (1e-10 if rep["iterations"] == it else 1e-6)
 
 
 def test_hanging_entries_untouched(golden):
