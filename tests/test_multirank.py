@@ -8,6 +8,7 @@ import subprocess
 import sys
 
 import numpy as np
+import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
@@ -61,3 +62,27 @@ def test_reference_arm_runs_on_rank_zero_only():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
                        capture_output=True, text=True, env=env, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_reference_arm_line():
+    """Rank 0 of the reference arm: the reference's own CG::solveHomogen on the
+    CPU-runnable instance (7,423 points), one JSON line with the native arm's
+    metric and unit, a measured (never scaled) value, and no part of this
+    repository's library loaded."""
+    import json
+    exe = os.path.join(ROOT, "oracle", "_ref", "fast_d3", "ref_harness")
+    if not os.path.exists(exe):
+        pytest.skip("the reference harness (oracle/_ref) is not built")
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '1']; "
+            "runpy.run_path('bench.py', run_name='__main__'); "
+            "import loadsg_b200; assert loadsg_b200._LIB is None, 'liblsg.so was loaded'")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == "s"
+    assert line["higher_is_better"] is False and line["config"]["n_points"] == 7423
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["n_points"] == 7423 and cb["iterations"] > 0
+    assert cb["rel_residual"] <= 1.01e-10 and line["value"] == cb["value"] > 0
+    assert line["e2e"] == {"value": line["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
