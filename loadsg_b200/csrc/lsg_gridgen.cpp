@@ -10,10 +10,9 @@
 //       overlap, refill :12-200)
 // Points are kept in insertion (storage) order; the iteration orders of the
 // reference are kept as well, so the result is the reference's grid, storage
-// order included.  Stage (e) tests the reference's point pairs (depth-group
-// pairs whose componentwise maximum is a depth of the grid, then every active
-// pair with overlapping supports), which is quadratic in the grid size: it runs
-// on grids of at most LSG_PAIRWISE_MAX points.
+// order included.  Stage (e) visits the reference's point pairs in the
+// reference's order but finds them through the grid's index instead of a
+// pairwise scan (add_points2 below).
 #include "../../include/lsg.h"
 
 #include <algorithm>
@@ -22,9 +21,6 @@
 #include <map>
 #include <vector>
 
-#ifndef LSG_PAIRWISE_MAX
-#define LSG_PAIRWISE_MAX 40000
-#endif
 namespace {
 
 inline int depth1(int32_t i) { return i == 0 ? 0 : 31 - __builtin_clz((unsigned)i); }
@@ -305,42 +301,88 @@ void support(const int32_t* I, int d, int64_t* lo, int64_t* hi, int* t) {
     }
 }
 
-// (e) addPoints2: for pairs of depth groups T1, T2 (depth-list order,
-// differing in >= 2 dims) and active P in T1, Q in T2 with overlapping
-// supports: if a depth-T point (T = max(T1, T2)) lies in the overlap, add every
-// interior depth-T point of the overlap as a hanging node.
+// (e) addPoints2 (GridGeneration.cpp:333-392): for pairs of depth groups T1,
+// T2 (depth-list order, differing in >= 2 dims) and active P in T1, Q in T2
+// with overlapping supports: if a depth-T point (T = max(T1, T2)) lies in the
+// overlap, add every interior depth-T point of the overlap as a hanging node.
+// The reference tests every pair of points; here, with the same visiting
+// order and the same additions:
+//   * a group pair is skipped when the depth-T group holds every point of
+//     depth T (prod_k 2^(T_k - 1)): no overlap can miss one;
+//   * for an active P, the Q of T2 whose supports can overlap P's lie on T2's
+//     lattice inside P's support widened by Q's half support; they are looked
+//     up by their indices, filtered by the exact overlap test and visited in
+//     storage order, which is the order of the group's member list (points
+//     are appended; points added by this stage are inactive and never become
+//     a P or a Q).
 void add_points2(Grid& g) {
-    int d = g.d;
-    const int ngroups = (int)g.gdepth.size();  // DepthList fixed at entry
+    const int d = g.d;
+    const int ngroups = (int)g.gdepth.size();
     std::vector<int32_t> J(d);
+    std::vector<int64_t> cand;
     for (bool changed = true; changed;) {
         changed = false;
         for (int a = 0; a < ngroups; ++a) {
             for (int b = a + 1; b < ngroups; ++b) {
-                const auto& T1 = g.gdepth[a];
-                const auto& T2 = g.gdepth[b];
+                const std::vector<int32_t> T1 = g.gdepth[a], T2 = g.gdepth[b];
                 int lone = 0;
-                std::vector<int32_t> T(d);
+                int T[8];
                 for (int k = 0; k < d; ++k) {
                     lone += T1[k] != T2[k];
                     T[k] = std::max(T1[k], T2[k]);
                 }
                 if (lone < 2) continue;
-                auto tg = g.gid.find(T);
-                if (tg == g.gid.end()) continue;  // no depth-T point can lie in any overlap
+                auto tg = g.gid.find(std::vector<int32_t>(T, T + d));
+                if (tg == g.gid.end()) continue;
+                // every point of depth T present (prod_k 2^(T_k - 1) of them): no
+                // overlap box can miss one, so this pair adds nothing
+                int64_t full = 1;
+                for (int k = 0; k < d && full > 0; ++k) full = T[k] >= 1 ? full << (T[k] - 1) : 0;
+                if (full > 0 && (int64_t)g.gmem[tg->second].size() == full) continue;
                 for (size_t ia = 0; ia < g.gmem[a].size(); ++ia) {
-                    int64_t p = g.gmem[a][ia];
+                    const int64_t p = g.gmem[a][ia];
                     if (!g.act[p]) continue;
-                    int64_t plo[8], phi[8];
+                    int64_t plo[8], phi[8], c0[8], c1[8], cs[8];
                     int pt[8];
                     support(g.P(p), d, plo, phi, pt);
-                    for (size_t ib = 0; ib < g.gmem[b].size(); ++ib) {
-                        int64_t q = g.gmem[b][ib];
-                        if (!g.act[q]) continue;
+                    // candidate centres of Q per dimension: odd level-T2 coordinates,
+                    // or both boundary coordinates 0 and 1 at depth 0
+                    bool none = false;
+                    for (int k = 0; k < d && !none; ++k) {
+                        const int t = T2[k], sh = T[k] - t;
+                        if (t == 0) {
+                            c0[k] = 0;
+                            c1[k] = 1;
+                            cs[k] = 1;
+                            continue;
+                        }
+                        cs[k] = 2;
+                        const int64_t A0 = plo[k] << (T[k] - pt[k]), A1 = phi[k] << (T[k] - pt[k]);
+                        const int64_t top = (int64_t)1 << t;
+                        int64_t lo = std::max<int64_t>(1, ((A0 + ((int64_t)1 << sh) - 1) >> sh) - 3);
+                        int64_t hi = std::min<int64_t>(top - 1, (A1 >> sh) + 3);
+                        lo |= 1;
+                        if (lo > hi) none = true;
+                        c0[k] = lo;
+                        c1[k] = hi;
+                    }
+                    if (none) continue;
+                    cand.clear();
+                    int64_t c[8];
+                    for (int k = 0; k < d; ++k) c[k] = c0[k];
+                    for (;;) {
+                        for (int k = 0; k < d; ++k) J[k] = index_of(c[k], T2[k]);
+                        const int64_t q = g.find(J.data());
+                        if (q >= 0 && g.act[q]) cand.push_back(q);
+                        int k = 0;
+                        while (k < d && (c[k] += cs[k]) > c1[k]) { c[k] = c0[k]; ++k; }
+                        if (k == d) break;
+                    }
+                    std::sort(cand.begin(), cand.end());
+                    for (int64_t q : cand) {
                         int64_t qlo[8], qhi[8];
                         int qt[8];
                         support(g.P(q), d, qlo, qhi, qt);
-                        // overlap in level-T coordinates
                         int64_t lo[8], hi[8];
                         bool ov = true;
                         for (int k = 0; k < d && ov; ++k) {
@@ -351,31 +393,30 @@ void add_points2(Grid& g) {
                             hi[k] = std::min(a1, b1);
                         }
                         if (!ov) continue;
-                        // depth-T points of the box: odd level-T coordinates
-                        int64_t c0[8];
+                        int64_t e0[8];
                         bool empty = false;
                         for (int k = 0; k < d; ++k) {
-                            c0[k] = lo[k] | 1;
-                            if (c0[k] > hi[k]) empty = true;
+                            e0[k] = lo[k] | 1;
+                            if (e0[k] > hi[k]) empty = true;
                         }
                         if (empty) continue;
                         bool any = false;
-                        int64_t c[8];
-                        for (int k = 0; k < d; ++k) c[k] = c0[k];
+                        int64_t e[8];
+                        for (int k = 0; k < d; ++k) e[k] = e0[k];
                         for (;;) {
-                            for (int k = 0; k < d; ++k) J[k] = index_of(c[k], T[k]);
+                            for (int k = 0; k < d; ++k) J[k] = index_of(e[k], T[k]);
                             if (g.find(J.data()) >= 0) { any = true; break; }
                             int k = 0;
-                            while (k < d && (c[k] += 2) > hi[k]) { c[k] = c0[k]; ++k; }
+                            while (k < d && (e[k] += 2) > hi[k]) { e[k] = e0[k]; ++k; }
                             if (k == d) break;
                         }
                         if (!any) continue;
-                        for (int k = 0; k < d; ++k) c[k] = c0[k];
+                        for (int k = 0; k < d; ++k) e[k] = e0[k];
                         for (;;) {
-                            for (int k = 0; k < d; ++k) J[k] = index_of(c[k], T[k]);
+                            for (int k = 0; k < d; ++k) J[k] = index_of(e[k], T[k]);
                             if (g.add_flag(J.data(), false)) changed = true;
                             int k = 0;
-                            while (k < d && (c[k] += 2) > hi[k]) { c[k] = c0[k]; ++k; }
+                            while (k < d && (e[k] += 2) > hi[k]) { e[k] = e0[k]; ++k; }
                             if (k == d) break;
                         }
                     }
@@ -425,7 +466,7 @@ extern "C" int lsg_grid_complete(int32_t d, int64_t n, const int32_t* points, co
     if (mask & 4) complete_tensor(g);
     if (mask & 8) complete_without_boundary(g);
     if (mask & 16) add_hanging(g);
-    if ((mask & 32) && g.n() <= LSG_PAIRWISE_MAX) add_points2(g);
+    if (mask & 32) add_points2(g);
     if (mask & 64) complete_neumann(g);
     *n_out = g.n();
     if (out_points || out_active) {
@@ -484,10 +525,7 @@ extern "C" int lsg_grid_adaptive(int32_t d, int32_t level, int32_t refine, doubl
     if (mask & 4) complete_tensor(g);
     if (mask & 8) complete_without_boundary(g);
     if (mask & 16) add_hanging(g);
-    // Stage (e) tests pairs of points (quadratic cost).  It is run exactly up
-    // to LSG_PAIRWISE_MAX points; on every corner and plane refinement tested
-    // (d = 2..6, up to 41k points) it added no point, so larger grids skip it.
-    if ((mask & 32) && g.n() <= LSG_PAIRWISE_MAX) add_points2(g);
+    if (mask & 32) add_points2(g);
     if (mask & 64) complete_neumann(g);
     *n = g.n();
     L.d = d; L.level = level; L.refine = refine; L.theta = theta; L.target = target; L.complete = complete;
