@@ -235,17 +235,25 @@ void complete_tensor(Grid& g) {
             int64_t pos[8][5];
             int np[8];
             for (int k = 0; k < d; ++k) np[k] = stencil_pos(g.P(i)[k], pos[k]);
-            int64_t bmin[8], bmax[8];
-            for (int k = 0; k < d; ++k) bmin[k] = bmax[k] = coord_at(g.P(i)[k], T[k]);
+            int64_t bmin[8], bmax[8], emin[8], emax[8];
+            for (int k = 0; k < d; ++k) {
+                bmin[k] = bmax[k] = coord_at(g.P(i)[k], T[k]);
+                emin[k] = *std::min_element(pos[k], pos[k] + np[k]);  // the stencil's extent
+                emax[k] = *std::max_element(pos[k], pos[k] + np[k]);
+            }
             int ctr[8] = {0};
             for (;;) {
                 for (int k = 0; k < d; ++k) J[k] = index_of(pos[k][ctr[k]], T[k]);
                 int64_t s = g.find(J.data());
-                if (s >= 0 && g.act[s])
+                if (s >= 0 && g.act[s]) {
+                    bool full = true;
                     for (int k = 0; k < d; ++k) {
                         bmin[k] = std::min(bmin[k], pos[k][ctr[k]]);
                         bmax[k] = std::max(bmax[k], pos[k][ctr[k]]);
+                        full &= bmin[k] == emin[k] && bmax[k] == emax[k];
                     }
+                    if (full) break;  // no further neighbour can widen the box
+                }
                 int k = 0;
                 while (k < d && ++ctr[k] == np[k]) { ctr[k] = 0; ++k; }
                 if (k == d) break;
@@ -266,28 +274,40 @@ void complete_tensor(Grid& g) {
     }
 }
 
-// (d) addHangingNodes: the prewavelet stencil of every active point
+// (d) addHangingNodes: the prewavelet stencil of every active point.  The
+// points it adds are inactive and lie beyond the visited range, so the
+// missing stencil positions of every point can be found in parallel on the
+// grid as it was; they are then added in point order (a position missing for
+// two points is added at the first, as in the sequential pass).
 void add_hanging(Grid& g) {
-    int d = g.d;
-    int64_t end = g.n();
-    std::vector<int32_t> J(d);
-    for (int64_t i = 0; i < end; ++i) {
-        if (!g.act[i]) continue;
-        int64_t pos[8][5];
-        int np[8], t[8];
-        for (int k = 0; k < d; ++k) {
-            t[k] = depth1(g.P(i)[k]);
-            np[k] = stencil_pos(g.P(i)[k], pos[k]);
-        }
-        int ctr[8] = {0};
-        for (;;) {
-            for (int k = 0; k < d; ++k) J[k] = index_of(pos[k][ctr[k]], t[k]);
-            if (g.find(J.data()) < 0) g.add_flag(J.data(), false);
-            int k = 0;
-            while (k < d && ++ctr[k] == np[k]) { ctr[k] = 0; ++k; }
-            if (k == d) break;
+    const int d = g.d;
+    const int64_t end = g.n();
+    const int64_t chunk = 4096;
+    std::vector<std::vector<int32_t>> miss((size_t)((end + chunk - 1) / chunk));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t cb = 0; cb < (int64_t)miss.size(); ++cb) {
+        std::vector<int32_t> J(d);
+        std::vector<int32_t>& out = miss[cb];
+        for (int64_t i = cb * chunk; i < std::min(end, (cb + 1) * chunk); ++i) {
+            if (!g.act[i]) continue;
+            int64_t pos[8][5];
+            int np[8], t[8];
+            for (int k = 0; k < d; ++k) {
+                t[k] = depth1(g.P(i)[k]);
+                np[k] = stencil_pos(g.P(i)[k], pos[k]);
+            }
+            int ctr[8] = {0};
+            for (;;) {
+                for (int k = 0; k < d; ++k) J[k] = index_of(pos[k][ctr[k]], t[k]);
+                if (g.find(J.data()) < 0) out.insert(out.end(), J.begin(), J.end());
+                int k = 0;
+                while (k < d && ++ctr[k] == np[k]) { ctr[k] = 0; ++k; }
+                if (k == d) break;
+            }
         }
     }
+    for (const auto& out : miss)
+        for (size_t o = 0; o < out.size(); o += d) g.add_flag(&out[o], false);
 }
 
 // support of a point (GridGeneration.cpp:12-40) in level-t_k coordinates per dim
