@@ -122,6 +122,15 @@ def test_regular_sizes(d, level, n):
     assert lsg.AdaptiveSparseGrid.regular(d, level).n == n
 
 
+@pytest.mark.parametrize("d,level,refine,n,hanging", [(5, 4, 2, 5768, 5), (6, 5, 2, 40811, 6),
+                                                     (6, 7, 3, 499107, 6)])
+def test_corner_family_sizes(d, level, refine, n, hanging):
+    """The benchmark's grid family, completed with every stage of
+    completeDirichletGrid (addPoints2 included at every size)."""
+    g = lsg.AdaptiveSparseGrid.adaptive(d, level, refine, 0.6, "corner")
+    assert g.n == n and int((g.active == 0).sum()) == hanging
+
+
 def test_invalid_grids_rejected():
     with pytest.raises(lsg.LsgError):
         lsg.Plan(lsg.AdaptiveSparseGrid(np.array([[0, 2]], np.int32)))  # boundary point
