@@ -98,9 +98,10 @@ def test_reference_main_compiles_unchanged():
     """examples_doxygen/poisson_regular.cpp of the reference, as it is, with
     only the include path pointing at the compatibility header: it compiles
     and links against liblsg.so (the binary is kept for the GPU test)."""
-    ref = os.environ.get("LOADSG_REFERENCE")
+    # LOADSG_REFERENCE, else the build recipe's default location of the sources
+    ref = os.environ.get("LOADSG_REFERENCE") or __import__("__graft_entry__").REFSRC
     if not ref:
-        pytest.skip("LOADSG_REFERENCE (the reference's library/source directory) not set")
+        pytest.skip("the reference's library/source directory is not available (LOADSG_REFERENCE)")
     src = os.path.join(os.path.dirname(os.path.abspath(ref)), "examples_doxygen", "poisson_regular.cpp")
     if not os.path.exists(src):
         pytest.skip(f"{src} not found")
